@@ -1,0 +1,193 @@
+/*
+ * qdkp -- C ABI of the B200 eight-band k.p eigensolve library (libqdkp.so, sm_100a).
+ *
+ * Drop-in boundary for qd3Dsolver's eigensolve hot path. The reference is pure Python; its
+ * "interface" for this path is two Python entry points, and the functions below are what a
+ * ctypes / cffi binding of those entry points calls:
+ *
+ *   kp_pryor.confined_hamiltonian(ops, fields, n_bands, hole_convention, strain,
+ *                                 include_hydrostatic, interband_strain)   kp_pryor.py:363-466
+ *       -> qdkp_operator_create / qdkp_operator_update_diagonal / qdkp_operator_destroy
+ *   H @ X  (scipy CSR times a block, eigensolvers.py:86,98,307-308; scipy lobpcg.py:788)
+ *       -> qdkp_apply, qdkp_apply_host
+ *   eigensolvers.folded_operator(A, sigma)                                 eigensolvers.py:301-310
+ *       -> qdkp_apply(..., QDKP_APPLY_FOLDED)
+ *   eigensolvers.solve_interior / solve_lowest (scipy.sparse.linalg.lobpcg inside)
+ *                                            eigensolvers.py:200-268, 313-372
+ *       -> qdkp_lobpcg_workspace_size / qdkp_lobpcg_solve
+ *   eigensolvers.residual_norms / rayleigh_quotients                       eigensolvers.py:76-101
+ *       -> qdkp_residuals
+ *
+ * Conventions
+ *   - Every function returns an int status: QDKP_OK (0) or a negative QDKP_ERR_* code;
+ *     qdkp_last_error() returns the message of the last failure on the calling thread.
+ *   - Grids are C-ordered (x slowest, z fastest); a coefficient field is n_sites doubles.
+ *   - Vector blocks are row-major (n, m) complex arrays with a leading dimension ld >= m
+ *     (numpy's C-ordered complex128 / complex64 layout); row = band * n_sites + site (band-major,
+ *     kp_confined.py:66 with sp.bmat at kp_pryor.py:466).
+ *   - "dev" pointers are CUDA device pointers on the operator's device; "stream" is a
+ *     cudaStream_t passed as void* (NULL = legacy default stream).
+ *   - The library allocates device memory only inside qdkp_operator_create (its coefficient
+ *     fields). Every other buffer, workspaces included, belongs to the caller.
+ */
+#ifndef QDKP_H
+#define QDKP_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  QDKP_OK = 0,
+  QDKP_ERR_ARG = -1,
+  QDKP_ERR_CUDA = -2,
+  QDKP_ERR_UNSUPPORTED = -3,
+  QDKP_ERR_WORKSPACE = -4,
+  QDKP_ERR_NUMERIC = -5
+};
+
+/* operator flags (kp_pryor.confined_hamiltonian keyword arguments) */
+enum {
+  QDKP_HOLE_CONVENTION = 1,  /* negate a 6- or 4-band operator (kp_pryor.py:239-240, 464) */
+  QDKP_STRAIN = 2,           /* Bir-Pikus shear terms from the strain fields (kp_pryor.py:419-424) */
+  QDKP_INTERBAND_STRAIN = 4  /* Pryor's u, v terms, 8-band only (kp_pryor.py:439-454) */
+};
+
+/* arithmetic of a vector block */
+enum { QDKP_C128 = 0, QDKP_C64 = 1 };
+
+/* qdkp_apply modes: Y = H X, Y = (H - sigma) X, Y = (H - sigma)^2 X */
+enum { QDKP_APPLY_PLAIN = 0, QDKP_APPLY_SHIFTED = 1, QDKP_APPLY_FOLDED = 2 };
+
+/* order of the 15 coefficient fields handed to qdkp_operator_create (kp_pryor.material_fields
+ * keys plus the six strain components, kp_pryor.py:564-593, strain_fourier.py:84-139) */
+enum {
+  QDKP_FIELD_GAMMA1 = 0, QDKP_FIELD_GAMMA2, QDKP_FIELD_GAMMA3, QDKP_FIELD_P0, QDKP_FIELD_EC,
+  QDKP_FIELD_EV, QDKP_FIELD_DELTA_SO, QDKP_FIELD_B, QDKP_FIELD_D, QDKP_FIELD_EXX,
+  QDKP_FIELD_EYY, QDKP_FIELD_EZZ, QDKP_FIELD_EXY, QDKP_FIELD_EYZ, QDKP_FIELD_EZX,
+  QDKP_FIELD_COUNT
+};
+
+typedef struct qdkp_operator qdkp_operator;
+
+/* Last error message of the calling thread ("" if none). */
+const char* qdkp_last_error(void);
+
+/* Library version string. */
+const char* qdkp_version(void);
+
+/*
+ * Build the device-resident operator; replaces kp_pryor.confined_hamiltonian
+ * (kp_pryor.py:363-466) with `ops` = GridOperators(shape=(nx,ny,nz), h, periodic=False,
+ * scheme='central') (kp_confined.py:398-454). fields[i] points to n_sites host doubles in
+ * QDKP_FIELD_* order. Fields a model does not use may be NULL (P0 for 6/4 bands, strain when
+ * QDKP_STRAIN is clear). The include_hydrostatic keyword is applied by the caller by folding
+ * a_c Tr(eps) into Ec and -a_v Tr(eps) into Ev before the call (the same sum, kp_pryor.py:425-428).
+ * n_bands is 8, 6 or 4 (kp_pryor.py:70).
+ */
+int qdkp_operator_create(int nx, int ny, int nz, double h, int n_bands, int flags,
+                         const double* const* fields, int device, qdkp_operator** out);
+
+/* Replace the Ec / Ev fields in place (Hartree or piezo potential updates that change only the
+ * diagonal, as pryor_fig6.eight_band_states does per iteration, pryor_fig6.py:97-106).
+ * Either pointer may be NULL to keep that field. Host doubles, n_sites each. */
+int qdkp_operator_update_diagonal(qdkp_operator* op, const double* Ec, const double* Ev);
+
+/* Grid shape, size and the nonzero count of the equivalent CSR (H.shape / H.nnz in
+ * pryor_fig4.py:148, heterostructure.py:842,988). Any output pointer may be NULL. */
+int qdkp_operator_info(const qdkp_operator* op, int* nx, int* ny, int* nz, int* n_bands,
+                       int64_t* n, int64_t* nnz);
+
+int qdkp_operator_destroy(qdkp_operator* op);
+
+/* Structural nonzero count of the CSR kp_pryor.confined_hamiltonian assembles for this grid
+ * and flags (every stencil coupling counted, clipped at the walls). scipy additionally drops
+ * entries whose value cancels to exactly 0 (e.g. diagonal strain terms on symmetry planes), so
+ * the reference's H.nnz is at most this. Needs no GPU. */
+int64_t qdkp_structural_nnz(int nx, int ny, int nz, int n_bands, int flags);
+
+/*
+ * Y = op(X) on device blocks: X (n, m) with leading dimension ldx, Y (n, m) with ldy, both
+ * complex128 (precision QDKP_C128) or complex64 (QDKP_C64). mode QDKP_APPLY_FOLDED needs a
+ * workspace of n * m complex elements of the same precision (ws, ws_bytes); the other modes
+ * take ws = NULL. X and Y must not overlap.
+ */
+int qdkp_apply(const qdkp_operator* op, const void* X, int64_t ldx, void* Y, int64_t ldy,
+               int m, double sigma, int mode, int precision, void* ws, size_t ws_bytes,
+               void* stream);
+
+/* Workspace bytes qdkp_apply_host needs for an (n, m) complex128 block in `mode`. */
+size_t qdkp_apply_host_workspace_size(const qdkp_operator* op, int m, int mode);
+
+/* The same apply on HOST complex128 buffers (the `A @ X` a scipy LinearOperator performs):
+ * copies X to the device workspace, applies, copies Y back; synchronous on `stream`. */
+int qdkp_apply_host(const qdkp_operator* op, const void* X_host, void* Y_host, int m,
+                    double sigma, int mode, void* ws, size_t ws_bytes, void* stream);
+
+/*
+ * LOBPCG (scipy.sparse.linalg.lobpcg as called by eigensolvers.py:247-248, 352-353:
+ * B = None, Y = None, largest = False) on A = op (folded = 0) or A = (op - sigma)^2
+ * (folded = 1, eigensolvers.folded_operator). All vectors stay on the device.
+ */
+typedef struct {
+  int block;             /* sizeX, columns of X0 */
+  int folded;            /* 1: A = (H - sigma)^2 (solve_interior), 0: A = H (solve_lowest) */
+  double sigma;
+  double tol;            /* residual tolerance on A; <= 0 selects sqrt(eps) * n (scipy) */
+  int maxiter;
+  int restart_control;   /* forced restart when the mean residual exceeds 2^this x best (20) */
+  int precision;         /* QDKP_C128 (plain) or QDKP_C64 (search directions in complex64) */
+  int verbosity;         /* 0 = silent */
+} qdkp_lobpcg_params;
+
+typedef struct {
+  int iterations;          /* len(residualNormsHistory) as scipy returns it */
+  int best_iteration;
+  int status;              /* QDKP_LOBPCG_* below */
+  int explicit_gram;       /* 1 once the Gram matrices were formed explicitly */
+  double best_mean_residual;
+  double seconds;          /* wall time inside qdkp_lobpcg_solve */
+  int64_t hx_applications; /* H X block applications (counted per column block) */
+} qdkp_lobpcg_info;
+
+enum {
+  QDKP_LOBPCG_CONVERGED = 0,        /* every residual below tol */
+  QDKP_LOBPCG_MAXITER = 1,          /* ran out of iterations; best iterate returned */
+  QDKP_LOBPCG_RCHOL_BREAKDOWN = 2,  /* Cholesky of the residual Gram failed (scipy breaks) */
+  QDKP_LOBPCG_EIGH_BREAKDOWN = 3,   /* the restart Rayleigh-Ritz eigh failed (scipy breaks) */
+  QDKP_LOBPCG_NONFINITE = 4         /* a residual became NaN/inf */
+};
+
+/* Workspace bytes qdkp_lobpcg_solve needs for an n x block problem. */
+size_t qdkp_lobpcg_workspace_size(const qdkp_operator* op, const qdkp_lobpcg_params* prm);
+
+/*
+ * Run LOBPCG. X0 (device, n x block complex128, leading dimension block) is the start block
+ * and is not modified. On return lambda[block] (host) holds the final Ritz values of A in
+ * ascending order and V (device, n x block complex128) the Ritz vectors of the best iterate
+ * after the final Rayleigh-Ritz (scipy lobpcg.py:1009-1060); resid_history (host, may be
+ * NULL) receives (maxiter + 3) x block residual norms, row-major, info->iterations rows used.
+ */
+int qdkp_lobpcg_solve(const qdkp_operator* op, const qdkp_lobpcg_params* prm, const void* X0,
+                      double* lambda, void* V, double* resid_history, qdkp_lobpcg_info* info,
+                      void* ws, size_t ws_bytes, void* stream);
+
+/*
+ * Rayleigh quotients and residual norms of H for the columns of V (device, n x k complex128,
+ * leading dimension ldv): rq[j] = v^H H v / v^H v and res[j] = ||H v_j - E_j v_j|| on the
+ * normalised v_j, with E = E_in if non-NULL else rq (eigensolvers.residual_norms /
+ * rayleigh_quotients, eigensolvers.py:76-101). rq and res are host arrays of k doubles.
+ * Workspace: qdkp_residuals_workspace_size bytes.
+ */
+size_t qdkp_residuals_workspace_size(const qdkp_operator* op, int k);
+int qdkp_residuals(const qdkp_operator* op, const void* V, int64_t ldv, int k,
+                   const double* E_in, double* rq, double* res, void* ws, size_t ws_bytes,
+                   void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* QDKP_H */

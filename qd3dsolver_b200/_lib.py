@@ -1,0 +1,98 @@
+"""ctypes binding of libqdkp.so (the C ABI declared in include/qdkp.h).
+
+The library is loaded from this package directory. There is no CPU fallback: if the shared
+object is missing or fails to load, every entry point raises.
+"""
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, 'libqdkp.so')
+
+QDKP_OK = 0
+HOLE_CONVENTION, STRAIN, INTERBAND_STRAIN = 1, 2, 4
+C128, C64 = 0, 1
+APPLY_PLAIN, APPLY_SHIFTED, APPLY_FOLDED = 0, 1, 2
+LOBPCG_STATUS = {0: 'converged', 1: 'maxiter', 2: 'cholesky_breakdown',
+                 3: 'eigh_breakdown', 4: 'nonfinite'}
+
+
+class QdkpError(RuntimeError):
+    pass
+
+
+class LobpcgParams(ctypes.Structure):
+    _fields_ = [('block', ctypes.c_int), ('folded', ctypes.c_int), ('sigma', ctypes.c_double),
+                ('tol', ctypes.c_double), ('maxiter', ctypes.c_int),
+                ('restart_control', ctypes.c_int), ('precision', ctypes.c_int),
+                ('verbosity', ctypes.c_int)]
+
+
+class LobpcgInfo(ctypes.Structure):
+    _fields_ = [('iterations', ctypes.c_int), ('best_iteration', ctypes.c_int),
+                ('status', ctypes.c_int), ('explicit_gram', ctypes.c_int),
+                ('best_mean_residual', ctypes.c_double), ('seconds', ctypes.c_double),
+                ('hx_applications', ctypes.c_int64)]
+
+
+_lib = None
+
+_SIGNATURES = {
+    'qdkp_last_error': (ctypes.c_char_p, []),
+    'qdkp_version': (ctypes.c_char_p, []),
+    'qdkp_operator_create': (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                            ctypes.c_double, ctypes.c_int, ctypes.c_int,
+                                            ctypes.POINTER(ctypes.c_void_p), ctypes.c_int,
+                                            ctypes.POINTER(ctypes.c_void_p)]),
+    'qdkp_operator_update_diagonal': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p,
+                                                     ctypes.c_void_p]),
+    'qdkp_operator_info': (ctypes.c_int, [ctypes.c_void_p] + [ctypes.POINTER(ctypes.c_int)] * 4
+                           + [ctypes.POINTER(ctypes.c_int64)] * 2),
+    'qdkp_operator_destroy': (ctypes.c_int, [ctypes.c_void_p]),
+    'qdkp_structural_nnz': (ctypes.c_int64, [ctypes.c_int] * 5),
+    'qdkp_apply': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+                                  ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_double,
+                                  ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t,
+                                  ctypes.c_void_p]),
+    'qdkp_apply_host_workspace_size': (ctypes.c_size_t, [ctypes.c_void_p, ctypes.c_int,
+                                                         ctypes.c_int]),
+    'qdkp_apply_host': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                       ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                       ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]),
+    'qdkp_lobpcg_workspace_size': (ctypes.c_size_t, [ctypes.c_void_p,
+                                                     ctypes.POINTER(LobpcgParams)]),
+    'qdkp_lobpcg_solve': (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(LobpcgParams),
+                                         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                         ctypes.c_void_p, ctypes.POINTER(LobpcgInfo),
+                                         ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]),
+    'qdkp_residuals_workspace_size': (ctypes.c_size_t, [ctypes.c_void_p, ctypes.c_int]),
+    'qdkp_residuals': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+                                      ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t,
+                                      ctypes.c_void_p]),
+}
+
+# Every symbol include/qdkp.h declares (checked by the CPU test suite).
+EXPORTS = tuple(_SIGNATURES)
+
+
+def lib():
+    """Load libqdkp.so once; raise if it is absent (there is no CPU fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise QdkpError(f"{LIB_PATH} is missing: build it with "
+                            f"`python -m qd3dsolver_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(rc, what):
+    if rc != QDKP_OK:
+        msg = lib().qdkp_last_error().decode(errors='replace')
+        raise QdkpError(f"{what} failed ({rc}): {msg}")

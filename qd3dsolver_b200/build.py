@@ -1,0 +1,66 @@
+"""Build libqdkp.so (sm_100a) in-tree with nvcc.
+
+    python -m qd3dsolver_b200.build [--verbose-ptxas]
+
+Compiles every .cu file of qd3dsolver_b200/csrc into qd3dsolver_b200/libqdkp.so. Objects go to
+qd3dsolver_b200/_build/ and are reused while their source and headers are unchanged.
+"""
+import hashlib
+import os
+import subprocess
+import sys
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+CSRC = os.path.join(PKG, 'csrc')
+BUILD = os.path.join(PKG, '_build')
+LIB = os.path.join(PKG, 'libqdkp.so')
+NVCC = os.environ.get('NVCC', '/usr/local/cuda/bin/nvcc')
+ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
+FLAGS = ['-O3', '-lineinfo', '-std=c++17', '-Xcompiler', '-fPIC', '--expt-relaxed-constexpr',
+         '-I', os.path.join(ROOT, 'include')]
+
+
+def _headers_digest():
+    h = hashlib.sha1()
+    for d in (CSRC, os.path.join(ROOT, 'include')):
+        for f in sorted(os.listdir(d)):
+            if f.endswith(('.cuh', '.h')):
+                with open(os.path.join(d, f), 'rb') as fh:
+                    h.update(fh.read())
+    return h.hexdigest()[:12]
+
+
+def build(verbose_ptxas=False, force=False):
+    os.makedirs(BUILD, exist_ok=True)
+    hdr = _headers_digest()
+    objs = []
+    for f in sorted(os.listdir(CSRC)):
+        if not f.endswith('.cu'):
+            continue
+        src = os.path.join(CSRC, f)
+        with open(src, 'rb') as fh:
+            dig = hashlib.sha1(fh.read() + hdr.encode() + ' '.join(FLAGS).encode()).hexdigest()[:16]
+        obj = os.path.join(BUILD, f"{f[:-3]}-{dig}.o")
+        objs.append(obj)
+        if os.path.exists(obj) and not force and not verbose_ptxas:
+            continue
+        cmd = [NVCC] + ARCH + FLAGS + ['-c', src, '-o', obj]
+        if verbose_ptxas:
+            cmd += ['-Xptxas', '-v']
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"nvcc failed on {f}:\n{r.stdout}\n{r.stderr}")
+        if verbose_ptxas:
+            sys.stderr.write(r.stderr)
+    tmp = LIB + '.tmp'
+    cmd = [NVCC] + ARCH + ['-shared', '-o', tmp] + objs + ['-lcudart']
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    os.replace(tmp, LIB)
+    return LIB
+
+
+if __name__ == '__main__':
+    print(build(verbose_ptxas='--verbose-ptxas' in sys.argv, force='--force' in sys.argv))

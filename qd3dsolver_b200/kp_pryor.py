@@ -1,0 +1,258 @@
+"""Drop-in for qd3Dsolver's `kp_pryor.confined_hamiltonian` backed by the B200 library.
+
+`confined_hamiltonian(ops, fields, n_bands=8, hole_convention=False, strain=None,
+include_hydrostatic=False, interband_strain=True)` takes the reference's arguments
+(kp_pryor.py:363-364) and returns a `KPOperator`: a scipy `LinearOperator` whose coefficient
+fields live on the GPU and whose `@` runs the matrix-free CUDA stencil instead of a CSR product.
+It provides everything the reference's callers use on `H` (shape, nnz, dtype, `H @ X` for 1-D
+and 2-D arrays, `diagonal()`), plus device-side application on torch tensors for the solvers.
+"""
+import ctypes
+
+import numpy as np
+import scipy.sparse.linalg as spla
+
+from . import _lib
+from ._lib import check, lib
+
+G = 0.0380998                      # eV nm^2, qdsolver_core.py:19
+FIELD_ORDER = ('gamma1', 'gamma2', 'gamma3', 'P0', 'Ec', 'Ev', 'delta_so', 'b', 'd',
+               'exx', 'eyy', 'ezz', 'exy', 'eyz', 'ezx')
+STRAIN_KEYS = ('exx', 'eyy', 'ezz', 'exy', 'eyz', 'ezx')
+BAND_LABELS_8 = ['CB+1/2', 'CB-1/2', 'LH+1/2', 'HH+3/2', 'HH-3/2', 'LH-1/2', 'SO+1/2', 'SO-1/2']
+BAND_SLICES = {8: slice(0, 8), 6: slice(2, 8), 4: slice(2, 6)}
+
+
+class GridOperators:
+    """Grid description with the interface of kp_confined.GridOperators (kp_confined.py:
+    398-454) that the device operator needs: shape, h, periodic, scheme. No CSR is built."""
+
+    SCHEMES = ('central',)
+
+    def __init__(self, shape, h, periodic=False, scheme='central'):
+        if scheme not in self.SCHEMES:
+            raise ValueError(f"scheme must be one of {self.SCHEMES}, got {scheme!r}")
+        self.shape = tuple(int(s) for s in shape)
+        self.h = float(h)
+        self.periodic = bool(periodic)
+        self.scheme = scheme
+
+
+def _strain_dict(strain):
+    if strain is None:
+        return None
+    if isinstance(strain, dict):
+        return {k: np.asarray(strain[k], dtype=float) for k in STRAIN_KEYS}
+    return {k: np.asarray(getattr(strain, k), dtype=float) for k in STRAIN_KEYS}
+
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        raise _lib.QdkpError("the qdkp operator needs a CUDA device; none is visible")
+    return torch
+
+
+class KPOperator(spla.LinearOperator):
+    """Device-resident eight- (or six-/four-) band k.p operator."""
+
+    def __init__(self, shape, h, n_bands, flags, fields, device=None):
+        torch = _torch()
+        self.grid_shape = tuple(int(s) for s in shape)
+        self.h = float(h)
+        self.n_bands = int(n_bands)
+        self.flags = int(flags)
+        self.device = torch.cuda.current_device() if device is None else int(device)
+        self.n_sites = int(np.prod(self.grid_shape))
+        n = self.n_bands * self.n_sites
+        super().__init__(dtype=np.dtype(np.complex128), shape=(n, n))
+        self._fields = {k: np.ascontiguousarray(fields[k], dtype=np.float64).ravel()
+                        if fields.get(k) is not None else None for k in FIELD_ORDER}
+        ptrs = (ctypes.c_void_p * len(FIELD_ORDER))(
+            *[v.ctypes.data if v is not None else None for v in
+              (self._fields[k] for k in FIELD_ORDER)])
+        h_ = ctypes.c_void_p()
+        nx, ny, nz = self.grid_shape
+        check(lib().qdkp_operator_create(nx, ny, nz, self.h, self.n_bands, self.flags, ptrs,
+                                         self.device, ctypes.byref(h_)),
+              'qdkp_operator_create')
+        self._handle = h_
+        nnz = ctypes.c_int64()
+        check(lib().qdkp_operator_info(h_, None, None, None, None, None, ctypes.byref(nnz)),
+              'qdkp_operator_info')
+        self._nnz = int(nnz.value)
+        self._ws = None
+
+    # -- lifetime ---------------------------------------------------------------------------
+    def close(self):
+        if getattr(self, '_handle', None) is not None and self._handle.value:
+            lib().qdkp_operator_destroy(self._handle)
+            self._handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        if self._handle is None:
+            raise _lib.QdkpError("operator has been closed")
+        return self._handle
+
+    # -- what the reference's callers use on H ----------------------------------------------
+    @property
+    def nnz(self):
+        """Structural nonzero count of the CSR the reference would assemble."""
+        return self._nnz
+
+    def diagonal(self):
+        """diag(H), the Jacobi preconditioner input (eigensolvers.py:154)."""
+        f = {k: (v.reshape(self.grid_shape) if v is not None else np.zeros(self.grid_shape))
+             for k, v in self._fields.items()}
+        h2 = self.h ** 2
+        dk = []
+        for key in ('gamma1', 'gamma2'):
+            a = f[key]
+            out = []
+            for ax in range(3):
+                d = np.zeros(self.grid_shape)
+                n = self.grid_shape[ax]
+                lo = [slice(None)] * 3
+                hi = [slice(None)] * 3
+                lo[ax] = slice(0, n - 1)
+                hi[ax] = slice(1, n)
+                t = 0.5 * (a[tuple(lo)] + a[tuple(hi)]) / h2
+                d[tuple(lo)] += t
+                d[tuple(hi)] += t
+                for edge in (0, n - 1):
+                    sl = [slice(None)] * 3
+                    sl[ax] = edge
+                    d[tuple(sl)] += a[tuple(sl)] / h2
+                out.append(d)
+            dk.append(out)
+        A = f['Ec'] + 6 * G / h2
+        P = -f['Ev'] + G * (dk[0][0] + dk[0][1] + dk[0][2])
+        Q = G * (dk[1][0] + dk[1][1] - 2 * dk[1][2])
+        if self.flags & _lib.STRAIN:
+            Q = Q - (f['b'] / 2.0) * (f['exx'] + f['eyy'] - 2.0 * f['ezz'])
+        bands = [A, A, -P + Q, -P - Q, -P - Q, -P + Q, -P - f['delta_so'], -P - f['delta_so']]
+        sl = BAND_SLICES[self.n_bands]
+        d = np.concatenate([b.ravel() for b in bands[sl]])
+        if (self.flags & _lib.HOLE_CONVENTION) and self.n_bands != 8:
+            d = -d
+        return d.astype(np.complex128)
+
+    def tocsc(self):
+        raise NotImplementedError("KPOperator is matrix-free: ILU preconditioning "
+                                  "(eigensolvers.ilu_preconditioner) needs the CSR path")
+
+    def __sub__(self, other):
+        raise NotImplementedError("KPOperator is matrix-free: form shifts with "
+                                  "apply(..., sigma=...) instead of H - sigma * I")
+
+    def _adjoint(self):
+        return self                                       # Hermitian by construction
+
+    # -- host application (scipy LinearOperator protocol) ------------------------------------
+    def _matvec(self, x):
+        return self._matmat(np.asarray(x).reshape(-1, 1)).reshape(-1)
+
+    def _matmat(self, X):
+        return self.apply_host(X)
+
+    def apply_host(self, X, sigma=0.0, mode=_lib.APPLY_PLAIN):
+        torch = _torch()
+        X = np.ascontiguousarray(X, dtype=np.complex128)
+        if X.ndim != 2 or X.shape[0] != self.shape[0]:
+            raise ValueError(f"expected an ({self.shape[0]}, m) block, got {X.shape}")
+        m = X.shape[1]
+        need = int(lib().qdkp_apply_host_workspace_size(self.handle, m, mode))
+        if self._ws is None or self._ws.numel() < need:
+            self._ws = torch.empty(need, dtype=torch.uint8, device=f'cuda:{self.device}')
+        Y = np.empty_like(X)
+        stream = torch.cuda.current_stream(self.device).cuda_stream
+        check(lib().qdkp_apply_host(self.handle, X.ctypes.data, Y.ctypes.data, m, float(sigma),
+                                    mode, self._ws.data_ptr(), self._ws.numel(), stream),
+              'qdkp_apply_host')
+        return Y
+
+    # -- device application -------------------------------------------------------------------
+    def apply(self, X, sigma=0.0, mode=_lib.APPLY_PLAIN, out=None, workspace=None):
+        """Y = H X, (H - sigma) X or (H - sigma)^2 X for a CUDA tensor X of shape (n, m),
+        complex128 or complex64 (row stride may exceed m)."""
+        torch = _torch()
+        if X.dim() != 2 or X.shape[0] != self.shape[0] or X.stride(1) != 1:
+            raise ValueError("X must be an (n, m) CUDA tensor with unit column stride")
+        prec = {torch.complex128: _lib.C128, torch.complex64: _lib.C64}.get(X.dtype)
+        if prec is None:
+            raise TypeError("X must be complex128 or complex64")
+        m = X.shape[1]
+        Y = torch.empty_like(X, memory_format=torch.contiguous_format) if out is None else out
+        ws_ptr, ws_bytes = None, 0
+        if mode == _lib.APPLY_FOLDED:
+            if workspace is None:
+                workspace = torch.empty_like(X, memory_format=torch.contiguous_format)
+            ws_ptr, ws_bytes = workspace.data_ptr(), workspace.numel() * workspace.element_size()
+        stream = torch.cuda.current_stream(X.device).cuda_stream
+        check(lib().qdkp_apply(self.handle, X.data_ptr(), X.stride(0), Y.data_ptr(),
+                               Y.stride(0), m, float(sigma), mode, prec, ws_ptr, ws_bytes, stream),
+              'qdkp_apply')
+        return Y
+
+    def update_diagonal(self, Ec=None, Ev=None):
+        """Swap in new Ec / Ev fields (Hartree or potential updates) without re-uploading."""
+        a = np.ascontiguousarray(Ec, dtype=np.float64).ravel() if Ec is not None else None
+        b = np.ascontiguousarray(Ev, dtype=np.float64).ravel() if Ev is not None else None
+        check(lib().qdkp_operator_update_diagonal(self.handle,
+                                                  a.ctypes.data if a is not None else None,
+                                                  b.ctypes.data if b is not None else None),
+              'qdkp_operator_update_diagonal')
+        if a is not None:
+            self._fields['Ec'] = a
+        if b is not None:
+            self._fields['Ev'] = b
+
+
+def confined_hamiltonian(ops, fields, n_bands=8, hole_convention=False, strain=None,
+                         include_hydrostatic=False, interband_strain=True):
+    """Device-resident replacement of kp_pryor.confined_hamiltonian (kp_pryor.py:363-466).
+
+    `ops` is anything with `.shape` and `.h` (kp_confined.GridOperators or this module's
+    GridOperators); only hard walls and the 'central' scheme exist on the device.
+    """
+    if getattr(ops, 'periodic', False):
+        raise NotImplementedError("periodic grids are only used for bulk validation and are "
+                                  "not built on the device")
+    if getattr(ops, 'scheme', 'central') != 'central':
+        raise NotImplementedError("only the default 'central' cross-term scheme is built")
+    if n_bands not in BAND_SLICES:
+        raise ValueError("n_bands must be 8, 6 or 4")
+    shape = tuple(int(s) for s in ops.shape)
+    st = _strain_dict(strain)
+    f = {k: np.asarray(fields[k], dtype=float) for k in
+         ('gamma1', 'gamma2', 'gamma3', 'delta_so', 'Ev', 'Ec')}
+    for k, v in f.items():
+        if v.shape != shape:
+            f[k] = np.broadcast_to(v, shape).copy()
+    f['P0'] = np.asarray(fields['P0'], dtype=float) if n_bands == 8 else None
+    flags = 0
+    if hole_convention:
+        flags |= _lib.HOLE_CONVENTION
+    if st is not None:
+        flags |= _lib.STRAIN
+        if interband_strain and n_bands == 8:
+            flags |= _lib.INTERBAND_STRAIN
+        f['b'] = np.asarray(fields['b'], dtype=float)
+        f['d'] = np.asarray(fields['d'], dtype=float)
+        f.update(st)
+        if include_hydrostatic:
+            # A + a_c Tr(eps) and P + a_v Tr(eps) (kp_pryor.py:425-428); P = -Ev + ...
+            tr = st['exx'] + st['eyy'] + st['ezz']
+            f['Ec'] = f['Ec'] + np.asarray(fields['a_c']) * tr
+            f['Ev'] = f['Ev'] - np.asarray(fields['a_v']) * tr
+    for k in list(f):
+        if f[k] is not None and f[k].shape != shape:
+            f[k] = np.broadcast_to(f[k], shape).copy()
+    return KPOperator(shape, ops.h, n_bands, flags, f)
