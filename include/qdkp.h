@@ -53,7 +53,8 @@ enum {
 enum {
   QDKP_HOLE_CONVENTION = 1,  /* negate a 6- or 4-band operator (kp_pryor.py:239-240, 464) */
   QDKP_STRAIN = 2,           /* Bir-Pikus shear terms from the strain fields (kp_pryor.py:419-424) */
-  QDKP_INTERBAND_STRAIN = 4  /* Pryor's u, v terms, 8-band only (kp_pryor.py:439-454) */
+  QDKP_INTERBAND_STRAIN = 4, /* Pryor's u, v terms, 8-band only (kp_pryor.py:439-454) */
+  QDKP_NEGATE = 8            /* apply -H (eigensolvers.solve_lowest_hole, eigensolvers.py:385) */
 };
 
 /* arithmetic of a vector block */

@@ -10,7 +10,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, 'libqdkp.so')
 
 QDKP_OK = 0
-HOLE_CONVENTION, STRAIN, INTERBAND_STRAIN = 1, 2, 4
+HOLE_CONVENTION, STRAIN, INTERBAND_STRAIN, NEGATE = 1, 2, 4, 8
 C128, C64 = 0, 1
 APPLY_PLAIN, APPLY_SHIFTED, APPLY_FOLDED = 0, 1, 2
 LOBPCG_STATUS = {0: 'converged', 1: 'maxiter', 2: 'cholesky_breakdown',

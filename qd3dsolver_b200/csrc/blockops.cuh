@@ -1,0 +1,53 @@
+// Tall-skinny block kernels and one-CTA small dense FP64 kernels used by the LOBPCG driver.
+//
+// Blocks are row-major (n, cols) complex arrays with a leading dimension (elements). Every
+// reduction over the long dimension is two-stage and deterministic: each CTA writes a partial,
+// a second kernel sums the partials in a fixed order.
+#pragma once
+#include "qdkp_common.cuh"
+
+namespace qdkp {
+
+constexpr int kMaxBlock = 24;          // largest LOBPCG block width (columns) supported
+constexpr int kMaxSmall = 3 * kMaxBlock;  // largest Rayleigh-Ritz dimension
+constexpr int kTallThreads = 256;
+constexpr int kSmallThreads = 512;
+
+// A group of up to three column blocks concatenated along the columns: [B0 | B1 | B2].
+template <typename T>
+struct BlockList {
+  const cplx<T>* p[3];
+  long long ld[3];
+  int cols[3];
+  int nblk;
+  __host__ __device__ int total() const {
+    int t = 0;
+    for (int i = 0; i < nblk; ++i) t += cols[i];
+    return t;
+  }
+};
+
+int launch_colnorm2(const double2* A, long long lda, const double2* B, long long ldb,
+                    const double* lambda, int m, long long n, double* partial, int nparts,
+                    double* out, cudaStream_t st);
+int launch_resid_gather(const double2* AX, long long ldax, const double2* X, long long ldx,
+                        const double* lambda, const int* idx, int ma, long long n, double2* R,
+                        long long ldr, cudaStream_t st);
+int launch_gather(const double2* src, long long lds, const int* idx, int ma, long long n,
+                  double2* dst, long long ldd, cudaStream_t st);
+int launch_copy(const double2* src, long long lds, int cols, long long n, double2* dst,
+                long long ldd, cudaStream_t st);
+// out (P x Q, row-major, ld Q) = A^H B for concatenated column lists.
+int launch_gram(const BlockList<double>& A, const BlockList<double>& B, long long n,
+                double2* partial, size_t partial_elems, double2* out, cudaStream_t st);
+size_t gram_partial_elems(int P, int Q);
+// Y = beta * Y + sum_k A_k C_k; C_k (cols_k x q, row-major, ld q) in device memory.
+int launch_update(const BlockList<double>& A, const double2* const* C, int q, long long n,
+                  double2* Y, long long ldy, int accumulate, cudaStream_t st);
+
+// Small dense (one CTA). Matrices row-major with ld = n. status: 0 ok, 1 failure.
+int launch_chol_inv(const double2* G, int n, double2* Uinv, int* status, cudaStream_t st);
+int launch_eigh(const double2* A, const double2* B, int n, double* w, double2* V,
+                double2* scratch, int* status, cudaStream_t st);
+
+}  // namespace qdkp

@@ -343,6 +343,7 @@ static int launch_apply_t(const qdkp_operator* op, const T* F, const void* X, in
   a.nx = op->nx; a.ny = op->ny; a.nz = op->nz; a.m = m; a.flags = op->flags;
   a.h = (T)op->h; a.sigma = (T)sigma; a.shifted = shifted;
   a.sign = ((op->flags & QDKP_HOLE_CONVENTION) && op->n_bands != 8) ? T(-1) : T(1);
+  if (op->flags & QDKP_NEGATE) a.sign = -a.sign;
   int S = (512 + m - 1) / m;
   S = S < 32 ? 32 : (S > 128 ? 128 : S);
   a.S = S;

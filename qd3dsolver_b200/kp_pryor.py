@@ -142,6 +142,8 @@ class KPOperator(spla.LinearOperator):
         d = np.concatenate([b.ravel() for b in bands[sl]])
         if (self.flags & _lib.HOLE_CONVENTION) and self.n_bands != 8:
             d = -d
+        if self.flags & _lib.NEGATE:
+            d = -d
         return d.astype(np.complex128)
 
     def tocsc(self):
@@ -200,6 +202,13 @@ class KPOperator(spla.LinearOperator):
                                Y.stride(0), m, float(sigma), mode, prec, ws_ptr, ws_bytes, stream),
               'qdkp_apply')
         return Y
+
+    def negated(self):
+        """-H as a second device operator (same fields, sign flipped in the stencil)."""
+        f = {k: (v.reshape(self.grid_shape) if v is not None else None)
+             for k, v in self._fields.items()}
+        return KPOperator(self.grid_shape, self.h, self.n_bands, self.flags ^ _lib.NEGATE, f,
+                          self.device)
 
     def update_diagonal(self, Ec=None, Ev=None):
         """Swap in new Ec / Ev fields (Hartree or potential updates) without re-uploading."""
