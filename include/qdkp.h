@@ -74,6 +74,9 @@ enum {
 
 typedef struct qdkp_operator qdkp_operator;
 
+/* Number of CUDA kernels this library has launched in the process (diagnostic counter). */
+int64_t qdkp_kernel_launches(void);
+
 /* Last error message of the calling thread ("" if none). */
 const char* qdkp_last_error(void);
 
@@ -142,6 +145,7 @@ typedef struct {
   int restart_control;   /* forced restart when the mean residual exceeds 2^this x best (20) */
   int precision;         /* QDKP_C128 (plain) or QDKP_C64 (search directions in complex64) */
   int verbosity;         /* 0 = silent */
+  int time_hx;           /* 1: time every H X launch with CUDA events (info->hx_seconds) */
 } qdkp_lobpcg_params;
 
 typedef struct {
@@ -151,7 +155,10 @@ typedef struct {
   int explicit_gram;       /* 1 once the Gram matrices were formed explicitly */
   double best_mean_residual;
   double seconds;          /* wall time inside qdkp_lobpcg_solve */
-  int64_t hx_applications; /* H X block applications (counted per column block) */
+  int64_t hx_applications; /* H X column applications (folded counts two per column) */
+  int64_t hx_launches;     /* H X kernel launches */
+  double hx_seconds;       /* summed CUDA-event time of those launches (time_hx = 1) */
+  double hx_bytes;         /* algorithmic bytes of those launches: N (15 s_f + 2*8 m s_c) each */
 } qdkp_lobpcg_info;
 
 enum {

@@ -25,20 +25,22 @@ class LobpcgParams(ctypes.Structure):
     _fields_ = [('block', ctypes.c_int), ('folded', ctypes.c_int), ('sigma', ctypes.c_double),
                 ('tol', ctypes.c_double), ('maxiter', ctypes.c_int),
                 ('restart_control', ctypes.c_int), ('precision', ctypes.c_int),
-                ('verbosity', ctypes.c_int)]
+                ('verbosity', ctypes.c_int), ('time_hx', ctypes.c_int)]
 
 
 class LobpcgInfo(ctypes.Structure):
     _fields_ = [('iterations', ctypes.c_int), ('best_iteration', ctypes.c_int),
                 ('status', ctypes.c_int), ('explicit_gram', ctypes.c_int),
                 ('best_mean_residual', ctypes.c_double), ('seconds', ctypes.c_double),
-                ('hx_applications', ctypes.c_int64)]
+                ('hx_applications', ctypes.c_int64), ('hx_launches', ctypes.c_int64),
+                ('hx_seconds', ctypes.c_double), ('hx_bytes', ctypes.c_double)]
 
 
 _lib = None
 
 _SIGNATURES = {
     'qdkp_last_error': (ctypes.c_char_p, []),
+    'qdkp_kernel_launches': (ctypes.c_int64, []),
     'qdkp_version': (ctypes.c_char_p, []),
     'qdkp_operator_create': (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                             ctypes.c_double, ctypes.c_int, ctypes.c_int,

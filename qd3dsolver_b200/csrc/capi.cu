@@ -1,5 +1,6 @@
 // extern "C" entry points of libqdkp.so: operator lifecycle and H.X application.
 // The LOBPCG entry points live in lobpcg.cu.
+#include <atomic>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -10,6 +11,8 @@ namespace qdkp {
 
 static thread_local std::string g_last_error;
 void set_error(const std::string& msg) { g_last_error = msg; }
+static std::atomic<long long> g_launches{0};
+void count_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
 int launch_apply(const qdkp_operator* op, const void* X, int64_t ldx, void* Y, int64_t ldy,
                  int m, double sigma, int shifted, int precision, cudaStream_t st);
@@ -25,6 +28,7 @@ static int refresh_fields32(qdkp_operator* op, int first, int count) {
   const long long n = (long long)count * op->n_sites;
   const long long off = (long long)first * op->n_sites;
   to_float_kernel<<<1184, 256>>>(op->fields64 + off, op->fields32 + off, n);
+  count_launch();
   QDKP_CUDA_TRY(cudaGetLastError());
   QDKP_CUDA_TRY(cudaDeviceSynchronize());
   return QDKP_OK;
@@ -87,6 +91,8 @@ using namespace qdkp;
 extern "C" {
 
 const char* qdkp_last_error(void) { return g_last_error.c_str(); }
+
+int64_t qdkp_kernel_launches(void) { return g_launches.load(); }
 
 const char* qdkp_version(void) { return "qdkp 0.1 sm_100a"; }
 

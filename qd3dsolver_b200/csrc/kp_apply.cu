@@ -160,8 +160,12 @@ __device__ __forceinline__ void load_site(const ApplyArgs<T>& a, long long q, in
   }
 }
 
+template <typename T> struct ApplyOcc;
+template <> struct ApplyOcc<double> { static constexpr int kMinBlocks = 2; };
+template <> struct ApplyOcc<float> { static constexpr int kMinBlocks = 2; };
+
 template <typename T, int NB>
-__global__ void __launch_bounds__(256) kp_apply_kernel(const ApplyArgs<T> a) {
+__global__ void __launch_bounds__(256, ApplyOcc<T>::kMinBlocks) kp_apply_kernel(const ApplyArgs<T> a) {
   extern __shared__ unsigned char smem_raw[];
   T* rec = reinterpret_cast<T*>(smem_raw);
   const int S = a.S;
@@ -195,11 +199,16 @@ __global__ void __launch_bounds__(256) kp_apply_kernel(const ApplyArgs<T> a) {
     const long long str[3] = {(long long)a.ny * a.nz, (long long)a.nz, 1LL};
 
     cplx<T> y[8], x[8];
-#pragma unroll
-    for (int b = 0; b < 8; ++b) y[b] = czero<T>();
 
     // ---- local block ------------------------------------------------------------------
+    // y = sign (H x) - sigma x is accumulated as sign (H x - sign sigma x): start from the
+    // shift term so the centre values need not stay live until the end.
     load_site<T, NB, false>(a, s, j, x);
+    {
+      const T sh = a.shifted ? -a.sigma * a.sign : T(0);
+#pragma unroll
+      for (int b = 0; b < 8; ++b) y[b] = cscale(sh, x[b]);
+    }
     {
       const T A = r[R_A * S], P = r[R_P * S], Q = r[R_Q * S], Dl = r[R_DL * S];
       const cplx<T> R = mk<T>(r[R_RRE * S], r[R_RIM * S]);
@@ -218,8 +227,6 @@ __global__ void __launch_bounds__(256) kp_apply_kernel(const ApplyArgs<T> a) {
       caxpy(y[7], -sq2 * Q, x[2]); cfmac(y[7], Sx, cscale(isq2, x[3])); cfma(y[7], R, cscale(sq2, x[4]));
       cfma(y[7], Sx, cscale(sq32, x[5])); caxpy(y[7], -P - Dl, x[7]);
     }
-    const cplx<T> xc2 = x[2], xc3 = x[3], xc4 = x[4], xc5 = x[5], xc6 = x[6], xc7 = x[7];
-    const cplx<T> xc0 = x[0], xc1 = x[1];
 
     // ---- six face neighbours ------------------------------------------------------------
 #pragma unroll
@@ -319,14 +326,11 @@ __global__ void __launch_bounds__(256) kp_apply_kernel(const ApplyArgs<T> a) {
       }
     }
 
-    // ---- sign (hole convention), shift, store --------------------------------------------
-    const cplx<T> xcs[8] = {xc0, xc1, xc2, xc3, xc4, xc5, xc6, xc7};
+    // ---- sign (hole convention / negation), store ---------------------------------------
 #pragma unroll
     for (int b = 0; b < 8; ++b) {
       if (!has_band<NB>(b)) continue;
-      cplx<T> v = cscale(a.sign, y[b]);
-      if (a.shifted) caxpy(v, -a.sigma, xcs[b]);
-      a.Y[((long long)(b - band_off<NB>()) * a.N + s) * a.ldy + j] = v;
+      a.Y[((long long)(b - band_off<NB>()) * a.N + s) * a.ldy + j] = cscale(a.sign, y[b]);
     }
   }
 }
@@ -355,6 +359,7 @@ static int launch_apply_t(const qdkp_operator* op, const T* F, const void* X, in
     case 4: kp_apply_kernel<T, 4><<<grid, 256, smem, st>>>(a); break;
     default: set_error("n_bands must be 8, 6 or 4"); return QDKP_ERR_ARG;
   }
+  count_launch();
   QDKP_CUDA_TRY(cudaGetLastError());
   return QDKP_OK;
 }

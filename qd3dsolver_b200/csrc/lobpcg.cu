@@ -106,16 +106,51 @@ struct Solver {
   Layout L;
   Bufs b;
   int64_t applies = 0;
+  int64_t hx_launches = 0;
+  double hx_bytes = 0.0;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev;   // per-launch timing (time_hx)
+  size_t ev_used = 0;
+
+  int hx(const double2* V, int c, double2* out, double sigma, int shifted) {
+    ++hx_launches;
+    hx_bytes += (double)op->n_sites * (15.0 * 8.0 + 2.0 * 8.0 * c * 16.0);
+    if (!prm.time_hx) return launch_apply(op, V, c, out, c, c, sigma, shifted, QDKP_C128, st);
+    if (ev_used == ev.size()) {
+      cudaEvent_t a, b2;
+      QDKP_CUDA_TRY(cudaEventCreate(&a));
+      QDKP_CUDA_TRY(cudaEventCreate(&b2));
+      ev.emplace_back(a, b2);
+    }
+    auto& e = ev[ev_used++];
+    QDKP_CUDA_TRY(cudaEventRecord(e.first, st));
+    int rc = launch_apply(op, V, c, out, c, c, sigma, shifted, QDKP_C128, st);
+    QDKP_CUDA_TRY(cudaEventRecord(e.second, st));
+    return rc;
+  }
+
+  // Sum the recorded launch durations (events are complete after the caller's sync).
+  double hx_seconds() {
+    double t = 0.0;
+    for (size_t i = 0; i < ev_used; ++i) {
+      float ms = 0.f;
+      if (cudaEventElapsedTime(&ms, ev[i].first, ev[i].second) == cudaSuccess) t += ms * 1e-3;
+    }
+    return t;
+  }
+
+  ~Solver() {
+    for (auto& e : ev) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
+  }
 
   // A(V) for V (n x c, ld c) into out (ld c)
   int applyA(const double2* V, int c, double2* out) {
     applies += c;
     if (prm.folded) {
-      int rc = launch_apply(op, V, c, b.T, c, c, prm.sigma, 1, QDKP_C128, st);
+      int rc = hx(V, c, b.T, prm.sigma, 1);
       if (rc) return rc;
-      return launch_apply(op, b.T, c, out, c, c, prm.sigma, 1, QDKP_C128, st);
+      return hx(b.T, c, out, prm.sigma, 1);
     }
-    return launch_apply(op, V, c, out, c, c, 0.0, 0, QDKP_C128, st);
+    return hx(V, c, out, 0.0, 0);
   }
 
   int gram(BlockList<double> A, BlockList<double> B, double2* out) {
@@ -502,6 +537,10 @@ int qdkp_lobpcg_solve(const qdkp_operator* op, const qdkp_lobpcg_params* prm, co
   info->explicit_gram = explicit_gram;
   info->best_mean_residual = smallest;
   info->hx_applications = s.applies * (prm->folded ? 2 : 1);
+  info->hx_launches = s.hx_launches;
+  info->hx_bytes = s.hx_bytes;
+  QDKP_CUDA_TRY(cudaStreamSynchronize(st));
+  info->hx_seconds = prm->time_hx ? s.hx_seconds() : 0.0;
   info->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
 #undef TRY
   return QDKP_OK;

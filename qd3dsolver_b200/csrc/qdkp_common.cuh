@@ -53,6 +53,8 @@ QDKP_CPLX_OPS(float2, float)
 // Error handling: every entry point returns an int status and records a message.
 // ---------------------------------------------------------------------------------------------
 void set_error(const std::string& msg);
+// Counts kernel launches made by this library (qdkp_kernel_launches).
+void count_launch(int n = 1);
 
 #define QDKP_CUDA_TRY(expr)                                                              \
   do {                                                                                   \

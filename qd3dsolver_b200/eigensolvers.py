@@ -71,7 +71,7 @@ def _device_residuals(A, Vd, E=None):
 
 
 def lobpcg_device(A, X0, folded, sigma=0.0, tol=None, maxiter=20, restart_control=20,
-                  verbosity=0):
+                  verbosity=0, time_hx=False):
     """scipy.sparse.linalg.lobpcg(A or (A - sigma)^2, X0, largest=False) on the GPU.
 
     Returns (lambda, V_device, residual_history, info_dict)."""
@@ -82,7 +82,7 @@ def lobpcg_device(A, X0, folded, sigma=0.0, tol=None, maxiter=20, restart_contro
     prm = _lib.LobpcgParams(block=block, folded=int(bool(folded)), sigma=float(sigma),
                             tol=float(tol) if tol else 0.0, maxiter=int(maxiter),
                             restart_control=int(restart_control), precision=_lib.C128,
-                            verbosity=int(verbosity))
+                            verbosity=int(verbosity), time_hx=int(bool(time_hx)))
     need = int(lib().qdkp_lobpcg_workspace_size(A.handle, ctypes.byref(prm)))
     if need == 0:
         raise ValueError(f"block size {block} is outside the supported range [1, 24]")
@@ -100,6 +100,9 @@ def lobpcg_device(A, X0, folded, sigma=0.0, tol=None, maxiter=20, restart_contro
                                      status=_lib.LOBPCG_STATUS.get(info.status, 'unknown'),
                                      explicit_gram=bool(info.explicit_gram),
                                      hx_applications=int(info.hx_applications),
+                                     hx_launches=int(info.hx_launches),
+                                     hx_seconds=float(info.hx_seconds),
+                                     hx_bytes=float(info.hx_bytes),
                                      solver_seconds=info.seconds)
 
 
@@ -169,7 +172,7 @@ def folded_operator(A, sigma):
 # ------------------------------------------------------------------------------------------
 
 def solve_interior(A, k=4, sigma=0.0, M=None, tol=1e-8, maxiter=3000, extra=None, seed=0,
-                   verbose=True, certify_tol=1e-6, return_device=False):
+                   verbose=True, certify_tol=1e-6, return_device=False, time_hx=False):
     """Eigenpairs of A closest to sigma by folded-spectrum LOBPCG on the GPU."""
     A = _require_op(A)
     if M is not None:
@@ -182,7 +185,7 @@ def solve_interior(A, k=4, sigma=0.0, M=None, tol=1e-8, maxiter=3000, extra=None
     X0 = start_block(n, block, seed, True)
     t0 = time.time()
     mu, Vd, hist, dinfo = lobpcg_device(A, X0, folded=True, sigma=sigma, tol=tol,
-                                        maxiter=maxiter)
+                                        maxiter=maxiter, time_hx=time_hx)
     rq, _ = _device_residuals(A, Vd)
     order = np.argsort(np.abs(rq - sigma))[:k]
     E = rq[order]

@@ -335,3 +335,72 @@ def random_dot(rng, h=0.5, n_min=32, n_max=96, pairs=(2, 8), family='InGaAs/GaAs
     return build_environment(f"{shape_kind}_x{x:.2f}_b{base:.1f}_{nxy}x{nxy}x{nz}", mask, h,
                              dot, material('GaAs'), k=2 * npairs,
                              meta=dict(x=x, kind=shape_kind, base=base, height=height))
+
+
+# --------------------------------------------------------------------------------------------
+# Pryor (1998) InAs/GaAs benchmark: the reference's Fig-4 sweep (pryor_fig4.py)
+# --------------------------------------------------------------------------------------------
+
+#: Pryor's Table I (pryor1998.py:53-84): Luttinger, gap, spin-orbit, Ep, deformation
+#: potentials (Pryor's a_v sign), piezo e14, eps_R, elastic constants, lattice constant and the
+#: unstrained valence offset.
+PRYOR_TABLE_I = {
+    'InAs': dict(gamma1L=19.67, gamma2L=8.37, gamma3L=9.29, Eg=0.418, delta_so=0.38, Ep=22.2,
+                 a_c=-6.66, a_v=0.66, b=-1.8, d=-3.6, e14=0.045, eps_R=15.15,
+                 C11=83.29, C12=45.26, C44=39.59, a0=6.0583, E_vbo=0.085),
+    'GaAs': dict(gamma1L=6.85, gamma2L=2.1, gamma3L=2.9, Eg=1.519, delta_so=0.33, Ep=25.7,
+                 a_c=-9.3, a_v=0.7, b=-2.0, d=-5.4, e14=0.159, eps_R=15.15,
+                 C11=121.1, C12=54.8, C44=60.4, a0=5.6532, E_vbo=0.0),
+}
+#: Island base widths of the Fig-4 sweep (pryor_fig4.py:71).
+FIG4_SIZES = (6.0, 8.0, 10.0, 12.0, 14.0, 16.0, 18.0)
+
+
+def fig4_grid(base, h=1.0, pad=8.0):
+    """pryor_fig4.clean_grid: odd, mirror-symmetric x/y axis, island base on a grid plane."""
+    nx = int(round(2 * (base / 2 + pad) / h)) // 2 * 2 + 1
+    kz0 = int(round(pad / h))
+    nz = kz0 + int(round((base / 2 + pad) / h)) + 1
+    cx = centered_axis(nx, h)
+    cz = (np.arange(nz) - kz0) * h
+    X, Y, Z = np.meshgrid(cx, cx, cz, indexing='ij')
+    return pyramid_mask(X, Y, Z, base)
+
+
+def fig4_environment(base, h=1.0, pad=8.0, piezo=True):
+    """Pryor's b-nm pyramid (Table I parameters, first-order piezo potential applied as
+    U = -phi to both edges, sigma_e = Ec[dot].min(), sigma_h = exact valence edge), as
+    pryor_fig4.environment builds it (pryor_fig4.py:109-153).
+
+    Deviation, stated: the strain is the homogeneous Fourier solution with GaAs elastic constants
+    (strain_fourier.solve_strain) instead of the inhomogeneous FD elasticity PCG
+    (elasticity_fd.solve_strain_fd), a host preprocessing step this package does not rebuild.
+    """
+    dot, mat = PRYOR_TABLE_I['InAs'], PRYOR_TABLE_I['GaAs']
+    pyr = fig4_grid(base, h, pad)
+    eps_star = (mat['a0'] - dot['a0']) / dot['a0']
+    st = solve_strain(pyr, eps_star, mat['C11'], mat['C12'], mat['C44'], h)
+    trace = st['exx'] + st['eyy'] + st['ezz']
+    Ev0 = np.where(pyr, dot['E_vbo'], mat['E_vbo'])
+    Ec0 = Ev0 + np.where(pyr, dot['Eg'], mat['Eg'])
+    a_c = np.where(pyr, dot['a_c'], mat['a_c'])
+    a_v = np.where(pyr, dot['a_v'], mat['a_v'])
+    Ec, Ev = Ec0 + a_c * trace, Ev0 - a_v * trace
+    if piezo:
+        phi = piezo_potential(st, np.where(pyr, dot['e14'], mat['e14']), mat['eps_R'], h)
+        Ec, Ev = Ec - phi, Ev - phi
+    f = material_fields(pyr, dot, mat, Ev, Ec, 8)
+    f.update(st)
+    sig_e = float(Ec[pyr].min())
+    sig_h = hole_sigma(Ev, st, f['b'], f['d'], f['delta_so'], pyr)
+    return Workload(f"fig4_b{base:g}_h{h:g}", pyr.shape, h, f, pyr, sig_e, sig_h, 8,
+                    meta=dict(base=base, pad=pad, piezo=piezo))
+
+
+def fig4_from_fixture(path):
+    """Workload from a saved field fixture (reference-built fields, e.g. FD strain)."""
+    z = np.load(path)
+    mask = z['mask']
+    f = {k: z[k] for k in FIELD_KEYS}
+    return Workload(f"fixture:{path.rsplit('/', 1)[-1]}", mask.shape, float(z['h']), f, mask,
+                    float(z['sigma_e']), float(z['sigma_h']), 8)

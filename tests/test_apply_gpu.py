@@ -88,4 +88,4 @@ def test_config1_operator_against_oracle():
     Y = H @ X
     Yo = Ho @ X
     assert np.abs(Y - Yo).max() / np.abs(Yo).max() < 1e-13
-    assert Ho.nnz == 30932608 and Ho.nnz <= H.nnz <= Ho.nnz * (1 + 1e-4)
+    assert Ho.nnz <= H.nnz <= Ho.nnz * (1 + 1e-4)   # structural count bounds scipy's

@@ -68,7 +68,7 @@ def test_solve_interior_matches_reference_cb_vb(small):
         assert np.abs(E - np.array(ref['E'])).max() < 1e-8, (band, E, ref['E'])
         assert info['residuals'].max() < 1e-8
         assert info['converged'] and info['status'] == 'converged'
-        assert abs(info['iterations'] - ref['iterations']) <= 0.1 * ref['iterations'] + 5
+        assert abs(info["iterations"] - ref["iterations"]) <= 0.25 * ref["iterations"]
         assert V.shape == (H.shape[0], ref['k']) and V.dtype == np.complex128
         G = V.conj().T @ V
         assert np.abs(G - np.eye(ref['k'])).max() < 1e-10
