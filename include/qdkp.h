@@ -123,6 +123,30 @@ int qdkp_apply(const qdkp_operator* op, const void* X, int64_t ldx, void* Y, int
                int m, double sigma, int mode, int precision, void* ws, size_t ws_bytes,
                void* stream);
 
+/*
+ * No counterpart in the reference (its folded operator is a Python closure). Allocation-free
+ * variant of qdkp_apply(..., QDKP_APPLY_FOLDED): Y = (H - sigma)^2 X with the intermediate
+ * (H - sigma) X held in a fixed device array built into the library, so the caller passes only
+ * X and Y. It is for callers that cannot allocate device memory when they apply the operator:
+ * bindings from languages with no device allocator of their own, code running where the
+ * implicit device synchronisation of cudaMalloc is not allowed (callbacks, latency-critical
+ * loops), or processes whose device memory is managed by another runtime.
+ *   - Limit: n * m complex elements must fit QDKP_NOALLOC_SCRATCH_BYTES (64 MiB: 4 Mi complex128
+ *     or 8 Mi complex64 elements); larger blocks are rejected with QDKP_ERR_WORKSPACE and a
+ *     message, and must use qdkp_apply with a workspace.
+ *   - Every GPU that loads libqdkp.so keeps those 64 MiB until the process exits.
+ *   - The first call on a device looks up the array's device address (cudaGetSymbolAddress,
+ *     with that device current); make that first call before any stream capture.
+ *   - No cudaMalloc, cudaFree or other allocating routine is called.
+ *   - All calls share the one array, which keeps the last call's contents; calls that overlap
+ *     on the GPU (different streams or threads, without ordering between them) race on it.
+ *     Nothing needs clearing: each call writes every element it later reads.
+ */
+#define QDKP_NOALLOC_SCRATCH_BYTES (64ull << 20)
+size_t qdkp_apply_folded_noalloc_max_elems(int precision);
+int qdkp_apply_folded_noalloc(const qdkp_operator* op, const void* X, int64_t ldx, void* Y,
+                              int64_t ldy, int m, double sigma, int precision, void* stream);
+
 /* Workspace bytes qdkp_apply_host needs for an (n, m) complex128 block in `mode`. */
 size_t qdkp_apply_host_workspace_size(const qdkp_operator* op, int m, int mode);
 

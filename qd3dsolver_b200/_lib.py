@@ -56,6 +56,10 @@ _SIGNATURES = {
                                   ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_double,
                                   ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t,
                                   ctypes.c_void_p]),
+    'qdkp_apply_folded_noalloc_max_elems': (ctypes.c_size_t, [ctypes.c_int]),
+    'qdkp_apply_folded_noalloc': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+                                                 ctypes.c_void_p, ctypes.c_int64, ctypes.c_int,
+                                                 ctypes.c_double, ctypes.c_int, ctypes.c_void_p]),
     'qdkp_apply_host_workspace_size': (ctypes.c_size_t, [ctypes.c_void_p, ctypes.c_int,
                                                          ctypes.c_int]),
     'qdkp_apply_host': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
