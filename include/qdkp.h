@@ -208,6 +208,32 @@ int qdkp_lobpcg_solve(const qdkp_operator* op, const qdkp_lobpcg_params* prm, co
                       void* ws, size_t ws_bytes, void* stream);
 
 /*
+ * Batched LOBPCG engine (no counterpart in the reference, which solves one operator at a time):
+ * many folded or plain eight-band solves resident on the GPU, advanced together one LOBPCG
+ * iteration (the same scipy iteration as qdkp_lobpcg_solve) per tick, with every decision taken
+ * on the device. Slots are admitted and retired between steps; each slot's workspace
+ * (qdkp_engine_slot_workspace_size bytes) belongs to the caller and must stay alive until the
+ * slot is retired. A solve gives the same result alone and in any mix.
+ */
+typedef struct qdkp_engine qdkp_engine;
+int qdkp_engine_create(int max_slots, int device, qdkp_engine** out);
+int qdkp_engine_destroy(qdkp_engine* e);
+size_t qdkp_engine_slot_workspace_size(const qdkp_operator* op, const qdkp_lobpcg_params* prm);
+/* Admit one solve: orthonormalises X0 (device, n x block complex128) and runs the initial
+ * Rayleigh-Ritz step (synchronous on `stream`). *slot receives the slot id. */
+int qdkp_engine_admit(qdkp_engine* e, const qdkp_operator* op, const qdkp_lobpcg_params* prm,
+                      const void* X0, void* ws, size_t ws_bytes, void* stream, int* slot);
+/* Launch `ticks` iterations of every running slot (asynchronous on `stream`). */
+int qdkp_engine_step(qdkp_engine* e, int ticks, void* stream);
+/* state[max_slots]: -1 free, 1 running, 0 stopped (status[] gives QDKP_LOBPCG_*);
+ * iterations[] = iterations started so far. Synchronous. */
+int qdkp_engine_poll(qdkp_engine* e, int* state, int* status, int* iterations, void* stream);
+/* Final Rayleigh-Ritz on the slot's best iterate (lobpcg.py:1009-1060): lambda[block] (host),
+ * V (device, n x block complex128), residuals[block] (host, may be NULL); frees the slot. */
+int qdkp_engine_retire(qdkp_engine* e, int slot, double* lambda, void* V, double* residuals,
+                       qdkp_lobpcg_info* info, void* stream);
+
+/*
  * Rayleigh quotients and residual norms of H for the columns of V (device, n x k complex128,
  * leading dimension ldv): rq[j] = v^H H v / v^H v and res[j] = ||H v_j - E_j v_j|| on the
  * normalised v_j, with E = E_in if non-NULL else rq (eigensolvers.residual_norms /

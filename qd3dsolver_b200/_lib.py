@@ -71,6 +71,21 @@ _SIGNATURES = {
                                          ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                          ctypes.c_void_p, ctypes.POINTER(LobpcgInfo),
                                          ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]),
+    'qdkp_engine_create': (ctypes.c_int, [ctypes.c_int, ctypes.c_int,
+                                          ctypes.POINTER(ctypes.c_void_p)]),
+    'qdkp_engine_destroy': (ctypes.c_int, [ctypes.c_void_p]),
+    'qdkp_engine_slot_workspace_size': (ctypes.c_size_t, [ctypes.c_void_p,
+                                                          ctypes.POINTER(LobpcgParams)]),
+    'qdkp_engine_admit': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p,
+                                         ctypes.POINTER(LobpcgParams), ctypes.c_void_p,
+                                         ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p,
+                                         ctypes.POINTER(ctypes.c_int)]),
+    'qdkp_engine_step': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
+    'qdkp_engine_poll': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                        ctypes.c_void_p, ctypes.c_void_p]),
+    'qdkp_engine_retire': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                          ctypes.c_void_p, ctypes.c_void_p,
+                                          ctypes.POINTER(LobpcgInfo), ctypes.c_void_p]),
     'qdkp_residuals_workspace_size': (ctypes.c_size_t, [ctypes.c_void_p, ctypes.c_int]),
     'qdkp_residuals': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
                                       ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,

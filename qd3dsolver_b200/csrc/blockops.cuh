@@ -12,6 +12,12 @@ constexpr int kMaxBlock = 24;          // largest LOBPCG block width (columns) s
 constexpr int kMaxSmall = 3 * kMaxBlock;  // largest Rayleigh-Ritz dimension
 constexpr int kTallThreads = 256;
 constexpr int kSmallThreads = 512;
+// Gram kernels: 3 x 3 warps, each owning up to kGramMaxT x kGramMaxT 8x8 tiles of the real
+// product, rows staged kGramChunk at a time.
+constexpr int kGramWarpsR = 3, kGramWarpsC = 3;
+constexpr int kGramThreads = 32 * kGramWarpsR * kGramWarpsC;
+constexpr int kGramMaxT = 6;                        // tiles per warp per dimension
+constexpr int kGramChunk = 32;                      // rows staged per step
 
 // A group of up to three column blocks concatenated along the columns: [B0 | B1 | B2].
 template <typename T>

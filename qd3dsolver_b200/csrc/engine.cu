@@ -1,0 +1,943 @@
+// Batched LOBPCG engine (the served form): many solves resident on the device at once, each in
+// a slot, advanced together one LOBPCG iteration per tick. The iteration is scipy's
+// (lobpcg.py:688-973, B = M = Y = None, largest = False) exactly as the single-solve driver in
+// lobpcg.cu runs it; the difference is that every decision is taken on the device, so a tick is
+// a fixed launch sequence over all slots and the host only polls between ticks.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <vector>
+
+#include "engine_dev.cuh"
+
+namespace qdkp {
+
+int launch_apply(const qdkp_operator* op, const void* X, int64_t ldx, void* Y, int64_t ldy,
+                 int m, double sigma, int shifted, int precision, cudaStream_t st);
+
+constexpr int kERowsPerCta = 2048;   // rows per CTA of the row kernels
+constexpr int kENormRows = 2048;     // rows per CTA of the norm kernel
+constexpr int kEGramSplit = 16;
+
+enum GramWhich { GR_XR = 0, GR_RR, GR_PP, GR_WW, GR_WAW };
+enum UpdWhich { UP_RPROJ = 0, UP_RNORM, UP_PNORM, UP_APNORM, UP_PNEW, UP_APNEW, UP_XNEW, UP_AXNEW };
+enum RowWhich { RW_COPYBEST = 0, RW_RESID, RW_GATHERP };
+
+// ---------------------------------------------------------------------------------------------
+// residual norms of A X - X lambda: partials per CTA, reduced in the decision kernel
+// ---------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(kTallThreads)
+e_norm_kernel(const ESlot* __restrict__ S, int ns) {
+  const int k = slot_of(S, ns, blockIdx.x, &ESlot::norm0);
+  const ESlot& d = S[k];
+  const EState* st = d.st;
+  if (!st->running) return;
+  const int part = blockIdx.x - d.norm0;
+  const int m = d.m;
+  const long long r0 = (long long)part * kENormRows;
+  const long long r1 = min(d.n, r0 + kENormRows);
+  double acc[kMaxBlock];
+#pragma unroll
+  for (int j = 0; j < kMaxBlock; ++j) acc[j] = 0.0;
+  for (long long r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
+#pragma unroll
+    for (int j = 0; j < kMaxBlock; ++j) {
+      if (j < m) {
+        const double2 a = d.AX[r * m + j], x = d.X[r * m + j];
+        const double l = st->lam[j];
+        const double re = a.x - l * x.x, im = a.y - l * x.y;
+        acc[j] = fma(re, re, fma(im, im, acc[j]));
+      }
+    }
+  }
+  __shared__ double red[kTallThreads / 32][kMaxBlock];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int j = 0; j < kMaxBlock; ++j) {
+    if (j < m) {
+      double v = acc[j];
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if (lane == 0) red[warp][j] = v;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < m) {
+    double s = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w][threadIdx.x];
+    d.npart[(long long)part * m + threadIdx.x] = s;
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// per-slot decisions at the top of an iteration (lobpcg.py:688-760)
+// ---------------------------------------------------------------------------------------------
+__global__ void e_decide_kernel(const ESlot* __restrict__ S) {
+  const ESlot& d = S[blockIdx.x];
+  EState* st = d.st;
+  __shared__ double nrm[kMaxBlock];
+  const int m = d.m;
+  if (threadIdx.x < m) {
+    double s = 0.0;
+    for (int b = 0; b < d.nparts; ++b) s += d.npart[(long long)b * m + threadIdx.x];
+    nrm[threadIdx.x] = sqrt(fabs(s));
+  }
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  st->idle = 1; st->copy_best = 0; st->skip_recompute = 1; st->skip_p = 1; st->skip_pnorm = 1;
+  if (!st->running) return;
+  if (st->iter >= d.maxiter) { st->running = 0; st->status = QDKP_LOBPCG_MAXITER; return; }
+  st->iter += 1;
+  double mean = 0.0, mx = 0.0;
+  bool finite = true;
+  for (int j = 0; j < m; ++j) {
+    st->norms[j] = nrm[j];
+    mean += nrm[j];
+    mx = fmax(mx, nrm[j]);
+    finite = finite && isfinite(nrm[j]);
+  }
+  mean /= m;
+  if (!finite) { st->running = 0; st->status = QDKP_LOBPCG_NONFINITE; return; }
+  if (mean < st->smallest) {
+    st->smallest = mean;
+    st->best_iter = st->iter;
+    st->copy_best = 1;
+  } else if (mean > ldexp(1.0, d.restart_control) * st->smallest) {
+    st->forced = 1;
+    st->skip_recompute = 0;
+  }
+  int ma = 0;
+  for (int j = 0; j < m; ++j) {
+    st->active[j] = st->active[j] && (nrm[j] > d.tol);
+    if (st->active[j]) st->idx[ma++] = j;
+  }
+  st->ma = ma;
+  if (ma == 0) { st->running = 0; st->status = QDKP_LOBPCG_CONVERGED; return; }
+  const double myeps = 1.4901161193847656e-08;   // sqrt(eps) for complex128
+  st->explicit_gram = !(mx > myeps && !st->explicit_gram);
+  st->idle = 0;
+  st->skip_p = st->iter == 0 ? 1 : 0;
+}
+
+// ---------------------------------------------------------------------------------------------
+// row kernels: copy of the best iterate, residual gather, P gather
+// ---------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(kTallThreads)
+e_row_kernel(const ESlot* __restrict__ S, int ns, int which) {
+  const int k = slot_of(S, ns, blockIdx.x, &ESlot::row0);
+  const ESlot& d = S[k];
+  const EState* st = d.st;
+  const int m = d.m;
+  if (which == RW_COPYBEST) { if (!st->copy_best) return; }
+  else if (st->idle || (which == RW_GATHERP && st->skip_p)) return;
+  const long long r0 = (long long)(blockIdx.x - d.row0) * d.rows_per_cta;
+  const long long r1 = min(d.n, r0 + d.rows_per_cta);
+  const int ma = st->ma;
+  if (which == RW_COPYBEST) {
+    for (long long e = r0 * m + threadIdx.x; e < r1 * m; e += blockDim.x) d.best[e] = d.X[e];
+  } else if (which == RW_RESID) {
+    for (long long e = r0 * ma + threadIdx.x; e < r1 * ma; e += blockDim.x) {
+      const long long r = e / ma;
+      const int c = (int)(e - r * ma);
+      const int j = st->idx[c];
+      const double l = st->lam[j];
+      const double2 a = d.AX[r * m + j], x = d.X[r * m + j];
+      d.Ra[e] = make_double2(a.x - l * x.x, a.y - l * x.y);
+    }
+  } else {
+    for (long long e = r0 * ma + threadIdx.x; e < r1 * ma; e += blockDim.x) {
+      const long long r = e / ma;
+      const int c = (int)(e - r * ma);
+      const int j = st->idx[c];
+      d.Pa[e] = d.P[r * m + j];
+      d.APa[e] = d.AP[r * m + j];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Gram products, multi-slot (same FP64 MMA scheme as gram_partial_kernel)
+// ---------------------------------------------------------------------------------------------
+__device__ bool gram_lists(const ESlot& d, int which, BlockList<double>& A, BlockList<double>& B,
+                           double2*& out) {
+  const EState* st = d.st;
+  if (st->idle) return false;
+  const int m = d.m, ma = st->ma, mp = st->mp;
+  auto set1 = [](BlockList<double>& L, const double2* p, int c) {
+    L.nblk = 1; L.p[0] = p; L.ld[0] = c; L.cols[0] = c;
+  };
+  switch (which) {
+    case GR_XR: set1(A, d.X, m); set1(B, d.Ra, ma); out = d.W; return true;
+    case GR_RR: set1(A, d.Ra, ma); set1(B, d.Ra, ma); out = d.G; return true;
+    case GR_PP:
+      if (st->skip_p) return false;
+      set1(A, d.Pa, ma); set1(B, d.Pa, ma); out = d.G; return true;
+    default: {
+      A.nblk = mp ? 3 : 2;
+      A.p[0] = d.X; A.ld[0] = m; A.cols[0] = m;
+      A.p[1] = d.Ra; A.ld[1] = ma; A.cols[1] = ma;
+      A.p[2] = d.Pa; A.ld[2] = ma; A.cols[2] = mp;
+      if (which == GR_WW) { B = A; out = d.gS; return true; }
+      B.nblk = A.nblk;
+      B.p[0] = d.AX; B.ld[0] = m; B.cols[0] = m;
+      B.p[1] = d.ARa; B.ld[1] = ma; B.cols[1] = ma;
+      B.p[2] = d.APa; B.ld[2] = ma; B.cols[2] = mp;
+      out = d.gT;
+      return true;
+    }
+  }
+}
+
+template <int MAXT>
+__global__ void __launch_bounds__(kGramThreads)
+e_gram_kernel(const ESlot* __restrict__ S, int ns, int which) {
+  extern __shared__ double gsm_e[];
+  const int k = slot_of(S, ns, blockIdx.x, &ESlot::gram0);
+  const ESlot& d = S[k];
+  BlockList<double> A, B;
+  double2* out;
+  if (!gram_lists(d, which, A, B, out)) return;
+  const int part = blockIdx.x - d.gram0;
+  const int P = A.total(), Q = B.total();
+  const int RP = (2 * P + 7) / 8 * 8, RQ = (2 * Q + 7) / 8 * 8;
+  double* sA = gsm_e;
+  double* sB = gsm_e + kGramChunk * RP;
+  const long long r0 = (long long)part * d.rows_per_gpart;
+  const long long r1 = min(d.n, r0 + d.rows_per_gpart);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = lane >> 2, t4 = lane & 3;
+  const int TR = RP / 8, TC = RQ / 8;
+  const int wr = warp / kGramWarpsC, wc = warp % kGramWarpsC;
+  const int tr_per = (TR + kGramWarpsR - 1) / kGramWarpsR, tc_per = (TC + kGramWarpsC - 1) / kGramWarpsC;
+  const int tr0 = wr * tr_per, tc0 = wc * tc_per;
+  double acc[MAXT][MAXT][2];
+#pragma unroll
+  for (int i = 0; i < MAXT; ++i)
+#pragma unroll
+    for (int j = 0; j < MAXT; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+  for (long long rt = r0; rt < r1; rt += kGramChunk) {
+    for (int e = threadIdx.x; e < kGramChunk * (RP / 2); e += blockDim.x) {
+      const int row = e / (RP / 2), c = e - row * (RP / 2);
+      double2 z = make_double2(0.0, 0.0);
+      if (rt + row < r1 && c < P) z = list_elem(A, rt + row, c);
+      *reinterpret_cast<double2*>(&sA[row * RP + 2 * c]) = z;
+    }
+    for (int e = threadIdx.x; e < kGramChunk * (RQ / 2); e += blockDim.x) {
+      const int row = e / (RQ / 2), c = e - row * (RQ / 2);
+      double2 z = make_double2(0.0, 0.0);
+      if (rt + row < r1 && c < Q) z = list_elem(B, rt + row, c);
+      *reinterpret_cast<double2*>(&sB[row * RQ + 2 * c]) = z;
+    }
+    __syncthreads();
+#pragma unroll 2
+    for (int k0 = 0; k0 < kGramChunk; k0 += 4) {
+      double a[MAXT], b[MAXT];
+#pragma unroll
+      for (int i = 0; i < MAXT; ++i) {
+        const int ti = tr0 + i;
+        a[i] = (i < tr_per && ti < TR) ? sA[(k0 + t4) * RP + ti * 8 + g] : 0.0;
+      }
+#pragma unroll
+      for (int j = 0; j < MAXT; ++j) {
+        const int tj = tc0 + j;
+        b[j] = (j < tc_per && tj < TC) ? sB[(k0 + t4) * RQ + tj * 8 + g] : 0.0;
+      }
+#pragma unroll
+      for (int i = 0; i < MAXT; ++i)
+#pragma unroll
+        for (int j = 0; j < MAXT; ++j)
+          if (i < tr_per && j < tc_per) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+    }
+    __syncthreads();
+  }
+  double* outp = d.gpart + (long long)part * RP * RQ;
+#pragma unroll
+  for (int i = 0; i < MAXT; ++i)
+#pragma unroll
+    for (int j = 0; j < MAXT; ++j) {
+      const int ti = tr0 + i, tj = tc0 + j;
+      if (i < tr_per && j < tc_per && ti < TR && tj < TC) {
+        const int row = ti * 8 + g, col = tj * 8 + 2 * t4;
+        outp[(long long)row * RQ + col] = acc[i][j][0];
+        outp[(long long)row * RQ + col + 1] = acc[i][j][1];
+      }
+    }
+}
+
+__global__ void e_gram_reduce1(const ESlot* __restrict__ S, int which) {
+  const ESlot& d = S[blockIdx.z];
+  BlockList<double> A, B;
+  double2* out;
+  if (!gram_lists(d, which, A, B, out)) return;
+  const int P = A.total(), Q = B.total();
+  const int RP = (2 * P + 7) / 8 * 8, RQ = (2 * Q + 7) / 8 * 8;
+  const int elems = RP * RQ;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= elems) return;
+  const int per = (d.gparts + kEGramSplit - 1) / kEGramSplit;
+  const int b0 = blockIdx.y * per, b1 = min(d.gparts, b0 + per);
+  double s = 0.0;
+  for (int b = b0; b < b1; ++b) s += d.gpart[(long long)b * elems + e];
+  d.gpart[(long long)(d.gparts + blockIdx.y) * elems + e] = s;
+}
+
+__global__ void e_gram_reduce2(const ESlot* __restrict__ S, int which) {
+  const ESlot& d = S[blockIdx.y];
+  BlockList<double> A, B;
+  double2* out;
+  if (!gram_lists(d, which, A, B, out)) return;
+  const int P = A.total(), Q = B.total();
+  const int RP = (2 * P + 7) / 8 * 8, RQ = (2 * Q + 7) / 8 * 8;
+  const int elems = RP * RQ;
+  const int o = blockIdx.x * blockDim.x + threadIdx.x;
+  if (o >= P * Q) return;
+  const int i = o / Q, j = o - i * Q;
+  const long long rr = (long long)(2 * i) * RQ + 2 * j;
+  double re = 0.0, im = 0.0;
+  for (int sp = 0; sp < kEGramSplit; ++sp) {
+    const double* c = d.gpart + (long long)(d.gparts + sp) * elems;
+    re += c[rr] + c[rr + RQ + 1];
+    im += c[rr + 1] - c[rr + RQ];
+  }
+  out[o] = make_double2(re, im);
+}
+
+// ---------------------------------------------------------------------------------------------
+// block updates, multi-slot (FP64 MMA, rows staged through shared memory: in-place safe)
+// ---------------------------------------------------------------------------------------------
+__device__ bool upd_lists(const ESlot& d, int which, BlockList<double>& A, const double2* C[3],
+                          int& q, double2*& Y, int& accumulate, int& neg) {
+  const EState* st = d.st;
+  if (st->idle) return false;
+  const int m = d.m, ma = st->ma, mp = st->mp;
+  accumulate = 0; neg = 0;
+  auto set = [&](int i, const double2* p, int ld, int c, const double2* cf) {
+    A.p[i] = p; A.ld[i] = ld; A.cols[i] = c; C[i] = cf;
+  };
+  switch (which) {
+    case UP_RPROJ: A.nblk = 1; set(0, d.X, m, m, d.W); q = ma; Y = d.Ra; accumulate = 1; neg = 1; return true;
+    case UP_RNORM: A.nblk = 1; set(0, d.Ra, ma, ma, d.U); q = ma; Y = d.Ra; return true;
+    case UP_PNORM:
+      if (st->skip_pnorm) return false;
+      A.nblk = 1; set(0, d.Pa, ma, ma, d.U); q = ma; Y = d.Pa; return true;
+    case UP_APNORM:
+      if (st->skip_pnorm) return false;
+      A.nblk = 1; set(0, d.APa, ma, ma, d.U); q = ma; Y = d.APa; return true;
+    case UP_PNEW:
+      A.nblk = mp ? 2 : 1; set(0, d.Ra, ma, ma, d.Cr); set(1, d.Pa, ma, mp, d.Cp);
+      q = m; Y = d.P; return true;
+    case UP_APNEW:
+      A.nblk = mp ? 2 : 1; set(0, d.ARa, ma, ma, d.Cr); set(1, d.APa, ma, mp, d.Cp);
+      q = m; Y = d.AP; return true;
+    case UP_XNEW:
+      A.nblk = 2; set(0, d.X, m, m, d.Cx); set(1, d.P, m, m, d.Im); q = m; Y = d.X; return true;
+    default:
+      A.nblk = 2; set(0, d.AX, m, m, d.Cx); set(1, d.AP, m, m, d.Im); q = m; Y = d.AX; return true;
+  }
+}
+
+__global__ void __launch_bounds__(kUpdThreads)
+e_update_kernel(const ESlot* __restrict__ S, int ns, int which) {
+  extern __shared__ double usm_e[];
+  const int k = slot_of(S, ns, blockIdx.x, &ESlot::row0);
+  const ESlot& d = S[k];
+  BlockList<double> A;
+  const double2* Cf[3];
+  int q, accumulate, neg;
+  double2* Y;
+  if (!upd_lists(d, which, A, Cf, q, Y, accumulate, neg)) return;
+  const long long r0 = (long long)(blockIdx.x - d.row0) * d.rows_per_cta;
+  const long long r1 = min(d.n, r0 + d.rows_per_cta);
+  update_rows(A, Cf, q, r0, r1, Y, (long long)q, accumulate, neg, usm_e);
+}
+
+// ---------------------------------------------------------------------------------------------
+// per-slot Cholesky steps and Rayleigh-Ritz
+// ---------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(kSmallThreads) e_rchol_kernel(const ESlot* __restrict__ S) {
+  extern __shared__ double2 ssm_e[];
+  const ESlot& d = S[blockIdx.x];
+  EState* st = d.st;
+  if (st->idle) return;
+  const int n = st->ma;
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) ssm_e[e] = d.G[e];
+  __syncthreads();
+  const int fail = block_cholesky_upper(ssm_e, n);
+  if (fail) {
+    if (threadIdx.x == 0) { st->running = 0; st->status = QDKP_LOBPCG_RCHOL_BREAKDOWN; st->idle = 1; }
+    return;
+  }
+  block_upper_inverse(ssm_e, n, ssm_e + n * n);
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) d.U[e] = ssm_e[n * n + e];
+}
+
+__global__ void __launch_bounds__(kSmallThreads) e_pchol_kernel(const ESlot* __restrict__ S) {
+  extern __shared__ double2 ssm_e[];
+  const ESlot& d = S[blockIdx.x];
+  EState* st = d.st;
+  if (st->idle) return;
+  const int n = st->ma;
+  if (st->skip_p) {                        // iteration 0: no P yet, restart stays as it is
+    if (threadIdx.x == 0) { st->skip_pnorm = 1; st->mp = st->restart ? 0 : n; }
+    return;
+  }
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) ssm_e[e] = d.G[e];
+  __syncthreads();
+  const int fail = block_cholesky_upper(ssm_e, n);
+  if (!fail) {
+    block_upper_inverse(ssm_e, n, ssm_e + n * n);
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) d.U[e] = ssm_e[n * n + e];
+  }
+  if (threadIdx.x == 0) {
+    st->skip_pnorm = fail ? 1 : 0;
+    st->restart = fail ? 1 : st->forced;
+    st->mp = st->restart ? 0 : n;
+  }
+}
+
+// gramA / gramB of lobpcg.py:826-909 from S = W^H W and T = W^H AW, then the generalized eigh,
+// with the fall back to the two-block pencil when the three-block one is not definite.
+__device__ void e_assemble(const ESlot& d, const EState* st, int restart, int& dim) {
+  const int m = d.m, ma = st->ma, mp = restart ? 0 : st->mp;
+  const int tot = m + st->ma + st->mp;      // layout of gS / gT
+  dim = m + ma + mp;
+  const bool ex = st->explicit_gram;
+  for (int e = threadIdx.x; e < dim * dim; e += blockDim.x) {
+    int i = e / dim, j = e - i * dim;
+    bool lower = i > j;
+    if (lower) { const int t = i; i = j; j = t; }
+    const bool iX = i < m, iR = i >= m && i < m + ma, jX = j < m, jR = j >= m && j < m + ma;
+    const double2 Tij = d.gT[i * tot + j], Tji = d.gT[j * tot + i], Sij = d.gS[i * tot + j];
+    const double2 herm = make_double2(0.5 * (Tij.x + Tji.x), 0.5 * (Tij.y - Tji.y));
+    double2 a, b;
+    if (iX && jX) {
+      if (ex) { a = herm; b = Sij; }
+      else { a = make_double2(i == j ? st->lam[i] : 0.0, 0.0); b = make_double2(i == j ? 1.0 : 0.0, 0.0); }
+    } else if (iX && jR) {
+      a = Tij; b = ex ? Sij : make_double2(0.0, 0.0);
+    } else if ((iR && jR) || (!iX && !iR && !jX && !jR)) {
+      a = ex ? herm : Tij;
+      b = ex ? Sij : make_double2(i == j ? 1.0 : 0.0, 0.0);
+    } else {
+      a = Tij; b = Sij;
+    }
+    if (lower) { a.y = -a.y; b.y = -b.y; }
+    d.gA[e] = a;
+    d.gB[e] = b;
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(kSmallThreads) e_rr_kernel(const ESlot* __restrict__ S) {
+  extern __shared__ double2 rsm[];
+  const ESlot& d = S[blockIdx.x];
+  EState* st = d.st;
+  if (st->idle) return;
+  __shared__ int use_restart, ok, dim_s;
+  if (threadIdx.x == 0) { use_restart = st->mp == 0; ok = 0; }
+  __syncthreads();
+  for (int attempt = 0; attempt < 2; ++attempt) {
+    int dim;
+    e_assemble(d, st, use_restart, dim);
+    const int r = block_eigh(d.gA, d.gB, dim, d.w, d.E, d.scr, rsm, rsm + dim * dim);
+    if (threadIdx.x == 0) { ok = r == 0; dim_s = dim; }
+    __syncthreads();
+    if (ok || use_restart) break;
+    if (threadIdx.x == 0) use_restart = 1;    // drop P and retry (lobpcg.py:891-909)
+    __syncthreads();
+  }
+  if (!ok) {
+    if (threadIdx.x == 0) { st->running = 0; st->status = QDKP_LOBPCG_EIGH_BREAKDOWN; st->idle = 1; }
+    return;
+  }
+  const int m = d.m, ma = st->ma, dim = dim_s;
+  const int mp = dim - m - ma;
+  for (int e = threadIdx.x; e < dim * m; e += blockDim.x) {
+    const int i = e / m, j = e - i * m;
+    const double2 v = d.E[i * dim + j];
+    if (i < m) d.Cx[i * m + j] = v;
+    else if (i < m + ma) d.Cr[(i - m) * m + j] = v;
+    else d.Cp[(i - m - ma) * m + j] = v;
+  }
+  if (threadIdx.x < m) st->lam[threadIdx.x] = d.w[threadIdx.x];
+  if (threadIdx.x == 0) { st->restart = use_restart ? 1 : st->restart; st->mp = mp; }
+}
+
+}  // namespace qdkp
+
+// =============================================================================================
+// host side
+// =============================================================================================
+namespace qdkp {
+namespace {
+
+struct SlotHost {
+  bool used = false;
+  const qdkp_operator* op = nullptr;
+  qdkp_lobpcg_params prm{};
+  ESlot d{};
+  size_t gpart_doubles = 0;
+  int64_t applies = 0;
+};
+
+size_t align256(size_t b) { return (b + 255) / 256 * 256; }
+
+struct SlotLayout {
+  size_t blk, small, npart, gpart, total;
+  int nparts, gparts;
+  long long rows_per_gpart;
+};
+
+SlotLayout slot_layout(int64_t n, int m) {
+  SlotLayout L;
+  L.blk = align256((size_t)n * m * sizeof(double2));
+  L.small = align256((size_t)(3 * m) * (3 * m) * sizeof(double2));
+  L.nparts = (int)((n + kENormRows - 1) / kENormRows);
+  L.npart = align256((size_t)L.nparts * m * sizeof(double));
+  long long parts = (n + 255) / 256;
+  if (parts > 296) parts = 296;
+  if (parts < 1) parts = 1;
+  long long rpp = (n + parts - 1) / parts;
+  rpp = (rpp + kGramChunk - 1) / kGramChunk * kGramChunk;
+  L.gparts = (int)((n + rpp - 1) / rpp);
+  L.rows_per_gpart = rpp;
+  const size_t RP = (6 * m + 7) / 8 * 8;
+  L.gpart = align256((size_t)(L.gparts + kEGramSplit) * RP * RP * sizeof(double));
+  L.total = align256(sizeof(EState)) + 10 * L.blk + 14 * L.small +
+            align256(3 * m * sizeof(double)) + L.npart + L.gpart;
+  return L;
+}
+
+}  // namespace
+}  // namespace qdkp
+
+struct qdkp_engine {
+  int device = 0;
+  int max_slots = 0;
+  std::vector<qdkp::SlotHost> slots;
+  qdkp::ESlot* d_slots = nullptr;      // compact array of the used slots
+  qdkp::HXSlot* d_hx = nullptr;        // 4 x max_slots H.X descriptors
+  int* d_one = nullptr;                // constant 1 (skip flag)
+  std::vector<int> order;              // slot ids in compact order
+  int ns = 0, norm_ctas = 0, gram_ctas = 0, row_ctas = 0, hx_tiles = 0, S_max = 32;
+  int maxT = 2, m_max = 1;
+  bool dirty = true;
+};
+
+namespace qdkp {
+namespace {
+
+int apply_folded(const SlotHost& h, const double2* V, int c, double2* out, cudaStream_t st) {
+  const ESlot& d = h.d;
+  if (h.prm.folded) {
+    int rc = launch_apply(h.op, V, c, d.T, c, c, h.prm.sigma, 1, QDKP_C128, st);
+    if (rc) return rc;
+    return launch_apply(h.op, d.T, c, out, c, c, h.prm.sigma, 1, QDKP_C128, st);
+  }
+  return launch_apply(h.op, V, c, out, c, c, 0.0, 0, QDKP_C128, st);
+}
+
+BlockList<double> one(const double2* p, int c) {
+  BlockList<double> L;
+  L.nblk = 1; L.p[0] = p; L.ld[0] = c; L.cols[0] = c;
+  return L;
+}
+
+int gram1(const SlotHost& h, const double2* A, const double2* B, int m, double2* out,
+          cudaStream_t st) {
+  const size_t elems = h.gpart_doubles / 2;
+  return launch_gram(one(A, m), one(B, m), h.d.n, reinterpret_cast<double2*>(h.d.gpart), elems, out, st);
+}
+
+int read_sync(void* host, const void* dev, size_t bytes, cudaStream_t st) {
+  QDKP_CUDA_TRY(cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, st));
+  QDKP_CUDA_TRY(cudaStreamSynchronize(st));
+  return QDKP_OK;
+}
+
+int rebuild(qdkp_engine* e, cudaStream_t st) {
+  std::vector<ESlot> compact;
+  std::vector<HXSlot> hx(4 * (size_t)e->max_slots);
+  e->order.clear();
+  int norm0 = 0, gram0 = 0, row0 = 0, tile0 = 0, S_max = 32, m_max = 1;
+  for (int i = 0; i < e->max_slots; ++i) {
+    SlotHost& h = e->slots[i];
+    if (!h.used) continue;
+    ESlot d = h.d;
+    d.norm0 = norm0; norm0 += d.nparts;
+    d.gram0 = gram0; gram0 += d.gparts;
+    d.row0 = row0; row0 += (int)((d.n + d.rows_per_cta - 1) / d.rows_per_cta);
+    h.d = d;
+    const int k = (int)compact.size();
+    compact.push_back(d);
+    e->order.push_back(i);
+    const qdkp_operator* op = h.op;
+    const int S = apply_tile_sites(d.m);
+    S_max = std::max(S_max, S);
+    m_max = std::max(m_max, d.m);
+    const int tiles = (int)((op->n_sites + S - 1) / S);
+    const double sign = (op->flags & QDKP_NEGATE) ? -1.0 : 1.0;
+    for (int t = 0; t < 4; ++t) {
+      HXSlot x{};
+      x.F = op->fields64; x.N = op->n_sites;
+      x.nx = op->nx; x.ny = op->ny; x.nz = op->nz; x.flags = op->flags;
+      x.S = S; x.tile0 = tile0; x.h = op->h; x.sign = sign;
+      x.sigma = h.prm.sigma;
+      x.shifted = h.prm.folded ? 1 : 0;
+      const bool recompute = t < 2;
+      if (recompute) { x.m = d.m; x.m_dev = nullptr; x.ld_same = 0; x.ldx = d.m; x.ldy = d.m; }
+      else { x.m = 0; x.m_dev = &d.st->ma; x.ld_same = 1; }
+      const int* skipflag = recompute ? &d.st->skip_recompute : &d.st->idle;
+      if (h.prm.folded) {
+        x.X = (t == 0) ? (const void*)d.X : (t == 2) ? (const void*)d.Ra : (const void*)d.T;
+        x.Y = (t == 0 || t == 2) ? (void*)d.T : (t == 1) ? (void*)d.AX : (void*)d.ARa;
+        x.skip = skipflag;
+      } else {
+        x.X = recompute ? (const void*)d.X : (const void*)d.Ra;
+        x.Y = recompute ? (void*)d.AX : (void*)d.ARa;
+        x.skip = (t == 1 || t == 3) ? e->d_one : skipflag;
+      }
+      hx[(size_t)t * e->max_slots + k] = x;
+    }
+    tile0 += tiles;
+  }
+  e->ns = (int)compact.size();
+  e->norm_ctas = norm0; e->gram_ctas = gram0; e->row_ctas = row0; e->hx_tiles = tile0;
+  e->S_max = S_max; e->m_max = m_max;
+  const int RP = (6 * m_max + 7) / 8 * 8;
+  const int TR = RP / 8;
+  const int tper = (TR + kGramWarpsR - 1) / kGramWarpsR;
+  e->maxT = tper <= 2 ? 2 : tper <= 3 ? 3 : tper <= 4 ? 4 : 6;
+  if (e->ns) {
+    QDKP_CUDA_TRY(cudaMemcpyAsync(e->d_slots, compact.data(), compact.size() * sizeof(ESlot),
+                                  cudaMemcpyHostToDevice, st));
+    QDKP_CUDA_TRY(cudaMemcpyAsync(e->d_hx, hx.data(), hx.size() * sizeof(HXSlot),
+                                  cudaMemcpyHostToDevice, st));
+  }
+  e->dirty = false;
+  return QDKP_OK;
+}
+
+int launch_gram_multi(qdkp_engine* e, int which, cudaStream_t st) {
+  const int RP = (6 * e->m_max + 7) / 8 * 8;
+  const size_t smem = (size_t)kGramChunk * 2 * RP * sizeof(double);
+  switch (e->maxT) {
+    case 2: e_gram_kernel<2><<<e->gram_ctas, kGramThreads, smem, st>>>(e->d_slots, e->ns, which); break;
+    case 3: e_gram_kernel<3><<<e->gram_ctas, kGramThreads, smem, st>>>(e->d_slots, e->ns, which); break;
+    case 4: e_gram_kernel<4><<<e->gram_ctas, kGramThreads, smem, st>>>(e->d_slots, e->ns, which); break;
+    default: e_gram_kernel<6><<<e->gram_ctas, kGramThreads, smem, st>>>(e->d_slots, e->ns, which); break;
+  }
+  const int elems = RP * RP;
+  e_gram_reduce1<<<dim3((elems + 255) / 256, kEGramSplit, e->ns), 256, 0, st>>>(e->d_slots, which);
+  const int pq = (3 * e->m_max) * (3 * e->m_max);
+  e_gram_reduce2<<<dim3((pq + 127) / 128, e->ns), 128, 0, st>>>(e->d_slots, which);
+  count_launch(3);
+  QDKP_CUDA_TRY(cudaGetLastError());
+  return QDKP_OK;
+}
+
+int launch_update_multi(qdkp_engine* e, int which, cudaStream_t st) {
+  const int P = 2 * e->m_max;
+  const int KPp = (2 * P + 3) / 4 * 4, NQ = (2 * e->m_max + 7) / 8 * 8;
+  const size_t smem = ((size_t)KPp * NQ + (size_t)kUpdRows * (KPp + 1)) * sizeof(double);
+  e_update_kernel<<<e->row_ctas, kUpdThreads, smem, st>>>(e->d_slots, e->ns, which);
+  count_launch();
+  QDKP_CUDA_TRY(cudaGetLastError());
+  return QDKP_OK;
+}
+
+int tick(qdkp_engine* e, cudaStream_t st) {
+  const int ns = e->ns;
+  if (!ns) return QDKP_OK;
+  int rc;
+#define ETRY(x) do { rc = (x); if (rc != QDKP_OK) return rc; } while (0)
+  const size_t small_smem = 2 * (size_t)e->m_max * e->m_max * sizeof(double2);
+  const size_t rr_smem = 2 * (size_t)(3 * e->m_max) * (3 * e->m_max) * sizeof(double2);
+  e_norm_kernel<<<e->norm_ctas, kTallThreads, 0, st>>>(e->d_slots, ns);
+  e_decide_kernel<<<ns, 32, 0, st>>>(e->d_slots);
+  e_row_kernel<<<e->row_ctas, kTallThreads, 0, st>>>(e->d_slots, ns, RW_COPYBEST);
+  e_row_kernel<<<e->row_ctas, kTallThreads, 0, st>>>(e->d_slots, ns, RW_RESID);
+  count_launch(4);
+  QDKP_CUDA_TRY(cudaGetLastError());
+  ETRY(launch_apply_multi(e->d_hx + 0 * e->max_slots, ns, e->hx_tiles, e->S_max, QDKP_C128, st));
+  ETRY(launch_apply_multi(e->d_hx + 1 * e->max_slots, ns, e->hx_tiles, e->S_max, QDKP_C128, st));
+  e_row_kernel<<<e->row_ctas, kTallThreads, 0, st>>>(e->d_slots, ns, RW_GATHERP);
+  count_launch();
+  ETRY(launch_gram_multi(e, GR_XR, st));
+  ETRY(launch_update_multi(e, UP_RPROJ, st));
+  ETRY(launch_gram_multi(e, GR_RR, st));
+  e_rchol_kernel<<<ns, kSmallThreads, small_smem, st>>>(e->d_slots);
+  count_launch();
+  ETRY(launch_update_multi(e, UP_RNORM, st));
+  ETRY(launch_apply_multi(e->d_hx + 2 * e->max_slots, ns, e->hx_tiles, e->S_max, QDKP_C128, st));
+  ETRY(launch_apply_multi(e->d_hx + 3 * e->max_slots, ns, e->hx_tiles, e->S_max, QDKP_C128, st));
+  ETRY(launch_gram_multi(e, GR_PP, st));
+  e_pchol_kernel<<<ns, kSmallThreads, small_smem, st>>>(e->d_slots);
+  count_launch();
+  ETRY(launch_update_multi(e, UP_PNORM, st));
+  ETRY(launch_update_multi(e, UP_APNORM, st));
+  ETRY(launch_gram_multi(e, GR_WW, st));
+  ETRY(launch_gram_multi(e, GR_WAW, st));
+  e_rr_kernel<<<ns, kSmallThreads, rr_smem, st>>>(e->d_slots);
+  count_launch();
+  QDKP_CUDA_TRY(cudaGetLastError());
+  ETRY(launch_update_multi(e, UP_PNEW, st));
+  ETRY(launch_update_multi(e, UP_APNEW, st));
+  ETRY(launch_update_multi(e, UP_XNEW, st));
+  ETRY(launch_update_multi(e, UP_AXNEW, st));
+#undef ETRY
+  return QDKP_OK;
+}
+
+}  // namespace
+}  // namespace qdkp
+
+using namespace qdkp;
+
+extern "C" {
+
+int qdkp_engine_create(int max_slots, int device, qdkp_engine** out) {
+  QDKP_CHECK_ARG(out && max_slots >= 1 && max_slots <= 4096, "bad engine arguments");
+  QDKP_CUDA_TRY(cudaSetDevice(device));
+  auto* e = new qdkp_engine();
+  e->device = device;
+  e->max_slots = max_slots;
+  e->slots.resize(max_slots);
+  cudaError_t err = cudaMalloc(&e->d_slots, sizeof(ESlot) * max_slots);
+  if (err == cudaSuccess) err = cudaMalloc(&e->d_hx, sizeof(HXSlot) * 4 * max_slots);
+  if (err == cudaSuccess) err = cudaMalloc(&e->d_one, sizeof(int));
+  if (err == cudaSuccess) { const int one = 1; err = cudaMemcpy(e->d_one, &one, sizeof(int), cudaMemcpyHostToDevice); }
+  if (err != cudaSuccess) {
+    set_error(std::string("engine tables: ") + cudaGetErrorString(err));
+    cudaFree(e->d_slots); cudaFree(e->d_hx); cudaFree(e->d_one);
+    delete e;
+    return QDKP_ERR_CUDA;
+  }
+  // dynamic shared memory limits of the engine kernels
+  const int big = 200 * 1024;
+  cudaFuncSetAttribute(e_gram_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+  cudaFuncSetAttribute(e_gram_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+  cudaFuncSetAttribute(e_gram_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+  cudaFuncSetAttribute(e_gram_kernel<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+  cudaFuncSetAttribute(e_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+  cudaFuncSetAttribute(e_rr_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+  cudaFuncSetAttribute(e_rchol_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+  cudaFuncSetAttribute(e_pchol_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+  *out = e;
+  return QDKP_OK;
+}
+
+int qdkp_engine_destroy(qdkp_engine* e) {
+  if (!e) return QDKP_OK;
+  cudaSetDevice(e->device);
+  cudaFree(e->d_slots);
+  cudaFree(e->d_hx);
+  cudaFree(e->d_one);
+  delete e;
+  return QDKP_OK;
+}
+
+size_t qdkp_engine_slot_workspace_size(const qdkp_operator* op, const qdkp_lobpcg_params* prm) {
+  if (!op || !prm || prm->block < 1 || prm->block > kMaxBlock) return 0;
+  return slot_layout((int64_t)op->n_bands * op->n_sites, prm->block).total;
+}
+
+int qdkp_engine_admit(qdkp_engine* e, const qdkp_operator* op, const qdkp_lobpcg_params* prm,
+                      const void* X0, void* ws, size_t ws_bytes, void* stream, int* slot_out) {
+  QDKP_CHECK_ARG(e && op && prm && X0 && ws && slot_out, "NULL argument");
+  QDKP_CHECK_ARG(op->n_bands == 8, "the batched engine serves eight-band operators");
+  QDKP_CHECK_ARG(prm->block >= 1 && prm->block <= kMaxBlock, "block must be in [1, 24]");
+  QDKP_CHECK_ARG(prm->precision == QDKP_C128, "the engine computes in complex128");
+  QDKP_CHECK_ARG(op->device == e->device, "operator lives on another device");
+  const int64_t n = (int64_t)op->n_bands * op->n_sites;
+  const int m = prm->block;
+  QDKP_CHECK_ARG(n >= 5 * m, "problem too small for LOBPCG");
+  const SlotLayout L = slot_layout(n, m);
+  if (ws_bytes < L.total) { set_error("engine slot workspace too small"); return QDKP_ERR_WORKSPACE; }
+  int id = -1;
+  for (int i = 0; i < e->max_slots; ++i) if (!e->slots[i].used) { id = i; break; }
+  if (id < 0) { set_error("no free engine slot"); return QDKP_ERR_WORKSPACE; }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  SlotHost& h = e->slots[id];
+  h = SlotHost();
+  h.op = op;
+  h.prm = *prm;
+  char* p = static_cast<char*>(ws);
+  auto take = [&](size_t b) { char* r = p; p += align256(b); return r; };
+  ESlot& d = h.d;
+  d.st = (EState*)take(sizeof(EState));
+  d.X = (double2*)take(L.blk); d.AX = (double2*)take(L.blk); d.P = (double2*)take(L.blk);
+  d.AP = (double2*)take(L.blk); d.best = (double2*)take(L.blk); d.Ra = (double2*)take(L.blk);
+  d.ARa = (double2*)take(L.blk); d.Pa = (double2*)take(L.blk); d.APa = (double2*)take(L.blk);
+  d.T = (double2*)take(L.blk);
+  d.W = (double2*)take(L.small); d.G = (double2*)take(L.small); d.U = (double2*)take(L.small);
+  d.gS = (double2*)take(L.small); d.gT = (double2*)take(L.small); d.gA = (double2*)take(L.small);
+  d.gB = (double2*)take(L.small); d.E = (double2*)take(L.small);
+  d.scr = (double2*)take(2 * L.small);
+  d.Cx = (double2*)take(L.small); d.Cr = (double2*)take(L.small); d.Cp = (double2*)take(L.small);
+  d.Im = (double2*)take(L.small);
+  d.w = (double*)take(3 * m * sizeof(double));
+  d.npart = (double*)take(L.npart);
+  d.gpart = (double*)take(L.gpart);
+  h.gpart_doubles = L.gpart / sizeof(double);
+  d.n = n; d.m = m; d.folded = prm->folded;
+  d.tol = prm->tol > 0 ? prm->tol : std::sqrt(std::numeric_limits<double>::epsilon()) * (double)n;
+  d.maxiter = prm->maxiter;
+  d.restart_control = prm->restart_control > 0 ? prm->restart_control : 20;
+  d.nparts = L.nparts; d.gparts = L.gparts; d.rows_per_gpart = L.rows_per_gpart;
+  d.rows_per_cta = kERowsPerCta;
+  int rc;
+#define ATRY(x) do { rc = (x); if (rc != QDKP_OK) return rc; } while (0)
+  // X = orthonormalise(X0) (lobpcg.py:620-630)
+  ATRY(launch_copy((const double2*)X0, m, m, n, d.X, m, st));
+  ATRY(gram1(h, d.X, d.X, m, d.G, st));
+  ATRY(launch_chol_inv(d.G, m, d.U, (int*)d.w, st));
+  int stat = 0;
+  ATRY(read_sync(&stat, d.w, sizeof(int), st));
+  if (stat) { set_error("Linearly dependent initial approximations"); return QDKP_ERR_NUMERIC; }
+  {
+    const double2* C[1] = {d.U};
+    ATRY(launch_update(one(d.X, m), C, m, n, d.X, m, 0, st));
+  }
+  // initial Ritz vectors (lobpcg.py:633-660)
+  ATRY(apply_folded(h, d.X, m, d.AX, st));
+  ATRY(gram1(h, d.X, d.AX, m, d.gT, st));
+  ATRY(launch_eigh(d.gT, nullptr, m, d.w, d.E, d.scr, (int*)d.G, st));
+  ATRY(read_sync(&stat, d.G, sizeof(int), st));
+  if (stat) { set_error("initial Rayleigh-Ritz failed"); return QDKP_ERR_NUMERIC; }
+  {
+    const double2* C[1] = {d.E};
+    ATRY(launch_update(one(d.X, m), C, m, n, d.X, m, 0, st));
+    ATRY(launch_update(one(d.AX, m), C, m, n, d.AX, m, 0, st));
+  }
+  std::vector<double> w(m);
+  ATRY(read_sync(w.data(), d.w, m * sizeof(double), st));
+  EState s0{};
+  s0.running = 1; s0.status = QDKP_LOBPCG_MAXITER; s0.iter = -1; s0.idle = 1;
+  s0.ma = m; s0.mp = 0; s0.restart = 1; s0.forced = 0; s0.explicit_gram = 0;
+  s0.best_iter = prm->maxiter; s0.skip_recompute = 1; s0.skip_p = 1; s0.skip_pnorm = 1;
+  s0.smallest = std::numeric_limits<double>::max();
+  for (int j = 0; j < m; ++j) { s0.active[j] = 1; s0.lam[j] = w[j]; }
+  std::vector<double2> Im((size_t)m * m, make_double2(0.0, 0.0));
+  for (int j = 0; j < m; ++j) Im[(size_t)j * m + j] = make_double2(1.0, 0.0);
+  QDKP_CUDA_TRY(cudaMemcpyAsync(d.Im, Im.data(), Im.size() * sizeof(double2), cudaMemcpyHostToDevice, st));
+  QDKP_CUDA_TRY(cudaMemcpyAsync(d.st, &s0, sizeof(EState), cudaMemcpyHostToDevice, st));
+  QDKP_CUDA_TRY(cudaStreamSynchronize(st));
+#undef ATRY
+  h.used = true;
+  e->dirty = true;
+  *slot_out = id;
+  return QDKP_OK;
+}
+
+int qdkp_engine_step(qdkp_engine* e, int ticks, void* stream) {
+  QDKP_CHECK_ARG(e && ticks >= 0, "bad arguments");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  QDKP_CUDA_TRY(cudaSetDevice(e->device));
+  if (e->dirty) { int rc = rebuild(e, st); if (rc) return rc; }
+  for (int t = 0; t < ticks; ++t) {
+    int rc = tick(e, st);
+    if (rc) return rc;
+  }
+  return QDKP_OK;
+}
+
+int qdkp_engine_poll(qdkp_engine* e, int* state, int* status, int* iterations, void* stream) {
+  QDKP_CHECK_ARG(e && state, "bad arguments");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  std::vector<EState> hs(e->max_slots);
+  for (int i = 0; i < e->max_slots; ++i) {
+    const SlotHost& h = e->slots[i];
+    if (!h.used) continue;
+    QDKP_CUDA_TRY(cudaMemcpyAsync(&hs[i], h.d.st, sizeof(EState), cudaMemcpyDeviceToHost, st));
+  }
+  QDKP_CUDA_TRY(cudaStreamSynchronize(st));
+  for (int i = 0; i < e->max_slots; ++i) {
+    const SlotHost& h = e->slots[i];
+    state[i] = !h.used ? -1 : (hs[i].running ? 1 : 0);
+    if (status) status[i] = h.used ? hs[i].status : -1;
+    if (iterations) iterations[i] = h.used ? hs[i].iter + 1 : 0;
+  }
+  return QDKP_OK;
+}
+
+int qdkp_engine_retire(qdkp_engine* e, int slot, double* lambda_out, void* V,
+                       double* residuals_out, qdkp_lobpcg_info* info, void* stream) {
+  QDKP_CHECK_ARG(e && slot >= 0 && slot < e->max_slots && e->slots[slot].used, "bad slot");
+  QDKP_CHECK_ARG(lambda_out && V && info, "NULL argument");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  SlotHost& h = e->slots[slot];
+  ESlot& d = h.d;
+  const int m = d.m;
+  const int64_t n = d.n;
+  int rc;
+#define RTRY(x) do { rc = (x); if (rc != QDKP_OK) return rc; } while (0)
+  EState s;
+  RTRY(read_sync(&s, d.st, sizeof(EState), st));
+  std::vector<double> lam(s.lam, s.lam + m), rn2(m), norms(m);
+  // residuals of the last iterate; it becomes the best one if it improved (lobpcg.py:975-995)
+  double* dl = d.w;
+  QDKP_CUDA_TRY(cudaMemcpyAsync(dl, lam.data(), m * sizeof(double), cudaMemcpyHostToDevice, st));
+  RTRY(launch_colnorm2(d.AX, m, d.X, m, dl, m, n, d.npart, d.nparts, d.gpart, st));
+  RTRY(read_sync(rn2.data(), d.gpart, m * sizeof(double), st));
+  double mean = 0.0;
+  for (int j = 0; j < m; ++j) mean += std::sqrt(std::fabs(rn2[j]));
+  mean /= m;
+  int best_iter = s.best_iter;
+  if (s.status != QDKP_LOBPCG_NONFINITE && mean < s.smallest) {
+    RTRY(launch_copy(d.X, m, m, n, d.best, m, st));
+    best_iter = s.iter + 1;
+  }
+  // final Rayleigh-Ritz on the best iterate (lobpcg.py:1009-1060)
+  RTRY(apply_folded(h, d.best, m, d.AX, st));
+  RTRY(gram1(h, d.best, d.AX, m, d.gT, st));
+  RTRY(gram1(h, d.best, d.best, m, d.gS, st));
+  {
+    std::vector<double2> t((size_t)m * m), s2((size_t)m * m), a((size_t)m * m), bb((size_t)m * m);
+    RTRY(read_sync(t.data(), d.gT, t.size() * sizeof(double2), st));
+    RTRY(read_sync(s2.data(), d.gS, s2.size() * sizeof(double2), st));
+    for (int i = 0; i < m; ++i)
+      for (int j = 0; j < m; ++j) {
+        const double2 x = t[(size_t)i * m + j], y = t[(size_t)j * m + i];
+        a[(size_t)i * m + j] = make_double2(0.5 * (x.x + y.x), 0.5 * (x.y - y.y));
+        const double2 u = s2[(size_t)i * m + j], v = s2[(size_t)j * m + i];
+        bb[(size_t)i * m + j] = make_double2(0.5 * (u.x + v.x), 0.5 * (u.y - v.y));
+      }
+    QDKP_CUDA_TRY(cudaMemcpyAsync(d.gA, a.data(), a.size() * sizeof(double2), cudaMemcpyHostToDevice, st));
+    QDKP_CUDA_TRY(cudaMemcpyAsync(d.gB, bb.data(), bb.size() * sizeof(double2), cudaMemcpyHostToDevice, st));
+  }
+  RTRY(launch_eigh(d.gA, d.gB, m, d.w, d.E, d.scr, (int*)d.G, st));
+  int stat = 0;
+  RTRY(read_sync(&stat, d.G, sizeof(int), st));
+  if (stat) { set_error("eigh has failed in lobpcg postprocessing"); return QDKP_ERR_NUMERIC; }
+  RTRY(read_sync(lam.data(), d.w, m * sizeof(double), st));
+  {
+    const double2* C[1] = {d.E};
+    RTRY(launch_update(one(d.best, m), C, m, n, (double2*)V, m, 0, st));
+    RTRY(launch_update(one(d.AX, m), C, m, n, d.AX, m, 0, st));
+  }
+  RTRY(launch_colnorm2(d.AX, m, (const double2*)V, m, d.w, m, n, d.npart, d.nparts, d.gpart, st));
+  RTRY(read_sync(rn2.data(), d.gpart, m * sizeof(double), st));
+  bool all = true;
+  for (int j = 0; j < m; ++j) {
+    norms[j] = std::sqrt(std::fabs(rn2[j]));
+    all = all && norms[j] <= d.tol;
+  }
+  std::memcpy(lambda_out, lam.data(), m * sizeof(double));
+  if (residuals_out) std::memcpy(residuals_out, norms.data(), m * sizeof(double));
+  int status = s.status;
+  if (status == QDKP_LOBPCG_MAXITER && all) status = QDKP_LOBPCG_CONVERGED;
+  std::memset(info, 0, sizeof(*info));
+  info->iterations = std::min(best_iter + 2, h.prm.maxiter + 3);
+  info->best_iteration = best_iter;
+  info->status = status;
+  info->explicit_gram = s.explicit_gram;
+  info->best_mean_residual = s.smallest;
+#undef RTRY
+  h.used = false;
+  e->dirty = true;
+  return QDKP_OK;
+}
+
+}  // extern "C"

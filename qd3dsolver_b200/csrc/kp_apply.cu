@@ -165,11 +165,8 @@ template <> struct ApplyOcc<double> { static constexpr int kMinBlocks = 2; };
 template <> struct ApplyOcc<float> { static constexpr int kMinBlocks = 2; };
 
 template <typename T, int NB>
-__global__ void __launch_bounds__(256, ApplyOcc<T>::kMinBlocks) kp_apply_kernel(const ApplyArgs<T> a) {
-  extern __shared__ unsigned char smem_raw[];
-  T* rec = reinterpret_cast<T*>(smem_raw);
+__device__ __forceinline__ void apply_tile(const ApplyArgs<T>& a, long long s0, T* rec) {
   const int S = a.S;
-  const long long s0 = (long long)blockIdx.x * S;
   const int ns = (int)min((long long)S, a.N - s0);
 
   for (int i = threadIdx.x; i < ns; i += blockDim.x) build_record<T, NB>(a, s0 + i, rec + i, S);
@@ -335,6 +332,54 @@ __global__ void __launch_bounds__(256, ApplyOcc<T>::kMinBlocks) kp_apply_kernel(
   }
 }
 
+template <typename T, int NB>
+__global__ void __launch_bounds__(256, ApplyOcc<T>::kMinBlocks) kp_apply_kernel(const ApplyArgs<T> a) {
+  extern __shared__ unsigned char smem_raw[];
+  apply_tile<T, NB>(a, (long long)blockIdx.x * a.S, reinterpret_cast<T*>(smem_raw));
+}
+
+// Many operators and blocks in one launch (the batched engine): CTA b serves slot k with
+// tile0[k] <= b < tile0[k+1]; the column count is read on the device (the slot's active width).
+template <typename T>
+__global__ void __launch_bounds__(256, ApplyOcc<T>::kMinBlocks)
+kp_apply_multi_kernel(const HXSlot* __restrict__ slots, int nslots) {
+  extern __shared__ unsigned char smem_raw[];
+  int k = 0;
+  while (k + 1 < nslots && (int)blockIdx.x >= slots[k + 1].tile0) ++k;
+  const HXSlot& d = slots[k];
+  if (d.skip && *d.skip) return;
+  const int m = d.m_dev ? *d.m_dev : d.m;
+  if (m <= 0) return;
+  ApplyArgs<T> a;
+  a.F = static_cast<const T*>(d.F);
+  a.X = static_cast<const cplx<T>*>(d.X);
+  a.Y = static_cast<cplx<T>*>(d.Y);
+  a.N = d.N; a.ldx = d.ld_same ? m : d.ldx; a.ldy = d.ld_same ? m : d.ldy;
+  a.nx = d.nx; a.ny = d.ny; a.nz = d.nz; a.m = m; a.flags = d.flags; a.S = d.S;
+  a.h = (T)d.h; a.sigma = (T)d.sigma; a.sign = (T)d.sign; a.shifted = d.shifted;
+  apply_tile<T, 8>(a, (long long)(blockIdx.x - d.tile0) * d.S, reinterpret_cast<T*>(smem_raw));
+}
+
+int launch_apply_multi(const HXSlot* slots_dev, int nslots, int total_tiles, int S_max,
+                       int precision, cudaStream_t st) {
+  if (total_tiles <= 0) return QDKP_OK;
+  if (precision == QDKP_C128) {
+    kp_apply_multi_kernel<double><<<total_tiles, 256, (size_t)R_COUNT * S_max * sizeof(double), st>>>(
+        slots_dev, nslots);
+  } else {
+    kp_apply_multi_kernel<float><<<total_tiles, 256, (size_t)R_COUNT * S_max * sizeof(float), st>>>(
+        slots_dev, nslots);
+  }
+  count_launch();
+  QDKP_CUDA_TRY(cudaGetLastError());
+  return QDKP_OK;
+}
+
+int apply_tile_sites(int m) {
+  int S = (512 + m - 1) / m;
+  return S < 32 ? 32 : (S > 128 ? 128 : S);
+}
+
 template <typename T>
 static int launch_apply_t(const qdkp_operator* op, const T* F, const void* X, int64_t ldx,
                           void* Y, int64_t ldy, int m, double sigma, int shifted,
@@ -348,8 +393,7 @@ static int launch_apply_t(const qdkp_operator* op, const T* F, const void* X, in
   a.h = (T)op->h; a.sigma = (T)sigma; a.shifted = shifted;
   a.sign = ((op->flags & QDKP_HOLE_CONVENTION) && op->n_bands != 8) ? T(-1) : T(1);
   if (op->flags & QDKP_NEGATE) a.sign = -a.sign;
-  int S = (512 + m - 1) / m;
-  S = S < 32 ? 32 : (S > 128 ? 128 : S);
+  const int S = apply_tile_sites(m);
   a.S = S;
   const size_t smem = (size_t)R_COUNT * S * sizeof(T);
   const unsigned grid = (unsigned)((op->n_sites + S - 1) / S);

@@ -78,6 +78,27 @@ enum FieldIndex {
 
 constexpr double kG = 0.0380998;   // hbar^2 / 2 m0 in eV nm^2 (qdsolver_core.py:19)
 
+// One operator/block pair of a multi-slot H.X launch (eight bands).
+struct HXSlot {
+  const void* F;          // fields in the launch precision
+  const void* X;
+  void* Y;
+  long long N, ldx, ldy;
+  int nx, ny, nz, flags;
+  int S;                  // sites per tile
+  int tile0;              // first CTA of this slot in the launch
+  int m;                  // column count if m_dev is NULL
+  const int* m_dev;       // device column count (active width), or NULL
+  const int* skip;        // nonzero: slot idle this tick
+  int ld_same;            // leading dimensions equal the column count
+  int shifted;
+  double h, sigma, sign;
+};
+
+int launch_apply_multi(const HXSlot* slots_dev, int nslots, int total_tiles, int S_max,
+                       int precision, cudaStream_t st);
+int apply_tile_sites(int m);
+
 }  // namespace qdkp
 
 // The operator handle (opaque to C callers).

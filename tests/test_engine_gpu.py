@@ -1,0 +1,68 @@
+"""The batched engine (served form): same solves as the single-solve drop-in, and every result
+identical alone and in a mix of other solves."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), 'golden')
+
+
+@pytest.fixture(scope='module')
+def ops():
+    from qd3dsolver_b200 import kp_pryor as kpg, workloads as wl
+    z = np.load(os.path.join(GOLDEN, 'solve_cases.npz'))
+    with open(os.path.join(GOLDEN, 'solve_cases.json')) as fh:
+        meta = json.load(fh)
+    f = {k[3:]: z[k] for k in z.files if k.startswith('f8_')}
+    st = {k: f[k] for k in wl.STRAIN_KEYS}
+    small = kpg.confined_hamiltonian(kpg.GridOperators(tuple(meta['shape']), float(z['h'])), f,
+                                     8, strain=st)
+    w = wl.fig4_from_fixture(os.path.join(GOLDEN, 'fig4_b10_fields.npz'))
+    fb = w.fields
+    fig4 = kpg.confined_hamiltonian(kpg.GridOperators(w.shape, w.h), fb, 8,
+                                    strain={k: fb[k] for k in wl.STRAIN_KEYS})
+    return dict(small=small, meta=meta, fig4=fig4, w=w)
+
+
+def test_engine_matches_single_solve(ops):
+    from qd3dsolver_b200 import eigensolvers as eg, serving
+    H, ref = ops['small'], ops['meta']['interior_cb']
+    E1, V1, i1 = eg.solve_interior(H, k=4, sigma=ref['sigma'], tol=ref['tol'],
+                                   maxiter=ref['maxiter'], verbose=False)
+    r = serving.Request(H, k=4, sigma=ref['sigma'], tol=ref['tol'], maxiter=ref['maxiter'])
+    serving.solve_batch([r], max_slots=4)
+    assert r.result['status'] == 'converged'
+    assert np.abs(r.result['E'] - E1).max() < 1e-10
+    assert abs(r.result['iterations'] - i1['iterations']) <= 0.03 * i1['iterations']  # norm sums differ in order
+    assert np.abs(r.result['E'] - np.array(ref['E'])).max() < 1e-8
+
+
+def test_engine_alone_equals_mix(ops):
+    """Each request's eigenvalues and residuals are the same alone and in the mix."""
+    from qd3dsolver_b200 import serving
+    w, H4, Hs, meta = ops['w'], ops['fig4'], ops['small'], ops['meta']
+
+    def reqs():
+        return [serving.Request(H4, k=8, sigma=w.sigma['cb'], tol=1e-7, maxiter=8000, tag='cb'),
+                serving.Request(Hs, k=4, sigma=meta['interior_vb']['sigma'], tol=1e-9,
+                                maxiter=4000, tag='small_vb'),
+                serving.Request(H4, k=8, sigma=w.sigma['vb'], tol=1e-7, maxiter=8000, tag='vb'),
+                serving.Request(Hs, k=4, sigma=meta['interior_cb']['sigma'], tol=1e-9,
+                                maxiter=4000, tag='small_cb')]
+    mix = serving.solve_batch(reqs(), max_slots=3, ticks_per_poll=5)   # 3 slots: continuous
+    alone = [serving.solve_batch([r], max_slots=1, ticks_per_poll=7)[0] for r in reqs()]
+    for a, b in zip(alone, mix):
+        assert a.tag == b.tag
+        assert a.result['iterations'] == b.result['iterations'], a.tag
+        assert np.abs(a.result['E'] - b.result['E']).max() <= 1e-12, a.tag
+        assert np.abs(a.result['residuals'] - b.result['residuals']).max() <= 1e-12, a.tag
+    # and the fig-4 solves reproduce the reference's eigenvalues
+    with open(os.path.join(GOLDEN, 'fig4_b10.json')) as fh:
+        ref = json.load(fh)
+    for r in mix:
+        if r.tag in ('cb', 'vb'):
+            assert np.abs(np.sort(r.result['E']) - np.array(ref[r.tag]['E'])).max() < 1e-6
+            assert r.result['converged']
