@@ -148,73 +148,10 @@ __global__ void __launch_bounds__(kGramThreads)
 gram_partial_kernel(const BlockList<double> A, const BlockList<double> B, long long n,
                     long long rows_per_part, double* __restrict__ partial) {
   extern __shared__ double gsm_d[];
-  const int P = A.total(), Q = B.total();
-  const int RP = (2 * P + 7) / 8 * 8, RQ = (2 * Q + 7) / 8 * 8;   // padded real widths
-  double* sA = gsm_d;                        // [kGramChunk][RP]
-  double* sB = gsm_d + kGramChunk * RP;      // [kGramChunk][RQ]
+  const int RP = (2 * A.total() + 7) / 8 * 8, RQ = (2 * B.total() + 7) / 8 * 8;
   const long long r0 = blockIdx.x * rows_per_part;
-  const long long r1 = min(n, r0 + rows_per_part);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int g = lane >> 2, t4 = lane & 3;
-  const int TR = RP / 8, TC = RQ / 8;
-  const int wr = warp / kGramWarpsC, wc = warp % kGramWarpsC;
-  const int tr_per = (TR + kGramWarpsR - 1) / kGramWarpsR, tc_per = (TC + kGramWarpsC - 1) / kGramWarpsC;
-  const int tr0 = wr * tr_per, tc0 = wc * tc_per;
-  double acc[MAXT][MAXT][2];
-#pragma unroll
-  for (int i = 0; i < MAXT; ++i)
-#pragma unroll
-    for (int j = 0; j < MAXT; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
-
-  for (long long rt = r0; rt < r1; rt += kGramChunk) {
-    // stage rows [rt, rt + chunk) of A' and B' (zero padded)
-    for (int e = threadIdx.x; e < kGramChunk * (RP / 2); e += blockDim.x) {
-      const int row = e / (RP / 2), c = e - row * (RP / 2);
-      double2 z = make_double2(0.0, 0.0);
-      if (rt + row < r1 && c < P) z = list_elem(A, rt + row, c);
-      *reinterpret_cast<double2*>(&sA[row * RP + 2 * c]) = z;
-    }
-    for (int e = threadIdx.x; e < kGramChunk * (RQ / 2); e += blockDim.x) {
-      const int row = e / (RQ / 2), c = e - row * (RQ / 2);
-      double2 z = make_double2(0.0, 0.0);
-      if (rt + row < r1 && c < Q) z = list_elem(B, rt + row, c);
-      *reinterpret_cast<double2*>(&sB[row * RQ + 2 * c]) = z;
-    }
-    __syncthreads();
-#pragma unroll 2
-    for (int k0 = 0; k0 < kGramChunk; k0 += 4) {
-      double a[MAXT], b[MAXT];
-#pragma unroll
-      for (int i = 0; i < MAXT; ++i) {
-        const int ti = tr0 + i;
-        a[i] = (i < tr_per && ti < TR) ? sA[(k0 + t4) * RP + ti * 8 + g] : 0.0;
-      }
-#pragma unroll
-      for (int j = 0; j < MAXT; ++j) {
-        const int tj = tc0 + j;
-        b[j] = (j < tc_per && tj < TC) ? sB[(k0 + t4) * RQ + tj * 8 + g] : 0.0;
-      }
-#pragma unroll
-      for (int i = 0; i < MAXT; ++i)
-#pragma unroll
-        for (int j = 0; j < MAXT; ++j)
-          if (i < tr_per && j < tc_per) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
-    }
-    __syncthreads();
-  }
-  // partial C' (RP x RQ, row-major) for this slice
-  double* out = partial + (long long)blockIdx.x * RP * RQ;
-#pragma unroll
-  for (int i = 0; i < MAXT; ++i)
-#pragma unroll
-    for (int j = 0; j < MAXT; ++j) {
-      const int ti = tr0 + i, tj = tc0 + j;
-      if (i < tr_per && j < tc_per && ti < TR && tj < TC) {
-        const int row = ti * 8 + g, col = tj * 8 + 2 * t4;
-        out[(long long)row * RQ + col] = acc[i][j][0];
-        out[(long long)row * RQ + col + 1] = acc[i][j][1];
-      }
-    }
+  gram_core<MAXT>(A, B, r0, min(n, r0 + rows_per_part),
+                  partial + (long long)blockIdx.x * RP * RQ, gsm_d);
 }
 
 // Stage 1: column-block sums of the partial C' slices (coalesced over the RP x RQ elements);
@@ -271,7 +208,16 @@ int launch_gram(const BlockList<double>& A, const BlockList<double>& B, long lon
     set_error("gram partial buffer too small");
     return QDKP_ERR_WORKSPACE;
   }
-  const size_t smem = (size_t)kGramChunk * (RP + RQ) * sizeof(double);
+  const size_t smem = (size_t)2 * kGramChunk * (RP + RQ) * sizeof(double);
+  static bool attr = false;
+  if (!attr) {
+    const int big = 200 * 1024;
+    cudaFuncSetAttribute(gram_partial_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    cudaFuncSetAttribute(gram_partial_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    cudaFuncSetAttribute(gram_partial_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    cudaFuncSetAttribute(gram_partial_kernel<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    attr = true;
+  }
   const int TR = RP / 8, TC = RQ / 8;
   const int tmax = std::max((TR + kGramWarpsR - 1) / kGramWarpsR, (TC + kGramWarpsC - 1) / kGramWarpsC);
   double* pd = reinterpret_cast<double*>(partial);
@@ -303,7 +249,7 @@ update_kernel(const BlockList<double> A, const CoefList C, int q, long long n, d
               long long ldy, int accumulate) {
   extern __shared__ double usm[];
   const double2* Cf[3] = {C.c[0], C.c[1], C.c[2]};
-  const long long per = ((n + gridDim.x - 1) / gridDim.x + kUpdRows - 1) / kUpdRows * kUpdRows;
+  const long long per = ((n + gridDim.x - 1) / gridDim.x + 63) / 64 * 64;
   const long long r0 = (long long)blockIdx.x * per;
   update_rows(A, Cf, q, r0, min(n, r0 + per), Y, ldy, accumulate, 0, usm);
 }
@@ -315,7 +261,7 @@ int launch_update(const BlockList<double>& A, const double2* const* C, int q, lo
   for (int b = 0; b < 3; ++b) cl.c[b] = b < A.nblk ? C[b] : nullptr;
   const int P = A.total();
   const int KPp = (2 * P + 3) / 4 * 4, NQ = (2 * q + 7) / 8 * 8;
-  const size_t smem = ((size_t)KPp * NQ + (size_t)kUpdRows * (KPp + 1)) * sizeof(double);
+  const size_t smem = ((size_t)KPp * NQ + (size_t)kUpdWarps * kUpdRows * (KPp + 2)) * sizeof(double);
   static bool attr = false;
   if (!attr) {
     QDKP_CUDA_TRY(cudaFuncSetAttribute(update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -272,15 +272,17 @@ static __device__ int block_eigh(const double2* __restrict__ A, const double2* _
 // Y' = A' C'' on the FP64 tensor cores for rows [r0, r1), with A' (rows x 2P) the real view of
 // [A_0 | A_1 | A_2] and C'' (2P x 2q) the real representation of the stacked complex
 // coefficients: C''_{2i,2j} = Re C_ij, C''_{2i,2j+1} = Im C_ij, C''_{2i+1,2j} = -Im C_ij,
-// C''_{2i+1,2j+1} = Re C_ij (negated when neg). An MMA accumulator pair (d0, d1) of a lane is
-// one complex output. Rows are staged 32 at a time and every warp has read the staged rows
-// before any row of Y is written, so Y may alias one of the inputs.
-constexpr int kUpdRows = 32;
+// C''_{2i+1,2j+1} = Re C_ij (negated when neg). An m8n8k4 MMA takes exactly 8 rows, so each
+// warp streams its own 8-row tiles: it stages the tile's inputs in its own shared-memory slice,
+// runs the MMAs against the CTA's C'' and writes the tile's outputs; no CTA barrier in the loop.
+// A warp has staged all 8 rows before it writes any of them, so Y may alias one of the inputs.
+constexpr int kUpdRows = 8;
 constexpr int kUpdThreads = 256;
+constexpr int kUpdWarps = kUpdThreads / 32;
 
-static __device__ size_t update_smem_doubles(int P, int q) {
+static __device__ __forceinline__ size_t update_smem_doubles(int P, int q) {
   const int KPp = (2 * P + 3) / 4 * 4, NQ = (2 * q + 7) / 8 * 8;
-  return (size_t)KPp * NQ + (size_t)kUpdRows * (KPp + 1);
+  return (size_t)KPp * NQ + (size_t)kUpdWarps * kUpdRows * (KPp + 2);
 }
 
 static __device__ void update_rows(const BlockList<double>& A, const double2* const* C, int q,
@@ -290,9 +292,10 @@ static __device__ void update_rows(const BlockList<double>& A, const double2* co
   const int KP = 2 * P;
   const int KPp = (KP + 3) / 4 * 4;
   const int NQ = (2 * q + 7) / 8 * 8;
+  const int lda_s = KPp + 2;             // even: 16-byte aligned double2 stores
   double* sC = usm;
-  double* sA = usm + KPp * NQ;
-  const int lda_s = KPp + 1;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double* sA = usm + KPp * NQ + (size_t)warp * kUpdRows * lda_s;
   const double sg = neg ? -1.0 : 1.0;
   int off[3];
   int tot = 0;
@@ -309,57 +312,156 @@ static __device__ void update_rows(const BlockList<double>& A, const double2* co
     sC[(2 * i + 1) * NQ + 2 * j] = -sg * c.y;
     sC[(2 * i + 1) * NQ + 2 * j + 1] = sg * c.x;
   }
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int e = lane; e < kUpdRows * (KPp - KP); e += 32) {
+    const int row = e / (KPp - KP), c = e - row * (KPp - KP);
+    sA[row * lda_s + KP + c] = 0.0;
+  }
+  __syncthreads();
   const int g = lane >> 2, t4 = lane & 3;
-  const int mt = warp & 3;
-  const int nhalf = warp >> 2;
   const int NT = NQ / 8;
-  const int nt_per = (NT + 1) / 2;
-  const int nt0 = nhalf * nt_per;
-  for (long long rb = r0; rb < r1; rb += kUpdRows) {
-    __syncthreads();
+  for (long long rb = r0 + (long long)warp * kUpdRows; rb < r1;
+       rb += (long long)kUpdWarps * kUpdRows) {
     for (int b = 0; b < A.nblk; ++b) {
       const int cb = A.cols[b];
-      for (int e = threadIdx.x; e < kUpdRows * cb; e += blockDim.x) {
+      const double2* __restrict__ src = A.p[b];
+      const long long ld = A.ld[b];
+      for (int e = lane; e < kUpdRows * cb; e += 32) {
         const int row = e / cb, c = e - row * cb;
         double2 z = make_double2(0.0, 0.0);
-        if (rb + row < r1) z = A.p[b][(rb + row) * A.ld[b] + c];
-        sA[row * lda_s + 2 * (off[b] + c)] = z.x;
-        sA[row * lda_s + 2 * (off[b] + c) + 1] = z.y;
+        if (rb + row < r1) z = src[(rb + row) * ld + c];
+        *reinterpret_cast<double2*>(&sA[row * lda_s + 2 * (off[b] + c)]) = z;
       }
     }
-    for (int e = threadIdx.x; e < kUpdRows * (KPp - KP); e += blockDim.x) {
-      const int row = e / (KPp - KP), c = e - row * (KPp - KP);
-      sA[row * lda_s + KP + c] = 0.0;
-    }
-    __syncthreads();
-    double acc[3][2];
-    const long long rowg = rb + mt * 8 + g;
+    __syncwarp();
+    const long long rowg = rb + g;
+    double acc[6][2];
 #pragma unroll
-    for (int j = 0; j < 3; ++j) {
-      const int col = (nt0 + j) * 4 + t4;
+    for (int j = 0; j < 6; ++j) {
+      const int col = j * 4 + t4;
       double2 y0 = make_double2(0.0, 0.0);
-      if (accumulate && j < nt_per && nt0 + j < NT && col < q && rowg < r1) y0 = Y[rowg * ldy + col];
+      if (accumulate && j < NT && col < q && rowg < r1) y0 = Y[rowg * ldy + col];
       acc[j][0] = y0.x; acc[j][1] = y0.y;
     }
     for (int k0 = 0; k0 < KPp; k0 += 4) {
-      const double a = sA[(mt * 8 + g) * lda_s + k0 + t4];
+      const double a = sA[g * lda_s + k0 + t4];
 #pragma unroll
-      for (int j = 0; j < 3; ++j) {
-        if (j < nt_per && nt0 + j < NT) {
-          const double bb = sC[(k0 + t4) * NQ + (nt0 + j) * 8 + g];
-          dmma(acc[j][0], acc[j][1], a, bb);
-        }
+      for (int j = 0; j < 6; ++j) {
+        if (j < NT) dmma(acc[j][0], acc[j][1], a, sC[(k0 + t4) * NQ + j * 8 + g]);
       }
     }
-    __syncthreads();
 #pragma unroll
-    for (int j = 0; j < 3; ++j) {
-      const int col = (nt0 + j) * 4 + t4;
-      if (j < nt_per && nt0 + j < NT && col < q && rowg < r1)
-        Y[rowg * ldy + col] = make_double2(acc[j][0], acc[j][1]);
+    for (int j = 0; j < 6; ++j) {
+      const int col = j * 4 + t4;
+      if (j < NT && col < q && rowg < r1) Y[rowg * ldy + col] = make_double2(acc[j][0], acc[j][1]);
+    }
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Gram core: partial C' = A'^T B' (real views) of rows [r0, r1) on the FP64 MMA units.
+// Rows are staged in chunks of kGramChunk through a two-stage cp.async pipeline (16-byte copies
+// of complex elements straight into the real-view layout), so the next chunk loads while the
+// current one is multiplied. Writes the RP x RQ partial (row-major) to `out`.
+// ---------------------------------------------------------------------------------------------
+static __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" :: "r"(s), "l"(gmem));
+}
+static __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+static __device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::); }
+static __device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;\n" ::); }
+
+static __device__ __forceinline__ void gram_stage(const BlockList<double>& L, int P, int RP,
+                                                  long long rt, long long r1, double* buf) {
+  for (int e = threadIdx.x; e < kGramChunk * (RP / 2); e += blockDim.x) {
+    const int row = e / (RP / 2), c = e - row * (RP / 2);
+    double* dst = &buf[row * RP + 2 * c];
+    if (rt + row < r1 && c < P) {
+      int b = 0, cc = c;
+      while (b < L.nblk - 1 && cc >= L.cols[b]) { cc -= L.cols[b]; ++b; }
+      cp_async16(dst, L.p[b] + (rt + row) * L.ld[b] + cc);
+    } else {
+      *reinterpret_cast<double2*>(dst) = make_double2(0.0, 0.0);
     }
   }
+}
+
+static __device__ __forceinline__ size_t gram_smem_bytes(int P, int Q) {
+  const int RP = (2 * P + 7) / 8 * 8, RQ = (2 * Q + 7) / 8 * 8;
+  return (size_t)2 * kGramChunk * (RP + RQ) * sizeof(double);
+}
+
+template <int MAXT>
+static __device__ void gram_core(const BlockList<double>& A, const BlockList<double>& B,
+                                 long long r0, long long r1, double* __restrict__ out,
+                                 double* gsm) {
+  const int P = A.total(), Q = B.total();
+  const int RP = (2 * P + 7) / 8 * 8, RQ = (2 * Q + 7) / 8 * 8;
+  double* sA[2] = {gsm, gsm + kGramChunk * RP};
+  double* sB[2] = {gsm + 2 * kGramChunk * RP, gsm + 2 * kGramChunk * RP + kGramChunk * RQ};
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = lane >> 2, t4 = lane & 3;
+  const int TR = RP / 8, TC = RQ / 8;
+  const int wr = warp / kGramWarpsC, wc = warp % kGramWarpsC;
+  const int tr_per = (TR + kGramWarpsR - 1) / kGramWarpsR, tc_per = (TC + kGramWarpsC - 1) / kGramWarpsC;
+  const int tr0 = wr * tr_per, tc0 = wc * tc_per;
+  double acc[MAXT][MAXT][2];
+#pragma unroll
+  for (int i = 0; i < MAXT; ++i)
+#pragma unroll
+    for (int j = 0; j < MAXT; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+  const int nchunks = r1 > r0 ? (int)((r1 - r0 + kGramChunk - 1) / kGramChunk) : 0;
+  if (nchunks > 0) {
+    gram_stage(A, P, RP, r0, r1, sA[0]);
+    gram_stage(B, Q, RQ, r0, r1, sB[0]);
+  }
+  cp_async_commit();
+  for (int ch = 0; ch < nchunks; ++ch) {
+    const int cur = ch & 1;
+    if (ch + 1 < nchunks) {
+      const long long rn = r0 + (long long)(ch + 1) * kGramChunk;
+      gram_stage(A, P, RP, rn, r1, sA[cur ^ 1]);
+      gram_stage(B, Q, RQ, rn, r1, sB[cur ^ 1]);
+    }
+    cp_async_commit();
+    cp_async_wait1();
+    __syncthreads();
+    const double* a_s = sA[cur];
+    const double* b_s = sB[cur];
+#pragma unroll 2
+    for (int k0 = 0; k0 < kGramChunk; k0 += 4) {
+      double a[MAXT], b[MAXT];
+#pragma unroll
+      for (int i = 0; i < MAXT; ++i) {
+        const int ti = tr0 + i;
+        a[i] = (i < tr_per && ti < TR) ? a_s[(k0 + t4) * RP + ti * 8 + g] : 0.0;
+      }
+#pragma unroll
+      for (int j = 0; j < MAXT; ++j) {
+        const int tj = tc0 + j;
+        b[j] = (j < tc_per && tj < TC) ? b_s[(k0 + t4) * RQ + tj * 8 + g] : 0.0;
+      }
+#pragma unroll
+      for (int i = 0; i < MAXT; ++i)
+#pragma unroll
+        for (int j = 0; j < MAXT; ++j)
+          if (i < tr_per && j < tc_per) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+    }
+    __syncthreads();
+  }
+  cp_async_wait0();
+#pragma unroll
+  for (int i = 0; i < MAXT; ++i)
+#pragma unroll
+    for (int j = 0; j < MAXT; ++j) {
+      const int ti = tr0 + i, tj = tc0 + j;
+      if (i < tr_per && j < tc_per && ti < TR && tj < TC) {
+        const int row = ti * 8 + g, col = tj * 8 + 2 * t4;
+        out[(long long)row * RQ + col] = acc[i][j][0];
+        out[(long long)row * RQ + col + 1] = acc[i][j][1];
+      }
+    }
 }
 
 }  // namespace qdkp

@@ -17,11 +17,11 @@ namespace qdkp {
 int launch_apply(const qdkp_operator* op, const void* X, int64_t ldx, void* Y, int64_t ldy,
                  int m, double sigma, int shifted, int precision, cudaStream_t st);
 
-constexpr int kERowsPerCta = 2048;   // rows per CTA of the row kernels
+constexpr int kERowsPerCta = 512;    // rows per CTA of the row kernels
 constexpr int kENormRows = 2048;     // rows per CTA of the norm kernel
 constexpr int kEGramSplit = 16;
 
-enum GramWhich { GR_XR = 0, GR_RR, GR_PP, GR_WW, GR_WAW };
+enum GramWhich { GR_XR = 0, GR_RR, GR_PP, GR_WW, GR_WAW, GR_BA, GR_BB };
 enum UpdWhich { UP_RPROJ = 0, UP_RNORM, UP_PNORM, UP_APNORM, UP_PNEW, UP_APNEW, UP_XNEW, UP_AXNEW };
 enum RowWhich { RW_COPYBEST = 0, RW_RESID, RW_GATHERP };
 
@@ -173,7 +173,28 @@ __device__ bool gram_lists(const ESlot& d, int which, BlockList<double>& A, Bloc
     case GR_PP:
       if (st->skip_p) return false;
       set1(A, d.Pa, ma); set1(B, d.Pa, ma); out = d.G; return true;
-    default: {
+    case GR_BA:      // non-explicit: [X | R | P]^H [AR | AP]
+      if (st->explicit_gram) return false;
+      A.nblk = mp ? 3 : 2;
+      A.p[0] = d.X; A.ld[0] = m; A.cols[0] = m;
+      A.p[1] = d.Ra; A.ld[1] = ma; A.cols[1] = ma;
+      A.p[2] = d.Pa; A.ld[2] = ma; A.cols[2] = mp;
+      B.nblk = mp ? 2 : 1;
+      B.p[0] = d.ARa; B.ld[0] = ma; B.cols[0] = ma;
+      B.p[1] = d.APa; B.ld[1] = ma; B.cols[1] = mp;
+      out = d.gT;
+      return true;
+    case GR_BB:      // non-explicit: [X | R]^H P
+      if (st->explicit_gram || mp == 0) return false;
+      A.nblk = 2;
+      A.p[0] = d.X; A.ld[0] = m; A.cols[0] = m;
+      A.p[1] = d.Ra; A.ld[1] = ma; A.cols[1] = ma;
+      set1(B, d.Pa, mp);
+      B.ld[0] = ma;
+      out = d.gS;
+      return true;
+    default: {       // explicit Gram mode: the full W^H W and W^H AW
+      if (!st->explicit_gram) return false;
       A.nblk = mp ? 3 : 2;
       A.p[0] = d.X; A.ld[0] = m; A.cols[0] = m;
       A.p[1] = d.Ra; A.ld[1] = ma; A.cols[1] = ma;
@@ -199,70 +220,10 @@ e_gram_kernel(const ESlot* __restrict__ S, int ns, int which) {
   double2* out;
   if (!gram_lists(d, which, A, B, out)) return;
   const int part = blockIdx.x - d.gram0;
-  const int P = A.total(), Q = B.total();
-  const int RP = (2 * P + 7) / 8 * 8, RQ = (2 * Q + 7) / 8 * 8;
-  double* sA = gsm_e;
-  double* sB = gsm_e + kGramChunk * RP;
+  const int RP = (2 * A.total() + 7) / 8 * 8, RQ = (2 * B.total() + 7) / 8 * 8;
   const long long r0 = (long long)part * d.rows_per_gpart;
-  const long long r1 = min(d.n, r0 + d.rows_per_gpart);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int g = lane >> 2, t4 = lane & 3;
-  const int TR = RP / 8, TC = RQ / 8;
-  const int wr = warp / kGramWarpsC, wc = warp % kGramWarpsC;
-  const int tr_per = (TR + kGramWarpsR - 1) / kGramWarpsR, tc_per = (TC + kGramWarpsC - 1) / kGramWarpsC;
-  const int tr0 = wr * tr_per, tc0 = wc * tc_per;
-  double acc[MAXT][MAXT][2];
-#pragma unroll
-  for (int i = 0; i < MAXT; ++i)
-#pragma unroll
-    for (int j = 0; j < MAXT; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
-  for (long long rt = r0; rt < r1; rt += kGramChunk) {
-    for (int e = threadIdx.x; e < kGramChunk * (RP / 2); e += blockDim.x) {
-      const int row = e / (RP / 2), c = e - row * (RP / 2);
-      double2 z = make_double2(0.0, 0.0);
-      if (rt + row < r1 && c < P) z = list_elem(A, rt + row, c);
-      *reinterpret_cast<double2*>(&sA[row * RP + 2 * c]) = z;
-    }
-    for (int e = threadIdx.x; e < kGramChunk * (RQ / 2); e += blockDim.x) {
-      const int row = e / (RQ / 2), c = e - row * (RQ / 2);
-      double2 z = make_double2(0.0, 0.0);
-      if (rt + row < r1 && c < Q) z = list_elem(B, rt + row, c);
-      *reinterpret_cast<double2*>(&sB[row * RQ + 2 * c]) = z;
-    }
-    __syncthreads();
-#pragma unroll 2
-    for (int k0 = 0; k0 < kGramChunk; k0 += 4) {
-      double a[MAXT], b[MAXT];
-#pragma unroll
-      for (int i = 0; i < MAXT; ++i) {
-        const int ti = tr0 + i;
-        a[i] = (i < tr_per && ti < TR) ? sA[(k0 + t4) * RP + ti * 8 + g] : 0.0;
-      }
-#pragma unroll
-      for (int j = 0; j < MAXT; ++j) {
-        const int tj = tc0 + j;
-        b[j] = (j < tc_per && tj < TC) ? sB[(k0 + t4) * RQ + tj * 8 + g] : 0.0;
-      }
-#pragma unroll
-      for (int i = 0; i < MAXT; ++i)
-#pragma unroll
-        for (int j = 0; j < MAXT; ++j)
-          if (i < tr_per && j < tc_per) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
-    }
-    __syncthreads();
-  }
-  double* outp = d.gpart + (long long)part * RP * RQ;
-#pragma unroll
-  for (int i = 0; i < MAXT; ++i)
-#pragma unroll
-    for (int j = 0; j < MAXT; ++j) {
-      const int ti = tr0 + i, tj = tc0 + j;
-      if (i < tr_per && j < tc_per && ti < TR && tj < TC) {
-        const int row = ti * 8 + g, col = tj * 8 + 2 * t4;
-        outp[(long long)row * RQ + col] = acc[i][j][0];
-        outp[(long long)row * RQ + col + 1] = acc[i][j][1];
-      }
-    }
+  gram_core<MAXT>(A, B, r0, min(d.n, r0 + d.rows_per_gpart),
+                  d.gpart + (long long)part * RP * RQ, gsm_e);
 }
 
 __global__ void e_gram_reduce1(const ESlot* __restrict__ S, int which) {
@@ -400,15 +361,24 @@ __global__ void __launch_bounds__(kSmallThreads) e_pchol_kernel(const ESlot* __r
 // with the fall back to the two-block pencil when the three-block one is not definite.
 __device__ void e_assemble(const ESlot& d, const EState* st, int restart, int& dim) {
   const int m = d.m, ma = st->ma, mp = restart ? 0 : st->mp;
-  const int tot = m + st->ma + st->mp;      // layout of gS / gT
+  const int tot = m + st->ma + st->mp;      // rows of gT; layout of the explicit products
   dim = m + ma + mp;
   const bool ex = st->explicit_gram;
+  const int nAB = st->ma + st->mp;          // non-explicit gT = [X|R|P]^H [AR|AP]: tot x nAB
   for (int e = threadIdx.x; e < dim * dim; e += blockDim.x) {
     int i = e / dim, j = e - i * dim;
     bool lower = i > j;
     if (lower) { const int t = i; i = j; j = t; }
     const bool iX = i < m, iR = i >= m && i < m + ma, jX = j < m, jR = j >= m && j < m + ma;
-    const double2 Tij = d.gT[i * tot + j], Tji = d.gT[j * tot + i], Sij = d.gS[i * tot + j];
+    double2 Tij, Tji, Sij;
+    if (ex) {
+      Tij = d.gT[i * tot + j]; Tji = d.gT[j * tot + i]; Sij = d.gS[i * tot + j];
+    } else {
+      // column j >= m of W^H AW is column j - m of [AR | AP]; gS = [X|R]^H P (m+ma x mp)
+      Tij = j >= m ? d.gT[i * nAB + (j - m)] : make_double2(0.0, 0.0);
+      Tji = (i >= m && j >= m) ? d.gT[j * nAB + (i - m)] : make_double2(0.0, 0.0);
+      Sij = (j >= m + ma && i < m + ma) ? d.gS[i * st->mp + (j - m - ma)] : make_double2(0.0, 0.0);
+    }
     const double2 herm = make_double2(0.5 * (Tij.x + Tji.x), 0.5 * (Tij.y - Tji.y));
     double2 a, b;
     if (iX && jX) {
@@ -621,7 +591,7 @@ int rebuild(qdkp_engine* e, cudaStream_t st) {
 
 int launch_gram_multi(qdkp_engine* e, int which, cudaStream_t st) {
   const int RP = (6 * e->m_max + 7) / 8 * 8;
-  const size_t smem = (size_t)kGramChunk * 2 * RP * sizeof(double);
+  const size_t smem = (size_t)2 * kGramChunk * 2 * RP * sizeof(double);
   switch (e->maxT) {
     case 2: e_gram_kernel<2><<<e->gram_ctas, kGramThreads, smem, st>>>(e->d_slots, e->ns, which); break;
     case 3: e_gram_kernel<3><<<e->gram_ctas, kGramThreads, smem, st>>>(e->d_slots, e->ns, which); break;
@@ -640,7 +610,7 @@ int launch_gram_multi(qdkp_engine* e, int which, cudaStream_t st) {
 int launch_update_multi(qdkp_engine* e, int which, cudaStream_t st) {
   const int P = 2 * e->m_max;
   const int KPp = (2 * P + 3) / 4 * 4, NQ = (2 * e->m_max + 7) / 8 * 8;
-  const size_t smem = ((size_t)KPp * NQ + (size_t)kUpdRows * (KPp + 1)) * sizeof(double);
+  const size_t smem = ((size_t)KPp * NQ + (size_t)kUpdWarps * kUpdRows * (KPp + 2)) * sizeof(double);
   e_update_kernel<<<e->row_ctas, kUpdThreads, smem, st>>>(e->d_slots, e->ns, which);
   count_launch();
   QDKP_CUDA_TRY(cudaGetLastError());
@@ -677,6 +647,8 @@ int tick(qdkp_engine* e, cudaStream_t st) {
   count_launch();
   ETRY(launch_update_multi(e, UP_PNORM, st));
   ETRY(launch_update_multi(e, UP_APNORM, st));
+  ETRY(launch_gram_multi(e, GR_BA, st));
+  ETRY(launch_gram_multi(e, GR_BB, st));
   ETRY(launch_gram_multi(e, GR_WW, st));
   ETRY(launch_gram_multi(e, GR_WAW, st));
   e_rr_kernel<<<ns, kSmallThreads, rr_smem, st>>>(e->d_slots);

@@ -401,12 +401,34 @@ int qdkp_lobpcg_solve(const qdkp_operator* op, const qdkp_lobpcg_params* prm, co
     BlockList<double> AWl = mp ? blist({{b.AX, m}, {b.ARa, ma}, {b.APa, mp}})
                                : blist({{b.AX, m}, {b.ARa, ma}});
     AWl.ld[0] = m; AWl.ld[1] = ma; if (mp) AWl.ld[2] = mp;
-    TRY(s.gram(Wl, Wl, b.gS));
-    TRY(s.gram(Wl, AWl, b.gT));
-    hS.resize((size_t)tot * tot);
-    hT.resize((size_t)tot * tot);
-    TRY(s.sync_read(hS.data(), b.gS, hS.size() * sizeof(double2)));
-    TRY(s.sync_read(hT.data(), b.gT, hT.size() * sizeof(double2)));
+    hS.assign((size_t)tot * tot, make_double2(0.0, 0.0));
+    hT.assign((size_t)tot * tot, make_double2(0.0, 0.0));
+    if (explicit_gram) {
+      TRY(s.gram(Wl, Wl, b.gS));
+      TRY(s.gram(Wl, AWl, b.gT));
+      TRY(s.sync_read(hS.data(), b.gS, hS.size() * sizeof(double2)));
+      TRY(s.sync_read(hT.data(), b.gT, hT.size() * sizeof(double2)));
+    } else {
+      // only the blocks the non-explicit pencils read (lobpcg.py:856-861): [X|R|P]^H [AR|AP]
+      // and [X|R]^H P, scattered into the full W^H AW / W^H W layouts
+      const int nAB = ma + mp;
+      BlockList<double> ABl = mp ? blist({{b.ARa, ma}, {b.APa, mp}}) : blist({{b.ARa, ma}});
+      ABl.ld[0] = ma; if (mp) ABl.ld[1] = ma;
+      TRY(s.gram(Wl, ABl, b.gT));
+      std::vector<double2> t2((size_t)tot * nAB);
+      TRY(s.sync_read(t2.data(), b.gT, t2.size() * sizeof(double2)));
+      for (int i = 0; i < tot; ++i)
+        for (int c = 0; c < nAB; ++c) hT[(size_t)i * tot + m + c] = t2[(size_t)i * nAB + c];
+      if (mp) {
+        BlockList<double> XR = blist({{b.X, m}, {b.Ra, ma}});
+        XR.ld[0] = m; XR.ld[1] = ma;
+        TRY(s.gram(XR, blist({{b.Pa, mp}}, ma), b.gS));
+        std::vector<double2> s2((size_t)(m + ma) * mp);
+        TRY(s.sync_read(s2.data(), b.gS, s2.size() * sizeof(double2)));
+        for (int i = 0; i < m + ma; ++i)
+          for (int c = 0; c < mp; ++c) hS[(size_t)i * tot + m + ma + c] = s2[(size_t)i * mp + c];
+      }
+    }
     int dim = 0;
     bool solved = false;
     std::vector<double> w(tot);
