@@ -143,15 +143,15 @@ constexpr int kGramParts = 296;
 // f64 kind). A CTA of 3 x 3 warps owns all 8x8 tiles of C' for its slice of rows; each warp
 // owns a rectangle of up to 6 x 6 tiles and keeps them in registers across the slice.
 
-template <int MAXT>
-__global__ void __launch_bounds__(kGramThreads)
+template <int MR, int MC>
+__global__ void __launch_bounds__(512)
 gram_partial_kernel(const BlockList<double> A, const BlockList<double> B, long long n,
                     long long rows_per_part, double* __restrict__ partial) {
   extern __shared__ double gsm_d[];
   const int RP = (2 * A.total() + 7) / 8 * 8, RQ = (2 * B.total() + 7) / 8 * 8;
   const long long r0 = blockIdx.x * rows_per_part;
-  gram_core<MAXT>(A, B, r0, min(n, r0 + rows_per_part),
-                  partial + (long long)blockIdx.x * RP * RQ, gsm_d);
+  gram_core<MR, MC>(A, B, r0, min(n, r0 + rows_per_part),
+                    partial + (long long)blockIdx.x * RP * RQ, gsm_d);
 }
 
 // Stage 1: column-block sums of the partial C' slices (coalesced over the RP x RQ elements);
@@ -202,30 +202,28 @@ int launch_gram(const BlockList<double>& A, const BlockList<double>& B, long lon
   if (parts > kGramParts) parts = kGramParts;
   if (parts < 1) parts = 1;
   long long rpp = (n + parts - 1) / parts;
-  rpp = (rpp + kGramChunk - 1) / kGramChunk * kGramChunk;
+  rpp = (rpp + 3) / 4 * 4;
   parts = (n + rpp - 1) / rpp;
   if ((size_t)(parts + kGramSplit) * RP * RQ > 2 * partial_elems) {
     set_error("gram partial buffer too small");
     return QDKP_ERR_WORKSPACE;
   }
-  const size_t smem = (size_t)2 * kGramChunk * (RP + RQ) * sizeof(double);
+  const size_t smem = (size_t)RP * RQ * sizeof(double);
   static bool attr = false;
   if (!attr) {
     const int big = 200 * 1024;
-    cudaFuncSetAttribute(gram_partial_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-    cudaFuncSetAttribute(gram_partial_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-    cudaFuncSetAttribute(gram_partial_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-    cudaFuncSetAttribute(gram_partial_kernel<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    cudaFuncSetAttribute(gram_partial_kernel<3, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    cudaFuncSetAttribute(gram_partial_kernel<3, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    cudaFuncSetAttribute(gram_partial_kernel<6, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
     attr = true;
   }
-  const int TR = RP / 8, TC = RQ / 8;
-  const int tmax = std::max((TR + kGramWarpsR - 1) / kGramWarpsR, (TC + kGramWarpsC - 1) / kGramWarpsC);
+  int MR, MC, threads;
+  gram_shape(P, Q, MR, MC, threads);
   double* pd = reinterpret_cast<double*>(partial);
   const unsigned grid = (unsigned)parts;
-  if (tmax <= 2) gram_partial_kernel<2><<<grid, kGramThreads, smem, st>>>(A, B, n, rpp, pd);
-  else if (tmax <= 3) gram_partial_kernel<3><<<grid, kGramThreads, smem, st>>>(A, B, n, rpp, pd);
-  else if (tmax <= 4) gram_partial_kernel<4><<<grid, kGramThreads, smem, st>>>(A, B, n, rpp, pd);
-  else gram_partial_kernel<6><<<grid, kGramThreads, smem, st>>>(A, B, n, rpp, pd);
+  if (MR == 3 && MC == 3) gram_partial_kernel<3, 3><<<grid, threads, smem, st>>>(A, B, n, rpp, pd);
+  else if (MR == 3) gram_partial_kernel<3, 6><<<grid, threads, smem, st>>>(A, B, n, rpp, pd);
+  else gram_partial_kernel<6, 6><<<grid, threads, smem, st>>>(A, B, n, rpp, pd);
   count_launch();
   const int elems = RP * RQ;
   double* part2 = pd + (size_t)parts * elems;
@@ -261,7 +259,7 @@ int launch_update(const BlockList<double>& A, const double2* const* C, int q, lo
   for (int b = 0; b < 3; ++b) cl.c[b] = b < A.nblk ? C[b] : nullptr;
   const int P = A.total();
   const int KPp = (2 * P + 3) / 4 * 4, NQ = (2 * q + 7) / 8 * 8;
-  const size_t smem = ((size_t)KPp * NQ + (size_t)kUpdWarps * kUpdRows * (KPp + 2)) * sizeof(double);
+  const size_t smem = ((size_t)KPp * NQ + (size_t)4 * NQ) * sizeof(double);
   static bool attr = false;
   if (!attr) {
     QDKP_CUDA_TRY(cudaFuncSetAttribute(update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,

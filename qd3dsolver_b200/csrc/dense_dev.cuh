@@ -162,16 +162,6 @@ static __device__ void block_jacobi(double2* C, double2* V, int n) {
         C[p * n + j] = np; C[q * n + j] = nq;
       }
       __syncthreads();
-      if (threadIdx.x < npair) {
-        const int k = threadIdx.x, p = rp[k], q = rq[k];
-        if (q < n && rsn[k] != 0.0) {
-          C[p * n + q] = make_double2(0.0, 0.0);
-          C[q * n + p] = make_double2(0.0, 0.0);
-          C[p * n + p].y = 0.0;
-          C[q * n + q].y = 0.0;
-        }
-      }
-      __syncthreads();
     }
     if (!rotated) break;
     __syncthreads();
@@ -281,8 +271,8 @@ constexpr int kUpdThreads = 256;
 constexpr int kUpdWarps = kUpdThreads / 32;
 
 static __device__ __forceinline__ size_t update_smem_doubles(int P, int q) {
-  const int KPp = (2 * P + 3) / 4 * 4, NQ = (2 * q + 7) / 8 * 8;
-  return (size_t)KPp * NQ + (size_t)kUpdWarps * kUpdRows * (KPp + 2);
+  const int KPp = (2 * P + 3) / 4 * 4 + 4, NQ = (2 * q + 7) / 8 * 8;
+  return (size_t)KPp * NQ;
 }
 
 static __device__ void update_rows(const BlockList<double>& A, const double2* const* C, int q,
@@ -292,15 +282,14 @@ static __device__ void update_rows(const BlockList<double>& A, const double2* co
   const int KP = 2 * P;
   const int KPp = (KP + 3) / 4 * 4;
   const int NQ = (2 * q + 7) / 8 * 8;
-  const int lda_s = KPp + 2;             // even: 16-byte aligned double2 stores
   double* sC = usm;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  double* sA = usm + KPp * NQ + (size_t)warp * kUpdRows * lda_s;
   const double sg = neg ? -1.0 : 1.0;
   int off[3];
   int tot = 0;
   for (int b = 0; b < A.nblk; ++b) { off[b] = tot; tot += A.cols[b]; }
-  for (int e = threadIdx.x; e < KPp * NQ; e += blockDim.x) sC[e] = 0.0;
+  // KPp + 4 rows: a k step may run up to 3 rows past the last block (multiplied by zeros)
+  for (int e = threadIdx.x; e < (KPp + 4) * NQ; e += blockDim.x) sC[e] = 0.0;
   __syncthreads();
   for (int e = threadIdx.x; e < P * q; e += blockDim.x) {
     const int i = e / q, j = e - i * q;
@@ -312,156 +301,171 @@ static __device__ void update_rows(const BlockList<double>& A, const double2* co
     sC[(2 * i + 1) * NQ + 2 * j] = -sg * c.y;
     sC[(2 * i + 1) * NQ + 2 * j + 1] = sg * c.x;
   }
-  for (int e = lane; e < kUpdRows * (KPp - KP); e += 32) {
-    const int row = e / (KPp - KP), c = e - row * (KPp - KP);
-    sA[row * lda_s + KP + c] = 0.0;
-  }
   __syncthreads();
   const int g = lane >> 2, t4 = lane & 3;
   const int NT = NQ / 8;
   for (long long rb = r0 + (long long)warp * kUpdRows; rb < r1;
        rb += (long long)kUpdWarps * kUpdRows) {
-    for (int b = 0; b < A.nblk; ++b) {
-      const int cb = A.cols[b];
-      const double2* __restrict__ src = A.p[b];
-      const long long ld = A.ld[b];
-      for (int e = lane; e < kUpdRows * cb; e += 32) {
-        const int row = e / cb, c = e - row * cb;
-        double2 z = make_double2(0.0, 0.0);
-        if (rb + row < r1) z = src[(rb + row) * ld + c];
-        *reinterpret_cast<double2*>(&sA[row * lda_s + 2 * (off[b] + c)]) = z;
-      }
-    }
-    __syncwarp();
     const long long rowg = rb + g;
+    const bool rok = rowg < r1;
     double acc[6][2];
 #pragma unroll
     for (int j = 0; j < 6; ++j) {
       const int col = j * 4 + t4;
       double2 y0 = make_double2(0.0, 0.0);
-      if (accumulate && j < NT && col < q && rowg < r1) y0 = Y[rowg * ldy + col];
+      if (accumulate && j < NT && col < q && rok) y0 = Y[rowg * ldy + col];
       acc[j][0] = y0.x; acc[j][1] = y0.y;
     }
-    for (int k0 = 0; k0 < KPp; k0 += 4) {
-      const double a = sA[g * lda_s + k0 + t4];
+    // A fragment of an m8n8k4 MMA: lane (g, t4) holds A'[row g][k0 + t4], i.e. the real or
+    // imaginary part of one complex element of its row -- read straight from global memory.
+    int kbase = 0;
+    for (int b = 0; b < A.nblk; ++b) {
+      const double* __restrict__ src =
+          reinterpret_cast<const double*>(A.p[b]) + (rok ? rowg : rb) * 2 * A.ld[b];
+      const int kb = 2 * A.cols[b];
+      for (int k = 0; k < kb; k += 4) {
+        const double a = (rok && k + t4 < kb) ? src[k + t4] : 0.0;
+        const int kr = kbase + k + t4 - t4;   // row block of C'' for this k step
 #pragma unroll
-      for (int j = 0; j < 6; ++j) {
-        if (j < NT) dmma(acc[j][0], acc[j][1], a, sC[(k0 + t4) * NQ + j * 8 + g]);
+        for (int j = 0; j < 6; ++j)
+          if (j < NT) dmma(acc[j][0], acc[j][1], a, sC[(kr + t4) * NQ + j * 8 + g]);
       }
+      kbase += kb;
     }
 #pragma unroll
     for (int j = 0; j < 6; ++j) {
       const int col = j * 4 + t4;
-      if (j < NT && col < q && rowg < r1) Y[rowg * ldy + col] = make_double2(acc[j][0], acc[j][1]);
+      if (j < NT && col < q && rok) Y[rowg * ldy + col] = make_double2(acc[j][0], acc[j][1]);
     }
-    __syncwarp();
   }
 }
 
 // ---------------------------------------------------------------------------------------------
-// Gram core: partial C' = A'^T B' (real views) of rows [r0, r1) on the FP64 MMA units.
-// Rows are staged in chunks of kGramChunk through a two-stage cp.async pipeline (16-byte copies
-// of complex elements straight into the real-view layout), so the next chunk loads while the
-// current one is multiplied. Writes the RP x RQ partial (row-major) to `out`.
+// Gram core: partial C' = A'^T B' (real views: row r, column 2c + {re, im}) of rows [r0, r1) on
+// the FP64 MMA units. Each warp owns a rectangle of MR x MC 8x8 tiles of C' and a slice of the
+// rows; it loads its m8n8k4 fragments straight from global memory (lane (g, t4) of a k step
+// reads row k0 + t4, real column 8 tile + g: eight lanes cover 64 contiguous bytes) and keeps
+// its tiles in registers, so the row loop has no barrier. The row slices of a tile rectangle are
+// summed in shared memory in a fixed order at the end (deterministic), giving one RP x RQ
+// partial per CTA.
 // ---------------------------------------------------------------------------------------------
-static __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" :: "r"(s), "l"(gmem));
-}
-static __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-static __device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::); }
-static __device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;\n" ::); }
-
-static __device__ __forceinline__ void gram_stage(const BlockList<double>& L, int P, int RP,
-                                                  long long rt, long long r1, double* buf) {
-  for (int e = threadIdx.x; e < kGramChunk * (RP / 2); e += blockDim.x) {
-    const int row = e / (RP / 2), c = e - row * (RP / 2);
-    double* dst = &buf[row * RP + 2 * c];
-    if (rt + row < r1 && c < P) {
-      int b = 0, cc = c;
-      while (b < L.nblk - 1 && cc >= L.cols[b]) { cc -= L.cols[b]; ++b; }
-      cp_async16(dst, L.p[b] + (rt + row) * L.ld[b] + cc);
-    } else {
-      *reinterpret_cast<double2*>(dst) = make_double2(0.0, 0.0);
-    }
-  }
-}
+constexpr int kGramCtaThreads = 256;
 
 static __device__ __forceinline__ size_t gram_smem_bytes(int P, int Q) {
   const int RP = (2 * P + 7) / 8 * 8, RQ = (2 * Q + 7) / 8 * 8;
-  return (size_t)2 * kGramChunk * (RP + RQ) * sizeof(double);
+  return (size_t)RP * RQ * sizeof(double);
 }
 
-template <int MAXT>
+// tile rectangles: tile rows split in groups of MR, tile columns in groups of MC
+template <int MR, int MC>
 static __device__ void gram_core(const BlockList<double>& A, const BlockList<double>& B,
                                  long long r0, long long r1, double* __restrict__ out,
                                  double* gsm) {
   const int P = A.total(), Q = B.total();
   const int RP = (2 * P + 7) / 8 * 8, RQ = (2 * Q + 7) / 8 * 8;
-  double* sA[2] = {gsm, gsm + kGramChunk * RP};
-  double* sB[2] = {gsm + 2 * kGramChunk * RP, gsm + 2 * kGramChunk * RP + kGramChunk * RQ};
+  const int TR = RP / 8, TC = RQ / 8;
+  const int GR = (TR + MR - 1) / MR, GC = (TC + MC - 1) / MC;
+  const int G = GR * GC;                          // tile rectangles (<= 8 by construction)
+  const int nwarps = blockDim.x >> 5;
+  const int slices = nwarps / G;                  // warps per rectangle
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int g = lane >> 2, t4 = lane & 3;
-  const int TR = RP / 8, TC = RQ / 8;
-  const int wr = warp / kGramWarpsC, wc = warp % kGramWarpsC;
-  const int tr_per = (TR + kGramWarpsR - 1) / kGramWarpsR, tc_per = (TC + kGramWarpsC - 1) / kGramWarpsC;
-  const int tr0 = wr * tr_per, tc0 = wc * tc_per;
-  double acc[MAXT][MAXT][2];
+  const int rect = warp % G, slice = warp / G;
+  const bool active_warp = slice < slices;
+  const int tr0 = (rect / GC) * MR, tc0 = (rect % GC) * MC;
+  // per tile: block index (-1: outside P / Q) and the real column inside that block's row
+  int ba[MR], ca[MR], bb[MC], cb[MC];
 #pragma unroll
-  for (int i = 0; i < MAXT; ++i)
-#pragma unroll
-    for (int j = 0; j < MAXT; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
-  const int nchunks = r1 > r0 ? (int)((r1 - r0 + kGramChunk - 1) / kGramChunk) : 0;
-  if (nchunks > 0) {
-    gram_stage(A, P, RP, r0, r1, sA[0]);
-    gram_stage(B, Q, RQ, r0, r1, sB[0]);
+  for (int i = 0; i < MR; ++i) {
+    const int col = (tr0 + i) * 8 + g;           // real column of A'
+    int c = col >> 1, blk = 0;
+    while (blk < A.nblk - 1 && c >= A.cols[blk]) { c -= A.cols[blk]; ++blk; }
+    const bool ok = active_warp && tr0 + i < TR && col < 2 * P;
+    ba[i] = ok ? blk : -1;
+    ca[i] = 2 * c + (col & 1);
   }
-  cp_async_commit();
-  for (int ch = 0; ch < nchunks; ++ch) {
-    const int cur = ch & 1;
-    if (ch + 1 < nchunks) {
-      const long long rn = r0 + (long long)(ch + 1) * kGramChunk;
-      gram_stage(A, P, RP, rn, r1, sA[cur ^ 1]);
-      gram_stage(B, Q, RQ, rn, r1, sB[cur ^ 1]);
-    }
-    cp_async_commit();
-    cp_async_wait1();
-    __syncthreads();
-    const double* a_s = sA[cur];
-    const double* b_s = sB[cur];
+#pragma unroll
+  for (int j = 0; j < MC; ++j) {
+    const int col = (tc0 + j) * 8 + g;
+    int c = col >> 1, blk = 0;
+    while (blk < B.nblk - 1 && c >= B.cols[blk]) { c -= B.cols[blk]; ++blk; }
+    const bool ok = active_warp && tc0 + j < TC && col < 2 * Q;
+    bb[j] = ok ? blk : -1;
+    cb[j] = 2 * c + (col & 1);
+  }
+  const double* A0 = reinterpret_cast<const double*>(A.p[0]);
+  const double* A1 = reinterpret_cast<const double*>(A.nblk > 1 ? A.p[1] : A.p[0]);
+  const double* A2 = reinterpret_cast<const double*>(A.nblk > 2 ? A.p[2] : A.p[0]);
+  const double* B0 = reinterpret_cast<const double*>(B.p[0]);
+  const double* B1 = reinterpret_cast<const double*>(B.nblk > 1 ? B.p[1] : B.p[0]);
+  const double* B2 = reinterpret_cast<const double*>(B.nblk > 2 ? B.p[2] : B.p[0]);
+  const long long la0 = 2 * A.ld[0], la1 = A.nblk > 1 ? 2 * A.ld[1] : 0, la2 = A.nblk > 2 ? 2 * A.ld[2] : 0;
+  const long long lb0 = 2 * B.ld[0], lb1 = B.nblk > 1 ? 2 * B.ld[1] : 0, lb2 = B.nblk > 2 ? 2 * B.ld[2] : 0;
+  double acc[MR][MC][2];
+#pragma unroll
+  for (int i = 0; i < MR; ++i)
+#pragma unroll
+    for (int j = 0; j < MC; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+  if (active_warp) {
 #pragma unroll 2
-    for (int k0 = 0; k0 < kGramChunk; k0 += 4) {
-      double a[MAXT], b[MAXT];
+    for (long long k0 = r0 + 4LL * slice; k0 < r1; k0 += 4LL * slices) {
+      const long long row = k0 + t4;
+      const bool ok = row < r1;
+      const double* ra0 = A0 + row * la0;
+      const double* ra1 = A1 + row * la1;
+      const double* ra2 = A2 + row * la2;
+      const double* rb0 = B0 + row * lb0;
+      const double* rb1 = B1 + row * lb1;
+      const double* rb2 = B2 + row * lb2;
+      double a[MR], b[MC];
 #pragma unroll
-      for (int i = 0; i < MAXT; ++i) {
-        const int ti = tr0 + i;
-        a[i] = (i < tr_per && ti < TR) ? a_s[(k0 + t4) * RP + ti * 8 + g] : 0.0;
+      for (int i = 0; i < MR; ++i) {
+        const double* base = ba[i] == 0 ? ra0 : (ba[i] == 1 ? ra1 : ra2);
+        a[i] = (ok && ba[i] >= 0) ? __ldg(base + ca[i]) : 0.0;
       }
 #pragma unroll
-      for (int j = 0; j < MAXT; ++j) {
-        const int tj = tc0 + j;
-        b[j] = (j < tc_per && tj < TC) ? b_s[(k0 + t4) * RQ + tj * 8 + g] : 0.0;
+      for (int j = 0; j < MC; ++j) {
+        const double* base = bb[j] == 0 ? rb0 : (bb[j] == 1 ? rb1 : rb2);
+        b[j] = (ok && bb[j] >= 0) ? __ldg(base + cb[j]) : 0.0;
       }
 #pragma unroll
-      for (int i = 0; i < MAXT; ++i)
+      for (int i = 0; i < MR; ++i)
 #pragma unroll
-        for (int j = 0; j < MAXT; ++j)
-          if (i < tr_per && j < tc_per) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+        for (int j = 0; j < MC; ++j) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+    }
+  }
+  // fixed-order sum of the row slices of each rectangle
+  for (int e = threadIdx.x; e < RP * RQ; e += blockDim.x) gsm[e] = 0.0;
+  __syncthreads();
+  for (int sl = 0; sl < slices; ++sl) {
+    if (active_warp && slice == sl) {
+#pragma unroll
+      for (int i = 0; i < MR; ++i)
+#pragma unroll
+        for (int j = 0; j < MC; ++j) {
+          const int ti = tr0 + i, tj = tc0 + j;
+          if (ti < TR && tj < TC) {
+            const int rr = ti * 8 + g, cc = tj * 8 + 2 * t4;
+            gsm[rr * RQ + cc] += acc[i][j][0];
+            gsm[rr * RQ + cc + 1] += acc[i][j][1];
+          }
+        }
     }
     __syncthreads();
   }
-  cp_async_wait0();
-#pragma unroll
-  for (int i = 0; i < MAXT; ++i)
-#pragma unroll
-    for (int j = 0; j < MAXT; ++j) {
-      const int ti = tr0 + i, tj = tc0 + j;
-      if (i < tr_per && j < tc_per && ti < TR && tj < TC) {
-        const int row = ti * 8 + g, col = tj * 8 + 2 * t4;
-        out[(long long)row * RQ + col] = acc[i][j][0];
-        out[(long long)row * RQ + col + 1] = acc[i][j][1];
-      }
+  for (int e = threadIdx.x; e < RP * RQ; e += blockDim.x) out[e] = gsm[e];
+}
+
+// (MR, MC, threads) for a product: the smallest tile rectangles that fit 8 warps, else 16.
+static inline void gram_shape(int P, int Q, int& MR, int& MC, int& threads) {
+  const int TR = ((2 * P + 7) / 8 * 8) / 8, TC = ((2 * Q + 7) / 8 * 8) / 8;
+  const int cand[3][2] = {{3, 3}, {3, 6}, {6, 6}};
+  for (int lim : {8, 16})
+    for (auto& c : cand) {
+      const int G = ((TR + c[0] - 1) / c[0]) * ((TC + c[1] - 1) / c[1]);
+      if (G <= lim) { MR = c[0]; MC = c[1]; threads = 32 * lim; return; }
     }
+  MR = MC = 6; threads = 512;
 }
 
 }  // namespace qdkp

@@ -210,20 +210,23 @@ __device__ bool gram_lists(const ESlot& d, int which, BlockList<double>& A, Bloc
   }
 }
 
-template <int MAXT>
-__global__ void __launch_bounds__(kGramThreads)
-e_gram_kernel(const ESlot* __restrict__ S, int ns, int which) {
+// Launched once per distinct block width m present: the tile shape (and so the order of every
+// sum) then depends only on the slot's own sizes, never on which other solves share the batch.
+template <int MR, int MC>
+__global__ void __launch_bounds__(512)
+e_gram_kernel(const ESlot* __restrict__ S, int ns, int which, int m_only) {
   extern __shared__ double gsm_e[];
   const int k = slot_of(S, ns, blockIdx.x, &ESlot::gram0);
   const ESlot& d = S[k];
+  if (d.m != m_only) return;
   BlockList<double> A, B;
   double2* out;
   if (!gram_lists(d, which, A, B, out)) return;
   const int part = blockIdx.x - d.gram0;
   const int RP = (2 * A.total() + 7) / 8 * 8, RQ = (2 * B.total() + 7) / 8 * 8;
   const long long r0 = (long long)part * d.rows_per_gpart;
-  gram_core<MAXT>(A, B, r0, min(d.n, r0 + d.rows_per_gpart),
-                  d.gpart + (long long)part * RP * RQ, gsm_e);
+  gram_core<MR, MC>(A, B, r0, min(d.n, r0 + d.rows_per_gpart),
+                    d.gpart + (long long)part * RP * RQ, gsm_e);
 }
 
 __global__ void e_gram_reduce1(const ESlot* __restrict__ S, int which) {
@@ -469,7 +472,7 @@ SlotLayout slot_layout(int64_t n, int m) {
   if (parts > 296) parts = 296;
   if (parts < 1) parts = 1;
   long long rpp = (n + parts - 1) / parts;
-  rpp = (rpp + kGramChunk - 1) / kGramChunk * kGramChunk;
+  rpp = (rpp + 3) / 4 * 4;
   L.gparts = (int)((n + rpp - 1) / rpp);
   L.rows_per_gpart = rpp;
   const size_t RP = (6 * m + 7) / 8 * 8;
@@ -492,6 +495,7 @@ struct qdkp_engine {
   std::vector<int> order;              // slot ids in compact order
   int ns = 0, norm_ctas = 0, gram_ctas = 0, row_ctas = 0, hx_tiles = 0, S_max = 32;
   int maxT = 2, m_max = 1;
+  std::vector<int> widths;             // distinct block widths among the used slots
   bool dirty = true;
 };
 
@@ -575,6 +579,10 @@ int rebuild(qdkp_engine* e, cudaStream_t st) {
   e->ns = (int)compact.size();
   e->norm_ctas = norm0; e->gram_ctas = gram0; e->row_ctas = row0; e->hx_tiles = tile0;
   e->S_max = S_max; e->m_max = m_max;
+  e->widths.clear();
+  for (const ESlot& d : compact)
+    if (std::find(e->widths.begin(), e->widths.end(), d.m) == e->widths.end()) e->widths.push_back(d.m);
+  std::sort(e->widths.begin(), e->widths.end());
   const int RP = (6 * m_max + 7) / 8 * 8;
   const int TR = RP / 8;
   const int tper = (TR + kGramWarpsR - 1) / kGramWarpsR;
@@ -590,19 +598,25 @@ int rebuild(qdkp_engine* e, cudaStream_t st) {
 }
 
 int launch_gram_multi(qdkp_engine* e, int which, cudaStream_t st) {
-  const int RP = (6 * e->m_max + 7) / 8 * 8;
-  const size_t smem = (size_t)2 * kGramChunk * 2 * RP * sizeof(double);
-  switch (e->maxT) {
-    case 2: e_gram_kernel<2><<<e->gram_ctas, kGramThreads, smem, st>>>(e->d_slots, e->ns, which); break;
-    case 3: e_gram_kernel<3><<<e->gram_ctas, kGramThreads, smem, st>>>(e->d_slots, e->ns, which); break;
-    case 4: e_gram_kernel<4><<<e->gram_ctas, kGramThreads, smem, st>>>(e->d_slots, e->ns, which); break;
-    default: e_gram_kernel<6><<<e->gram_ctas, kGramThreads, smem, st>>>(e->d_slots, e->ns, which); break;
+  for (int m : e->widths) {
+    int P = m, Q = m;
+    if (which == GR_BA) { P = 3 * m; Q = 2 * m; }
+    else if (which == GR_BB) { P = 2 * m; Q = m; }
+    else if (which == GR_WW || which == GR_WAW) { P = 3 * m; Q = 3 * m; }
+    const size_t smem = (size_t)((2 * P + 7) / 8 * 8) * ((2 * Q + 7) / 8 * 8) * sizeof(double);
+    int MR, MC, threads;
+    gram_shape(P, Q, MR, MC, threads);
+    if (MR == 3 && MC == 3) e_gram_kernel<3, 3><<<e->gram_ctas, threads, smem, st>>>(e->d_slots, e->ns, which, m);
+    else if (MR == 3) e_gram_kernel<3, 6><<<e->gram_ctas, threads, smem, st>>>(e->d_slots, e->ns, which, m);
+    else e_gram_kernel<6, 6><<<e->gram_ctas, threads, smem, st>>>(e->d_slots, e->ns, which, m);
+    count_launch();
   }
+  const int RP = (6 * e->m_max + 7) / 8 * 8;
   const int elems = RP * RP;
   e_gram_reduce1<<<dim3((elems + 255) / 256, kEGramSplit, e->ns), 256, 0, st>>>(e->d_slots, which);
   const int pq = (3 * e->m_max) * (3 * e->m_max);
   e_gram_reduce2<<<dim3((pq + 127) / 128, e->ns), 128, 0, st>>>(e->d_slots, which);
-  count_launch(3);
+  count_launch(2);
   QDKP_CUDA_TRY(cudaGetLastError());
   return QDKP_OK;
 }
@@ -610,7 +624,7 @@ int launch_gram_multi(qdkp_engine* e, int which, cudaStream_t st) {
 int launch_update_multi(qdkp_engine* e, int which, cudaStream_t st) {
   const int P = 2 * e->m_max;
   const int KPp = (2 * P + 3) / 4 * 4, NQ = (2 * e->m_max + 7) / 8 * 8;
-  const size_t smem = ((size_t)KPp * NQ + (size_t)kUpdWarps * kUpdRows * (KPp + 2)) * sizeof(double);
+  const size_t smem = ((size_t)KPp * NQ + (size_t)4 * NQ) * sizeof(double);
   e_update_kernel<<<e->row_ctas, kUpdThreads, smem, st>>>(e->d_slots, e->ns, which);
   count_launch();
   QDKP_CUDA_TRY(cudaGetLastError());
@@ -688,10 +702,9 @@ int qdkp_engine_create(int max_slots, int device, qdkp_engine** out) {
   }
   // dynamic shared memory limits of the engine kernels
   const int big = 200 * 1024;
-  cudaFuncSetAttribute(e_gram_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-  cudaFuncSetAttribute(e_gram_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-  cudaFuncSetAttribute(e_gram_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-  cudaFuncSetAttribute(e_gram_kernel<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+  cudaFuncSetAttribute(e_gram_kernel<3, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+  cudaFuncSetAttribute(e_gram_kernel<3, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+  cudaFuncSetAttribute(e_gram_kernel<6, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
   cudaFuncSetAttribute(e_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
   cudaFuncSetAttribute(e_rr_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
   cudaFuncSetAttribute(e_rchol_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
