@@ -243,12 +243,7 @@ def run_ours(args):
     total_ms = sum(r['ms'] for r in steps)
     pairs = sum(r['pairs'] for r in steps)
     if ws > 1:
-        import torch.distributed as dist
-        t = torch.tensor([total_ms, pairs], dtype=torch.float64, device=device)
-        tmax = t.clone()
-        dist.all_reduce(tmax[:1], op=dist.ReduceOp.MAX)
-        dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
-        total_ms, pairs = float(tmax[0]), float(t[1])
+        total_ms, pairs = combine_ranks(total_ms, pairs, device)
     value = pairs / (total_ms * 1e-3)
     lat = sorted(x for r in steps for x in r['lat'])
     hx_s = sum(r['hx_s'] for r in steps)
@@ -256,7 +251,7 @@ def run_ours(args):
     hx_n = sum(r['hx_n'] for r in steps)
 
     plain = None
-    if args.form == 'served' and rank == 0:
+    if args.form == 'served' and rank == 0 and not args.no_plain:
         # the plain c128 single-solve form on the same 14 solves, and its H.X launch timings
         torch.cuda.synchronize(device)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -271,27 +266,54 @@ def run_ours(args):
                                'p99': sorted(rp['lat'])[-1]}}
         hx_s, hx_b, hx_n = rp['hx_s'], rp['hx_b'], rp['hx_n']
 
-    # ---- e2e: the public API with host buffers (fields and X0 up, E and V down) --------------
+    # ---- e2e: the public API with host buffers (fields and X0 up, E and V down) -------------
     e2e = None
-    if rank == 0:
+    if rank == 0 and not args.no_e2e:
         torch.cuda.synchronize(device)
         h2d = d2h = 0
         t0 = time.perf_counter()
         e2e_pairs = 0
-        for w in wls:
-            H = make_operator(w)                       # uploads the 15 fields from the host
-            h2d += 15 * w.n_sites * 8
-            for band in BANDS:
-                E, V, info = eg.solve_interior(H, k=K, sigma=w.sigma[band], tol=TOL,
-                                               maxiter=MAXITER, verbose=False)   # X0 host->dev
-                h2d += H.shape[0] * BLOCK * 16
-                d2h += V.nbytes + E.nbytes
-                e2e_pairs += int((info['residuals'] <= RES_TOL).sum())
+        hops = [make_operator(w) for w in wls]          # uploads the 15 fields from the host
+        h2d += sum(15 * w.n_sites * 8 for w in wls)
+        if args.form == 'served':
+            reqs = [serving.Request(H, k=K, sigma=w.sigma[band], tol=TOL, maxiter=MAXITER)
+                    for w, H in zip(wls, hops) for band in BANDS]
+            serving.solve_batch(reqs, max_slots=len(reqs), ticks_per_poll=args.ticks_per_poll)
+            for r in reqs:                               # X0 drawn on the host and uploaded
+                h2d += r.H.shape[0] * r.block * 16
+                V = r.result['V'].cpu().numpy()
+                d2h += V.nbytes + r.result['E'].nbytes
+                e2e_pairs += int((r.result['residuals'] <= RES_TOL).sum())
+        else:
+            for w, H in zip(wls, hops):
+                for band in BANDS:
+                    E, V, info = eg.solve_interior(H, k=K, sigma=w.sigma[band], tol=TOL,
+                                                   maxiter=MAXITER, verbose=False)
+                    h2d += H.shape[0] * BLOCK * 16
+                    d2h += V.nbytes + E.nbytes
+                    e2e_pairs += int((info['residuals'] <= RES_TOL).sum())
+        for H in hops:
             H.close()
         torch.cuda.synchronize(device)
         e2e_t = time.perf_counter() - t0
         e2e = {'value': e2e_pairs / e2e_t, 'unit': 'eigenpairs/s', 'h2d_bytes_per_step': h2d,
-               'd2h_bytes_per_step': d2h, 'seconds_per_step': e2e_t}
+               'd2h_bytes_per_step': d2h, 'seconds_per_step': e2e_t,
+               'path': 'confined_hamiltonian + ' + ('serving.solve_batch' if args.form == 'served'
+                                                    else 'eigensolvers.solve_interior')}
+
+    # ---- serving: requests arriving over time (Poisson, seed 2), p50 / p99 latency ---------
+    stream = None
+    if rank == 0 and args.form == 'served' and not args.no_stream:
+        rng = np.random.default_rng(2)
+        reqs = [serving.Request(H, k=K, sigma=w.sigma[band], tol=TOL, maxiter=MAXITER)
+                for _ in range(2) for w, H in zip(wls, ops) for band in BANDS]
+        rng.shuffle(reqs)
+        # mean arrival rate: ~80 % of the batch throughput measured above
+        rate = 0.8 * (value / K)
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, size=len(reqs)))
+        _, stats = serving.serve(reqs, arrivals, max_slots=len(SIZES) * len(BANDS),
+                                 ticks_per_poll=args.ticks_per_poll)
+        stream = dict(requests=len(reqs), rate_per_s=rate, **stats)
 
     cpu = cpu_baseline(wls, steps[-1]['iters']) if (rank == 0 and ws == 1 and not args.no_cpu) else None
     hx2 = hx_config2(torch, device) if (rank == 0 and not args.no_config2) else None
@@ -328,6 +350,7 @@ def run_ours(args):
                          'launches': hx_n, 'avg_launch_us': hx_s / max(hx_n, 1) * 1e6,
                          'algorithmic_bytes_per_launch': hx_b / max(hx_n, 1)},
             'plain': plain,
+            'serving_stream': stream,
             'served_vs_plain': (value / plain['value']) if plain else None,
             'hx_config2': hx2,
             'cpu_baseline': cpu,
@@ -346,6 +369,18 @@ def run_ours(args):
     if ws > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def combine_ranks(total_ms, pairs, device):
+    """Whole-job numbers of a replica run: elapsed time is the max over ranks (device-timed on
+    each), converged eigenpairs the sum over ranks."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(total_ms)], dtype=torch.float64, device=device)
+    p = torch.tensor([float(pairs)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dist.all_reduce(p, op=dist.ReduceOp.SUM)
+    return float(t.item()), float(p.item())
 
 
 def hx_traffic():
@@ -393,6 +428,23 @@ def cpu_baseline(wls, iters):
                       'of all 14 solves; CSR SpMM single-threaded, BLAS on all cores'}
 
 
+def hx_probe(args):
+    """A few H.X launches on the 48x48x36 operator (profiling aid; prints one JSON line)."""
+    import torch
+    from qd3dsolver_b200 import workloads as wl
+    w = wl.config1()
+    H = make_operator(w)
+    dt = torch.complex128 if args.hx_dtype == 'c128' else torch.complex64
+    X = torch.randn(H.shape[0], args.hx_m, dtype=dt, device='cuda')
+    Y = torch.empty_like(X)
+    for _ in range(args.hx_launches):
+        H.apply(X, out=Y)
+    torch.cuda.synchronize()
+    print(json.dumps({'hx_probe': w.name, 'm': args.hx_m, 'dtype': args.hx_dtype,
+                      'launches': args.hx_launches}))
+    H.close()
+
+
 def run_reference(args):
     ws, rank, local = dist_env()
     if rank != 0:
@@ -432,11 +484,21 @@ def main():
     ap.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline sample')
     ap.add_argument('--no-config2', action='store_true', help='skip the 128x128x96 H.X timing')
     ap.add_argument('--form', choices=('served', 'plain'), default='served')
+    ap.add_argument('--no-plain', action='store_true', help='skip the plain-form comparison')
+    ap.add_argument('--no-e2e', action='store_true', help='skip the host-buffer end-to-end run')
+    ap.add_argument('--no-stream', action='store_true', help='skip the Poisson-arrival run')
+    ap.add_argument('--hx-probe', action='store_true',
+                    help='only run a few H.X launches on the 48x48x36 operator (profiling)')
+    ap.add_argument('--hx-m', type=int, default=12)
+    ap.add_argument('--hx-dtype', choices=('c128', 'c64'), default='c128')
+    ap.add_argument('--hx-launches', type=int, default=3)
     ap.add_argument('--ticks-per-poll', type=int, default=16)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    if args.impl == 'reference':
+    if args.hx_probe:
+        hx_probe(args)
+    elif args.impl == 'reference':
         run_reference(args)
     else:
         run_ours(args)

@@ -738,6 +738,7 @@ int qdkp_engine_admit(qdkp_engine* e, const qdkp_operator* op, const qdkp_lobpcg
   const int64_t n = (int64_t)op->n_bands * op->n_sites;
   const int m = prm->block;
   QDKP_CHECK_ARG(n >= 5 * m, "problem too small for LOBPCG");
+  QDKP_CHECK_ARG(n * m < (int64_t(1) << 31), "n * block must stay below 2^31 elements");
   const SlotLayout L = slot_layout(n, m);
   if (ws_bytes < L.total) { set_error("engine slot workspace too small"); return QDKP_ERR_WORKSPACE; }
   int id = -1;

@@ -17,6 +17,8 @@
 // block), reading the 15 raw fields of the site and its six face neighbours. Phase 2 gives each
 // thread (site, column) items: it loads the eight band components of the site, its six faces
 // and twelve edges for that column, and accumulates all eight output bands in registers.
+#include <algorithm>
+
 #include "qdkp_common.cuh"
 
 namespace qdkp {
@@ -67,7 +69,8 @@ __device__ __forceinline__ void first_order_coefs(const T* __restrict__ F, long 
 }
 
 template <typename T, int NB>
-__device__ void build_record(const ApplyArgs<T>& a, long long s, T* rec, int S) {
+__device__ void build_record(const ApplyArgs<T>& a, long long s, T* rec, int S,
+                             unsigned* nbmask) {
   const T* __restrict__ F = a.F;
   const long long N = a.N;
   const int iz = (int)(s % a.nz);
@@ -83,6 +86,23 @@ __device__ void build_record(const ApplyArgs<T>& a, long long s, T* rec, int S) 
   const bool strain = (a.flags & QDKP_STRAIN) != 0;
   const bool inter = NB == 8 && strain && (a.flags & QDKP_INTERBAND_STRAIN);
 
+  // neighbour mask: bit f (0..5) face x+, x-, y+, y-, z+, z-; bit 6 + 4 pl + e the in-plane
+  // edge e of plane pl (xy, zx, zy) with signs sa = e & 1 ? -1 : 1, sb = e & 2 ? -1 : 1
+  {
+    unsigned msk = 0;
+    for (int ax = 0; ax < 3; ++ax) {
+      if (coord[ax] + 1 < ext[ax]) msk |= 1u << (2 * ax);
+      if (coord[ax] > 0) msk |= 1u << (2 * ax + 1);
+    }
+    for (int pl = 0; pl < 3; ++pl) {
+      const int ea = pl == 0 ? 0 : 2, eb = pl == 0 ? 1 : (pl == 1 ? 0 : 1);
+      for (int e = 0; e < 4; ++e) {
+        const int ca = coord[ea] + ((e & 1) ? -1 : 1), cb = coord[eb] + ((e & 2) ? -1 : 1);
+        if (ca >= 0 && ca < ext[ea] && cb >= 0 && cb < ext[eb]) msk |= 1u << (6 + 4 * pl + e);
+      }
+    }
+    *nbmask = msk;
+  }
   const T g1 = F[F_G1 * N + s], g2 = F[F_G2 * N + s];
   T cu_p[3]; cplx<T> cv_p[3];
   if (NB == 8) first_order_coefs<T>(F, N, s, inter, cu_p, cv_p);
@@ -150,13 +170,15 @@ template <int NB> __device__ __forceinline__ constexpr bool has_band(int b) {
 }
 template <int NB> __device__ __forceinline__ constexpr int band_off() { return NB == 8 ? 0 : 2; }
 
+// x[b] = X[band b, site s + offset, column j] with xs = &X[0, s, j], bstr = N ldx (elements);
+// every offset fits 32 bits for the grids this library accepts (n ldx < 2^31).
 template <typename T, int NB, bool VB_ONLY>
-__device__ __forceinline__ void load_site(const ApplyArgs<T>& a, long long q, int j,
+__device__ __forceinline__ void load_site(const cplx<T>* __restrict__ xs, int bstr, int off,
                                           cplx<T> (&x)[8]) {
 #pragma unroll
   for (int b = 0; b < 8; ++b) {
     if (!has_band<NB>(b) || (VB_ONLY && b < 2)) { x[b] = czero<T>(); continue; }
-    x[b] = __ldg(&a.X[((long long)(b - band_off<NB>()) * a.N + q) * a.ldx + j]);
+    x[b] = __ldg(xs + ((b - band_off<NB>()) * bstr + off));
   }
 }
 
@@ -169,7 +191,9 @@ __device__ __forceinline__ void apply_tile(const ApplyArgs<T>& a, long long s0, 
   const int S = a.S;
   const int ns = (int)min((long long)S, a.N - s0);
 
-  for (int i = threadIdx.x; i < ns; i += blockDim.x) build_record<T, NB>(a, s0 + i, rec + i, S);
+  unsigned* nbm = reinterpret_cast<unsigned*>(rec + R_COUNT * S);
+  for (int i = threadIdx.x; i < ns; i += blockDim.x)
+    build_record<T, NB>(a, s0 + i, rec + i, S, nbm + i);
   __syncthreads();
 
   const T G = T(kG);
@@ -182,25 +206,23 @@ __device__ __forceinline__ void apply_tile(const ApplyArgs<T>& a, long long s0, 
   const int m = a.m;
   const int items = ns * m;
 
+  const int bstr = (int)(a.N * a.ldx);
+  const int ystr = (int)(a.N * a.ldy);
+  const int sx = a.ny * a.nz, sy = a.nz;
   for (int it = threadIdx.x; it < items; it += blockDim.x) {
     const int i = it / m;
     const int j = it - i * m;
     const long long s = s0 + i;
     const T* r = rec + i;
-    const int iz = (int)(s % a.nz);
-    const long long t = s / a.nz;
-    const int iy = (int)(t % a.ny);
-    const int ix = (int)(t / a.ny);
-    const int coord[3] = {ix, iy, iz};
-    const int ext[3] = {a.nx, a.ny, a.nz};
-    const long long str[3] = {(long long)a.ny * a.nz, (long long)a.nz, 1LL};
-
+    const unsigned msk = nbm[i];
+    const cplx<T>* __restrict__ xs = a.X + (s * a.ldx + j);
+    const int str[3] = {sx * (int)a.ldx, sy * (int)a.ldx, (int)a.ldx};
     cplx<T> y[8], x[8];
 
     // ---- local block ------------------------------------------------------------------
     // y = sign (H x) - sigma x is accumulated as sign (H x - sign sigma x): start from the
     // shift term so the centre values need not stay live until the end.
-    load_site<T, NB, false>(a, s, j, x);
+    load_site<T, NB, false>(xs, bstr, 0, x);
     {
       const T sh = a.shifted ? -a.sigma * a.sign : T(0);
 #pragma unroll
@@ -229,10 +251,8 @@ __device__ __forceinline__ void apply_tile(const ApplyArgs<T>& a, long long s0, 
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
       const int ax = f >> 1, dir = f & 1;
-      const bool in = dir == 0 ? (coord[ax] + 1 < ext[ax]) : (coord[ax] > 0);
-      if (!in) continue;
-      const long long q = dir == 0 ? s + str[ax] : s - str[ax];
-      load_site<T, NB, false>(a, q, j, x);
+      if (!(msk & (1u << f))) continue;
+      load_site<T, NB, false>(xs, bstr, dir == 0 ? str[ax] : -str[ax], x);
       const T kp = r[(R_T1 + f) * S], k2 = r[(R_T2 + f) * S];
       const T kq = wQ[ax] * k2, kr = wR[ax] * k2;
       if (NB == 8) { caxpy(y[0], -G * ih2, x[0]); caxpy(y[1], -G * ih2, x[1]); }
@@ -292,13 +312,11 @@ __device__ __forceinline__ void apply_tile(const ApplyArgs<T>& a, long long s0, 
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
         const int sa = (e & 1) ? -1 : 1, sb = (e & 2) ? -1 : 1;
-        const int ca = coord[ea] + sa, cb = coord[eb] + sb;
-        if (ca < 0 || ca >= ext[ea] || cb < 0 || cb >= ext[eb]) continue;
-        const long long q = s + sa * str[ea] + sb * str[eb];
+        if (!(msk & (1u << (6 + 4 * pl + e)))) continue;
         const T ga = r[(R_G3 + 2 * ea + (sa < 0)) * S];
         const T gb = r[(R_G3 + 2 * eb + (sb < 0)) * S];
         const T c = T(2) * sq3 * G * (-(T)(sa * sb) * i8h2) * (ga + gb);
-        load_site<T, NB, true>(a, q, j, x);
+        load_site<T, NB, true>(xs, bstr, sa * str[ea] + sb * str[eb], x);
         if (pl == 0) {
           caxpy_i(y[2], c, x[4]);
           caxpy_i(y[4], -c, x[2]);
@@ -327,7 +345,7 @@ __device__ __forceinline__ void apply_tile(const ApplyArgs<T>& a, long long s0, 
 #pragma unroll
     for (int b = 0; b < 8; ++b) {
       if (!has_band<NB>(b)) continue;
-      a.Y[((long long)(b - band_off<NB>()) * a.N + s) * a.ldy + j] = cscale(a.sign, y[b]);
+      a.Y[(s * a.ldy + j) + (long long)((b - band_off<NB>()) * ystr)] = cscale(a.sign, y[b]);
     }
   }
 }
@@ -364,11 +382,11 @@ int launch_apply_multi(const HXSlot* slots_dev, int nslots, int total_tiles, int
                        int precision, cudaStream_t st) {
   if (total_tiles <= 0) return QDKP_OK;
   if (precision == QDKP_C128) {
-    kp_apply_multi_kernel<double><<<total_tiles, 256, (size_t)R_COUNT * S_max * sizeof(double), st>>>(
-        slots_dev, nslots);
+    kp_apply_multi_kernel<double><<<total_tiles, 256,
+        (size_t)R_COUNT * S_max * sizeof(double) + S_max * sizeof(unsigned), st>>>(slots_dev, nslots);
   } else {
-    kp_apply_multi_kernel<float><<<total_tiles, 256, (size_t)R_COUNT * S_max * sizeof(float), st>>>(
-        slots_dev, nslots);
+    kp_apply_multi_kernel<float><<<total_tiles, 256,
+        (size_t)R_COUNT * S_max * sizeof(float) + S_max * sizeof(unsigned), st>>>(slots_dev, nslots);
   }
   count_launch();
   QDKP_CUDA_TRY(cudaGetLastError());
@@ -384,6 +402,10 @@ template <typename T>
 static int launch_apply_t(const qdkp_operator* op, const T* F, const void* X, int64_t ldx,
                           void* Y, int64_t ldy, int m, double sigma, int shifted,
                           cudaStream_t st) {
+  if ((int64_t)op->n_bands * op->n_sites * std::max(ldx, ldy) >= (int64_t(1) << 31)) {
+    set_error("H.X: n * leading dimension must stay below 2^31 elements");
+    return QDKP_ERR_UNSUPPORTED;
+  }
   ApplyArgs<T> a;
   a.F = F;
   a.X = static_cast<const cplx<T>*>(X);
@@ -395,7 +417,7 @@ static int launch_apply_t(const qdkp_operator* op, const T* F, const void* X, in
   if (op->flags & QDKP_NEGATE) a.sign = -a.sign;
   const int S = apply_tile_sites(m);
   a.S = S;
-  const size_t smem = (size_t)R_COUNT * S * sizeof(T);
+  const size_t smem = (size_t)R_COUNT * S * sizeof(T) + (size_t)S * sizeof(unsigned);
   const unsigned grid = (unsigned)((op->n_sites + S - 1) / S);
   switch (op->n_bands) {
     case 8: kp_apply_kernel<T, 8><<<grid, 256, smem, st>>>(a); break;
