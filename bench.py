@@ -178,7 +178,7 @@ def run_ours(args):
 
     def served_step():
         reqs = [serving.Request(H, k=K, sigma=w.sigma[band], tol=TOL, maxiter=MAXITER,
-                                tag=(w.meta['base'], band))
+                                tag=(w.meta['base'], band), precision=args.precision)
                 for w, H in zip(wls, ops) for band in BANDS]
         t0 = time.perf_counter()
         serving.solve_batch(reqs, max_slots=len(reqs), ticks_per_poll=args.ticks_per_poll)
@@ -276,7 +276,8 @@ def run_ours(args):
         hops = [make_operator(w) for w in wls]          # uploads the 15 fields from the host
         h2d += sum(15 * w.n_sites * 8 for w in wls)
         if args.form == 'served':
-            reqs = [serving.Request(H, k=K, sigma=w.sigma[band], tol=TOL, maxiter=MAXITER)
+            reqs = [serving.Request(H, k=K, sigma=w.sigma[band], tol=TOL, maxiter=MAXITER,
+                                    precision=args.precision)
                     for w, H in zip(wls, hops) for band in BANDS]
             serving.solve_batch(reqs, max_slots=len(reqs), ticks_per_poll=args.ticks_per_poll)
             for r in reqs:                               # X0 drawn on the host and uploaded
@@ -305,7 +306,8 @@ def run_ours(args):
     stream = None
     if rank == 0 and args.form == 'served' and not args.no_stream:
         rng = np.random.default_rng(2)
-        reqs = [serving.Request(H, k=K, sigma=w.sigma[band], tol=TOL, maxiter=MAXITER)
+        reqs = [serving.Request(H, k=K, sigma=w.sigma[band], tol=TOL, maxiter=MAXITER,
+                                precision=args.precision)
                 for _ in range(2) for w, H in zip(wls, ops) for band in BANDS]
         rng.shuffle(reqs)
         # mean arrival rate: ~80 % of the batch throughput measured above
@@ -325,12 +327,18 @@ def run_ours(args):
             'metric': METRIC, 'value': value, 'unit': 'eigenpairs/s', 'n_gpus': ws,
             'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': total_ms / args.steps,
             'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
-            'dtype': 'c128', 'data': 'synthetic',
+            'dtype': ('c64+c128' if (args.form == 'served' and args.precision == 'mixed')
+                      else 'c128'),
+            'data': 'synthetic',
             'config': {'workload': 'fig4 sweep: InAs/GaAs pyramids b=6..18 nm, h=1.0 nm, Pryor '
                                    'Table I, Fourier strain + piezo, cb+vb, k=8, block 12, '
                                    'tol 1e-7, maxiter 8000 (pryor_fig4.sweep)',
-                       'form': ('served: batched engine, 14 solves resident, continuous batching, '
-                                'c128' if args.form == 'served' else
+                       'form': (('served: batched engine, 14 solves resident, continuous '
+                                 'batching, CUDA-graph ticks, ' +
+                                 ('complex64 search to 1e-4 then complex128 finish (FP64 '
+                                  'Gram/Cholesky/Rayleigh-Ritz throughout)'
+                                  if args.precision == 'mixed' else 'complex128'))
+                                if args.form == 'served' else
                                 'plain c128 single-solve drop-in (solve_interior)'),
                        'solves_per_step': len(SIZES) * len(BANDS),
                        'eigenpairs_per_step': len(SIZES) * len(BANDS) * K,
@@ -445,6 +453,29 @@ def hx_probe(args):
     H.close()
 
 
+def engine_probe(args):
+    """The served engine on the 14 sweep solves for a fixed number of ticks, with direct kernel
+    launches (no graph), so that a profiler sees every kernel of a tick (profiling aid; prints
+    one JSON line)."""
+    import torch
+    from qd3dsolver_b200 import serving
+    wls = build_workloads()
+    ops = [make_operator(w) for w in wls]
+    eng = serving.Engine(len(wls) * len(BANDS), graphs=False)
+    reqs = [serving.Request(H, k=K, sigma=w.sigma[band], tol=TOL, maxiter=MAXITER,
+                            precision=args.precision)
+            for w, H in zip(wls, ops) for band in BANDS]
+    for r in reqs:
+        eng.admit(r)
+    eng.step(args.probe_ticks)
+    torch.cuda.synchronize()
+    print(json.dumps({'engine_probe': len(reqs), 'ticks': args.probe_ticks,
+                      'precision': args.precision}))
+    eng.close()
+    for H in ops:
+        H.close()
+
+
 def run_reference(args):
     ws, rank, local = dist_env()
     if rank != 0:
@@ -492,12 +523,19 @@ def main():
     ap.add_argument('--hx-m', type=int, default=12)
     ap.add_argument('--hx-dtype', choices=('c128', 'c64'), default='c128')
     ap.add_argument('--hx-launches', type=int, default=3)
+    ap.add_argument('--engine-probe', action='store_true',
+                    help='only run the served engine for --probe-ticks ticks (profiling)')
+    ap.add_argument('--probe-ticks', type=int, default=20)
     ap.add_argument('--ticks-per-poll', type=int, default=16)
+    ap.add_argument('--precision', choices=('mixed', 'c128'), default='mixed',
+                    help='served form: complex64 search + complex128 finish, or complex128 only')
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.hx_probe:
         hx_probe(args)
+    elif args.engine_probe:
+        engine_probe(args)
     elif args.impl == 'reference':
         run_reference(args)
     else:

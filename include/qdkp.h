@@ -147,6 +147,24 @@ size_t qdkp_apply_folded_noalloc_max_elems(int precision);
 int qdkp_apply_folded_noalloc(const qdkp_operator* op, const void* X, int64_t ldx, void* Y,
                               int64_t ldy, int m, double sigma, int precision, void* stream);
 
+/*
+ * H.X kernel selection (no counterpart in the reference, which multiplies an assembled CSR).
+ * Eight-band operators are applied by a staged kernel: a CTA owns a (y, z) tile of sites and a
+ * few columns, walks along x and keeps a ring of x planes in shared memory. The tile shape is
+ * one of QDKP_TILE_COUNT built shapes, chosen by a padding heuristic unless set here or by
+ * qdkp_operator_tune; QDKP_TILE_DIRECT selects the unstaged one-thread-per-(site, column) kernel
+ * (always used for 6- and 4-band slices). The choice is per operator and precision.
+ */
+enum { QDKP_TILE_AUTO = -1, QDKP_TILE_DIRECT = -2, QDKP_TILE_COUNT = 4 };
+int qdkp_operator_set_tile(qdkp_operator* op, int precision, int tile);
+int qdkp_operator_get_tile(const qdkp_operator* op, int precision, int* tile);
+/* Autotuner: times every tile shape and the direct kernel on the caller's device blocks X, Y
+ * (n x m, `precision`) with `reps` launches each, keeps the fastest for this operator and
+ * precision, and writes the per-candidate seconds per launch to seconds[QDKP_TILE_COUNT + 1]
+ * (may be NULL; index QDKP_TILE_COUNT is the direct kernel). Y is overwritten. Synchronous. */
+int qdkp_operator_tune(qdkp_operator* op, const void* X, int64_t ldx, void* Y, int64_t ldy,
+                       int m, int precision, int reps, double* seconds, void* stream);
+
 /* Workspace bytes qdkp_apply_host needs for an (n, m) complex128 block in `mode`. */
 size_t qdkp_apply_host_workspace_size(const qdkp_operator* op, int m, int mode);
 
@@ -223,8 +241,13 @@ size_t qdkp_engine_slot_workspace_size(const qdkp_operator* op, const qdkp_lobpc
  * Rayleigh-Ritz step (synchronous on `stream`). *slot receives the slot id. */
 int qdkp_engine_admit(qdkp_engine* e, const qdkp_operator* op, const qdkp_lobpcg_params* prm,
                       const void* X0, void* ws, size_t ws_bytes, void* stream, int* slot);
-/* Launch `ticks` iterations of every running slot (asynchronous on `stream`). */
+/* Launch `ticks` iterations of every running slot (asynchronous on `stream`). The tick sequence
+ * is fixed for a slot layout, so by default it is captured once per layout (and tick count) as
+ * a CUDA graph and replayed on the engine's own stream, ordered after `stream` and before later
+ * work on it by events. */
 int qdkp_engine_step(qdkp_engine* e, int ticks, void* stream);
+/* 0: launch the tick kernels directly on the caller's stream instead of replaying a graph. */
+int qdkp_engine_set_graphs(qdkp_engine* e, int enable);
 /* state[max_slots]: -1 free, 1 running, 0 stopped (status[] gives QDKP_LOBPCG_*);
  * iterations[] = iterations started so far. Synchronous. */
 int qdkp_engine_poll(qdkp_engine* e, int* state, int* status, int* iterations, void* stream);

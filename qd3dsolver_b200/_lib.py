@@ -13,6 +13,7 @@ QDKP_OK = 0
 HOLE_CONVENTION, STRAIN, INTERBAND_STRAIN, NEGATE = 1, 2, 4, 8
 C128, C64 = 0, 1
 APPLY_PLAIN, APPLY_SHIFTED, APPLY_FOLDED = 0, 1, 2
+TILE_AUTO, TILE_DIRECT, TILE_COUNT = -1, -2, 4
 LOBPCG_STATUS = {0: 'converged', 1: 'maxiter', 2: 'cholesky_breakdown',
                  3: 'eigh_breakdown', 4: 'nonfinite'}
 
@@ -60,6 +61,13 @@ _SIGNATURES = {
     'qdkp_apply_folded_noalloc': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
                                                  ctypes.c_void_p, ctypes.c_int64, ctypes.c_int,
                                                  ctypes.c_double, ctypes.c_int, ctypes.c_void_p]),
+    'qdkp_operator_set_tile': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
+    'qdkp_operator_get_tile': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int,
+                                              ctypes.POINTER(ctypes.c_int)]),
+    'qdkp_operator_tune': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+                                          ctypes.c_void_p, ctypes.c_int64, ctypes.c_int,
+                                          ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                          ctypes.c_void_p]),
     'qdkp_apply_host_workspace_size': (ctypes.c_size_t, [ctypes.c_void_p, ctypes.c_int,
                                                          ctypes.c_int]),
     'qdkp_apply_host': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
@@ -81,6 +89,7 @@ _SIGNATURES = {
                                          ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p,
                                          ctypes.POINTER(ctypes.c_int)]),
     'qdkp_engine_step': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
+    'qdkp_engine_set_graphs': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     'qdkp_engine_poll': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                         ctypes.c_void_p, ctypes.c_void_p]),
     'qdkp_engine_retire': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,

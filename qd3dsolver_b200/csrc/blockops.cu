@@ -3,6 +3,7 @@
 // parallel cyclic Jacobi) for the LOBPCG driver.
 #include <algorithm>
 #include <cmath>
+#include <type_traits>
 
 #include "dense_dev.cuh"
 
@@ -11,8 +12,9 @@ namespace qdkp {
 // ------------------------------------------------------------------------------------------------
 // Column norms: out[j] = sum_r |A[r, j] - lambda_j B[r, j]|^2 (B may be NULL).
 // ------------------------------------------------------------------------------------------------
+template <typename T>
 __global__ void __launch_bounds__(kTallThreads)
-colnorm2_partial(const double2* __restrict__ A, long long lda, const double2* __restrict__ B,
+colnorm2_partial(const cplx<T>* __restrict__ A, long long lda, const cplx<T>* __restrict__ B,
                  long long ldb, const double* __restrict__ lam, int m, long long n,
                  double* __restrict__ partial) {
   double acc[kMaxBlock];
@@ -23,11 +25,12 @@ colnorm2_partial(const double2* __restrict__ A, long long lda, const double2* __
 #pragma unroll
     for (int j = 0; j < kMaxBlock; ++j) {
       if (j < m) {
-        double2 a = A[r * lda + j];
+        const cplx<T> av = A[r * lda + j];
+        double2 a = make_double2((double)av.x, (double)av.y);
         if (B) {
-          const double2 b = B[r * ldb + j];
-          a.x -= lam[j] * b.x;
-          a.y -= lam[j] * b.y;
+          const cplx<T> b = B[r * ldb + j];
+          a.x -= lam[j] * (double)b.x;
+          a.y -= lam[j] * (double)b.y;
         }
         acc[j] = fma(a.x, a.x, fma(a.y, a.y, acc[j]));
       }
@@ -61,11 +64,12 @@ __global__ void reduce_partials(const double* __restrict__ partial, int nparts, 
   }
 }
 
-int launch_colnorm2(const double2* A, long long lda, const double2* B, long long ldb,
+template <typename T>
+int launch_colnorm2(const cplx<T>* A, long long lda, const cplx<T>* B, long long ldb,
                     const double* lambda, int m, long long n, double* partial, int nparts,
                     double* out, cudaStream_t st) {
   if (m > kMaxBlock) { set_error("block wider than kMaxBlock"); return QDKP_ERR_ARG; }
-  colnorm2_partial<<<nparts, kTallThreads, 0, st>>>(A, lda, B, ldb, lambda, m, n, partial);
+  colnorm2_partial<T><<<nparts, kTallThreads, 0, st>>>(A, lda, B, ldb, lambda, m, n, partial);
   count_launch();
   reduce_partials<<<1, 32, 0, st>>>(partial, nparts, m, out);
   count_launch();
@@ -101,34 +105,38 @@ int launch_resid_gather(const double2* AX, long long ldax, const double2* X, lon
   return QDKP_OK;
 }
 
-__global__ void gather_kernel(const double2* __restrict__ src, long long lds,
+template <typename TS, typename TD>
+__global__ void gather_kernel(const cplx<TS>* __restrict__ src, long long lds,
                               const int* __restrict__ idx, int ma, long long n,
-                              double2* __restrict__ dst, long long ldd) {
+                              cplx<TD>* __restrict__ dst, long long ldd) {
   const long long total = n * ma;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
        e += (long long)gridDim.x * blockDim.x) {
     const long long r = e / ma;
     const int c = (int)(e - r * ma);
-    dst[r * ldd + c] = src[r * lds + (idx ? idx[c] : c)];
+    const cplx<TS> v = src[r * lds + (idx ? idx[c] : c)];
+    dst[r * ldd + c] = mk<TD>((TD)v.x, (TD)v.y);
   }
 }
 
-int launch_gather(const double2* src, long long lds, const int* idx, int ma, long long n,
-                  double2* dst, long long ldd, cudaStream_t st) {
-  gather_kernel<<<1184, 256, 0, st>>>(src, lds, idx, ma, n, dst, ldd);
+template <typename TS, typename TD>
+int launch_gather(const cplx<TS>* src, long long lds, const int* idx, int ma, long long n,
+                  cplx<TD>* dst, long long ldd, cudaStream_t st) {
+  gather_kernel<TS, TD><<<1184, 256, 0, st>>>(src, lds, idx, ma, n, dst, ldd);
   count_launch();
   QDKP_CUDA_TRY(cudaGetLastError());
   return QDKP_OK;
 }
 
-int launch_copy(const double2* src, long long lds, int cols, long long n, double2* dst,
+template <typename TS, typename TD>
+int launch_copy(const cplx<TS>* src, long long lds, int cols, long long n, cplx<TD>* dst,
                 long long ldd, cudaStream_t st) {
-  if (lds == cols && ldd == cols) {
-    QDKP_CUDA_TRY(cudaMemcpyAsync(dst, src, (size_t)n * cols * sizeof(double2),
+  if (std::is_same<TS, TD>::value && lds == cols && ldd == cols) {
+    QDKP_CUDA_TRY(cudaMemcpyAsync(dst, src, (size_t)n * cols * sizeof(cplx<TD>),
                                   cudaMemcpyDeviceToDevice, st));
     return QDKP_OK;
   }
-  return launch_gather(src, lds, nullptr, cols, n, dst, ldd, st);
+  return launch_gather<TS, TD>(src, lds, nullptr, cols, n, dst, ldd, st);
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -143,11 +151,11 @@ constexpr int kGramParts = 296;
 // f64 kind). A CTA of 3 x 3 warps owns all 8x8 tiles of C' for its slice of rows; each warp
 // owns a rectangle of up to 6 x 6 tiles and keeps them in registers across the slice.
 
-template <int MR, int MC>
+template <int MR, int MC, typename T>
 __global__ void __launch_bounds__(512)
-gram_partial_kernel(const BlockList<double> A, const BlockList<double> B, long long n,
+gram_partial_kernel(const BlockList<T> A, const BlockList<T> B, long long n,
                     long long rows_per_part, double* __restrict__ partial) {
-  extern __shared__ double gsm_d[];
+  extern __shared__ __align__(16) unsigned char gsm_d[];
   const int RP = (2 * A.total() + 7) / 8 * 8, RQ = (2 * B.total() + 7) / 8 * 8;
   const long long r0 = blockIdx.x * rows_per_part;
   gram_core<MR, MC>(A, B, r0, min(n, r0 + rows_per_part),
@@ -190,7 +198,8 @@ size_t gram_partial_elems(int P, int Q) {
   return (size_t)(kGramParts + kGramSplit) * RP * RQ / 2 + 1;   // in double2 units
 }
 
-int launch_gram(const BlockList<double>& A, const BlockList<double>& B, long long n,
+template <typename T>
+int launch_gram(const BlockList<T>& A, const BlockList<T>& B, long long n,
                 double2* partial, size_t partial_elems, double2* out, cudaStream_t st) {
   const int P = A.total(), Q = B.total();
   if (P > kMaxSmall || Q > kMaxSmall || P <= 0 || Q <= 0) {
@@ -208,22 +217,22 @@ int launch_gram(const BlockList<double>& A, const BlockList<double>& B, long lon
     set_error("gram partial buffer too small");
     return QDKP_ERR_WORKSPACE;
   }
-  const size_t smem = (size_t)RP * RQ * sizeof(double);
+  const size_t smem = gram_smem_bytes(P, Q, (int)sizeof(cplx<T>));
   static bool attr = false;
   if (!attr) {
     const int big = 200 * 1024;
-    cudaFuncSetAttribute(gram_partial_kernel<3, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-    cudaFuncSetAttribute(gram_partial_kernel<3, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-    cudaFuncSetAttribute(gram_partial_kernel<6, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    cudaFuncSetAttribute(gram_partial_kernel<3, 3, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    cudaFuncSetAttribute(gram_partial_kernel<3, 6, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    cudaFuncSetAttribute(gram_partial_kernel<6, 6, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
     attr = true;
   }
   int MR, MC, threads;
   gram_shape(P, Q, MR, MC, threads);
   double* pd = reinterpret_cast<double*>(partial);
   const unsigned grid = (unsigned)parts;
-  if (MR == 3 && MC == 3) gram_partial_kernel<3, 3><<<grid, threads, smem, st>>>(A, B, n, rpp, pd);
-  else if (MR == 3) gram_partial_kernel<3, 6><<<grid, threads, smem, st>>>(A, B, n, rpp, pd);
-  else gram_partial_kernel<6, 6><<<grid, threads, smem, st>>>(A, B, n, rpp, pd);
+  if (MR == 3 && MC == 3) gram_partial_kernel<3, 3, T><<<grid, threads, smem, st>>>(A, B, n, rpp, pd);
+  else if (MR == 3) gram_partial_kernel<3, 6, T><<<grid, threads, smem, st>>>(A, B, n, rpp, pd);
+  else gram_partial_kernel<6, 6, T><<<grid, threads, smem, st>>>(A, B, n, rpp, pd);
   count_launch();
   const int elems = RP * RQ;
   double* part2 = pd + (size_t)parts * elems;
@@ -242,33 +251,35 @@ struct CoefList {
   const double2* c[3];
 };
 
+template <typename T>
 __global__ void __launch_bounds__(kUpdThreads)
-update_kernel(const BlockList<double> A, const CoefList C, int q, long long n, double2* Y,
+update_kernel(const BlockList<T> A, const CoefList C, int q, long long n, cplx<T>* Y,
               long long ldy, int accumulate) {
-  extern __shared__ double usm[];
+  extern __shared__ __align__(16) unsigned char usm[];
   const double2* Cf[3] = {C.c[0], C.c[1], C.c[2]};
-  const long long per = ((n + gridDim.x - 1) / gridDim.x + 63) / 64 * 64;
+  const long long per = ((n + gridDim.x - 1) / gridDim.x + kUpdChunk - 1) / kUpdChunk * kUpdChunk;
   const long long r0 = (long long)blockIdx.x * per;
+  if (r0 >= n) return;
   update_rows(A, Cf, q, r0, min(n, r0 + per), Y, ldy, accumulate, 0, usm);
 }
 
-int launch_update(const BlockList<double>& A, const double2* const* C, int q, long long n,
-                  double2* Y, long long ldy, int accumulate, cudaStream_t st) {
+template <typename T>
+int launch_update(const BlockList<T>& A, const double2* const* C, int q, long long n,
+                  cplx<T>* Y, long long ldy, int accumulate, cudaStream_t st) {
   if (q > kMaxBlock || A.total() > kMaxSmall || q < 1) { set_error("update dimensions out of range"); return QDKP_ERR_ARG; }
   CoefList cl;
   for (int b = 0; b < 3; ++b) cl.c[b] = b < A.nblk ? C[b] : nullptr;
   const int P = A.total();
-  const int KPp = (2 * P + 3) / 4 * 4, NQ = (2 * q + 7) / 8 * 8;
-  const size_t smem = ((size_t)KPp * NQ + (size_t)4 * NQ) * sizeof(double);
+  const size_t smem = update_smem_bytes(P, q, (int)sizeof(cplx<T>));
   static bool attr = false;
   if (!attr) {
-    QDKP_CUDA_TRY(cudaFuncSetAttribute(update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       120 * 1024));
+    QDKP_CUDA_TRY(cudaFuncSetAttribute(update_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       200 * 1024));
     attr = true;
   }
-  long long blocks = (n + kUpdRows - 1) / kUpdRows;
+  long long blocks = (n + kUpdChunk - 1) / kUpdChunk;
   if (blocks > 148 * 4) blocks = 148 * 4;
-  update_kernel<<<(unsigned)blocks, kUpdThreads, smem, st>>>(A, cl, q, n, Y, ldy, accumulate);
+  update_kernel<T><<<(unsigned)blocks, kUpdThreads, smem, st>>>(A, cl, q, n, Y, ldy, accumulate);
   count_launch();
   QDKP_CUDA_TRY(cudaGetLastError());
   return QDKP_OK;
@@ -324,5 +335,30 @@ int launch_eigh(const double2* A, const double2* B, int n, double* w, double2* V
   QDKP_CUDA_TRY(cudaGetLastError());
   return QDKP_OK;
 }
+
+// complex128 (plain form, refinement) and complex64 (mixed-precision search) blocks
+#define QDKP_BLOCKOPS_INST(T)                                                                      \
+  template int launch_colnorm2<T>(const cplx<T>*, long long, const cplx<T>*, long long,          \
+                                  const double*, int, long long, double*, int, double*,          \
+                                  cudaStream_t);                                                 \
+  template int launch_gram<T>(const BlockList<T>&, const BlockList<T>&, long long, double2*,     \
+                              size_t, double2*, cudaStream_t);                                   \
+  template int launch_update<T>(const BlockList<T>&, const double2* const*, int, long long,       \
+                                cplx<T>*, long long, int, cudaStream_t);
+QDKP_BLOCKOPS_INST(double)
+QDKP_BLOCKOPS_INST(float)
+#undef QDKP_BLOCKOPS_INST
+template int launch_gather<double, double>(const double2*, long long, const int*, int, long long,
+                                           double2*, long long, cudaStream_t);
+template int launch_gather<float, float>(const float2*, long long, const int*, int, long long,
+                                         float2*, long long, cudaStream_t);
+template int launch_copy<double, double>(const double2*, long long, int, long long, double2*,
+                                         long long, cudaStream_t);
+template int launch_copy<float, float>(const float2*, long long, int, long long, float2*,
+                                       long long, cudaStream_t);
+template int launch_copy<double, float>(const double2*, long long, int, long long, float2*,
+                                        long long, cudaStream_t);
+template int launch_copy<float, double>(const float2*, long long, int, long long, double2*,
+                                        long long, cudaStream_t);
 
 }  // namespace qdkp

@@ -33,23 +33,49 @@ struct BlockList {
   }
 };
 
-int launch_colnorm2(const double2* A, long long lda, const double2* B, long long ldb,
+// Tall block kernels, for complex128 (T = double) and complex64 (T = float) blocks; sums and
+// the Gram / coefficient matrices are FP64 either way.
+template <typename T>
+int launch_colnorm2(const cplx<T>* A, long long lda, const cplx<T>* B, long long ldb,
                     const double* lambda, int m, long long n, double* partial, int nparts,
                     double* out, cudaStream_t st);
 int launch_resid_gather(const double2* AX, long long ldax, const double2* X, long long ldx,
                         const double* lambda, const int* idx, int ma, long long n, double2* R,
                         long long ldr, cudaStream_t st);
-int launch_gather(const double2* src, long long lds, const int* idx, int ma, long long n,
-                  double2* dst, long long ldd, cudaStream_t st);
-int launch_copy(const double2* src, long long lds, int cols, long long n, double2* dst,
+template <typename TS, typename TD>
+int launch_gather(const cplx<TS>* src, long long lds, const int* idx, int ma, long long n,
+                  cplx<TD>* dst, long long ldd, cudaStream_t st);
+// dst = src (columns [0, cols)), converting the precision when TS != TD
+template <typename TS, typename TD>
+int launch_copy(const cplx<TS>* src, long long lds, int cols, long long n, cplx<TD>* dst,
                 long long ldd, cudaStream_t st);
+// overloads that spell the precision through the vector type (cplx<T> is not deducible)
+#define QDKP_TALL_OVERLOADS(C, R)                                                                \
+  inline int launch_colnorm2(const C* A, long long lda, const C* B, long long ldb,            \
+                             const double* lambda, int m, long long n, double* partial,       \
+                             int nparts, double* out, cudaStream_t st) {                      \
+    return launch_colnorm2<R>(A, lda, B, ldb, lambda, m, n, partial, nparts, out, st);        \
+  }                                                                                           \
+  inline int launch_gather(const C* src, long long lds, const int* idx, int ma, long long n,  \
+                           C* dst, long long ldd, cudaStream_t st) {                          \
+    return launch_gather<R, R>(src, lds, idx, ma, n, dst, ldd, st);                           \
+  }                                                                                           \
+  inline int launch_copy(const C* src, long long lds, int cols, long long n, C* dst,          \
+                         long long ldd, cudaStream_t st) {                                    \
+    return launch_copy<R, R>(src, lds, cols, n, dst, ldd, st);                                \
+  }
+QDKP_TALL_OVERLOADS(double2, double)
+QDKP_TALL_OVERLOADS(float2, float)
+#undef QDKP_TALL_OVERLOADS
 // out (P x Q, row-major, ld Q) = A^H B for concatenated column lists.
-int launch_gram(const BlockList<double>& A, const BlockList<double>& B, long long n,
+template <typename T>
+int launch_gram(const BlockList<T>& A, const BlockList<T>& B, long long n,
                 double2* partial, size_t partial_elems, double2* out, cudaStream_t st);
 size_t gram_partial_elems(int P, int Q);
 // Y = beta * Y + sum_k A_k C_k; C_k (cols_k x q, row-major, ld q) in device memory.
-int launch_update(const BlockList<double>& A, const double2* const* C, int q, long long n,
-                  double2* Y, long long ldy, int accumulate, cudaStream_t st);
+template <typename T>
+int launch_update(const BlockList<T>& A, const double2* const* C, int q, long long n,
+                  cplx<T>* Y, long long ldy, int accumulate, cudaStream_t st);
 
 // Small dense (one CTA). Matrices row-major with ld = n. status: 0 ok, 1 failure.
 int launch_chol_inv(const double2* G, int n, double2* Uinv, int* status, cudaStream_t st);

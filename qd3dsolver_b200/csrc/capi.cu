@@ -13,26 +13,10 @@ static thread_local std::string g_last_error;
 void set_error(const std::string& msg) { g_last_error = msg; }
 static std::atomic<long long> g_launches{0};
 void count_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+long long launches_so_far() { return g_launches.load(); }
 
 int launch_apply(const qdkp_operator* op, const void* X, int64_t ldx, void* Y, int64_t ldy,
                  int m, double sigma, int shifted, int precision, cudaStream_t st);
-
-__global__ void to_float_kernel(const double* __restrict__ src, float* __restrict__ dst,
-                                long long n) {
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x)
-    dst[i] = (float)src[i];
-}
-
-static int refresh_fields32(qdkp_operator* op, int first, int count) {
-  const long long n = (long long)count * op->n_sites;
-  const long long off = (long long)first * op->n_sites;
-  to_float_kernel<<<1184, 256>>>(op->fields64 + off, op->fields32 + off, n);
-  count_launch();
-  QDKP_CUDA_TRY(cudaGetLastError());
-  QDKP_CUDA_TRY(cudaDeviceSynchronize());
-  return QDKP_OK;
-}
 
 // Nonzero count of the CSR the reference assembles, counted from the stencil structure: each
 // (row band, column band) block couples a site to the offsets its operators reach, clipped at
@@ -116,16 +100,24 @@ int qdkp_operator_create(int nx, int ny, int nz, double h, int n_bands, int flag
   }
   QDKP_CUDA_TRY(cudaSetDevice(device));
   auto* op = new qdkp_operator();
+  op->fields64 = nullptr; op->rec64 = nullptr; op->rec32 = nullptr; op->nbmask = nullptr;
+  op->staged_cfg[0] = op->staged_cfg[1] = -1;
   op->nx = nx; op->ny = ny; op->nz = nz;
   op->n_sites = (int64_t)nx * ny * nz;
   op->h = h; op->n_bands = n_bands; op->flags = flags; op->device = device;
   const size_t bytes64 = (size_t)F_COUNT * op->n_sites * sizeof(double);
+  op->nzp = (nz + 3) / 4 * 4;
+  const size_t rec_doubles = record_doubles(nx, ny, op->nzp);
   cudaError_t e = cudaMalloc(&op->fields64, bytes64);
-  if (e == cudaSuccess) e = cudaMalloc(&op->fields32, bytes64 / 2);
+  if (e == cudaSuccess) e = cudaMalloc(&op->rec64, rec_doubles * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&op->rec32, rec_doubles * sizeof(float));
+  if (e == cudaSuccess) e = cudaMalloc(&op->nbmask, (size_t)op->n_sites * sizeof(unsigned));
+  // the z padding of the record stays zero
+  if (e == cudaSuccess) e = cudaMemset(op->rec64, 0, rec_doubles * sizeof(double));
+  if (e == cudaSuccess) e = cudaMemset(op->rec32, 0, rec_doubles * sizeof(float));
   if (e != cudaSuccess) {
     set_error(std::string("cudaMalloc of operator fields: ") + cudaGetErrorString(e));
-    cudaFree(op->fields64);
-    delete op;
+    qdkp_operator_destroy(op);
     return QDKP_ERR_CUDA;
   }
   for (int f = 0; f < F_COUNT; ++f) {
@@ -140,7 +132,7 @@ int qdkp_operator_create(int nx, int ny, int nz, double h, int n_bands, int flag
     qdkp_operator_destroy(op);
     return QDKP_ERR_CUDA;
   }
-  int rc = refresh_fields32(op, 0, F_COUNT);
+  int rc = build_records(op);
   if (rc != QDKP_OK) { qdkp_operator_destroy(op); return rc; }
   op->nnz_equiv = count_nnz(nx, ny, nz, n_bands, flags);
   *out = op;
@@ -155,7 +147,7 @@ int qdkp_operator_update_diagonal(qdkp_operator* op, const double* Ec, const dou
                                    cudaMemcpyHostToDevice));
   if (Ev) QDKP_CUDA_TRY(cudaMemcpy(op->fields64 + (size_t)F_EV * op->n_sites, Ev, nb,
                                    cudaMemcpyHostToDevice));
-  return refresh_fields32(op, F_EC, 2);
+  return build_records(op);
 }
 
 int qdkp_operator_info(const qdkp_operator* op, int* nx, int* ny, int* nz, int* n_bands,
@@ -182,7 +174,9 @@ int qdkp_operator_destroy(qdkp_operator* op) {
   if (!op) return QDKP_OK;
   cudaSetDevice(op->device);
   cudaFree(op->fields64);
-  cudaFree(op->fields32);
+  cudaFree(op->rec64);
+  cudaFree(op->rec32);
+  cudaFree(op->nbmask);
   delete op;
   return QDKP_OK;
 }

@@ -11,10 +11,12 @@ static __device__ __forceinline__ void dmma(double& d0, double& d1, double a, do
 }
 
 
-static __device__ __forceinline__ double2 list_elem(const BlockList<double>& L, long long r, int c) {
+template <typename T>
+static __device__ __forceinline__ double2 list_elem(const BlockList<T>& L, long long r, int c) {
   int b = 0;
   while (b < L.nblk - 1 && c >= L.cols[b]) { c -= L.cols[b]; ++b; }
-  return L.p[b][r * L.ld[b] + c];
+  const cplx<T> v = L.p[b][r * L.ld[b] + c];
+  return make_double2((double)v.x, (double)v.y);
 }
 
 
@@ -262,30 +264,34 @@ static __device__ int block_eigh(const double2* __restrict__ A, const double2* _
 // Y' = A' C'' on the FP64 tensor cores for rows [r0, r1), with A' (rows x 2P) the real view of
 // [A_0 | A_1 | A_2] and C'' (2P x 2q) the real representation of the stacked complex
 // coefficients: C''_{2i,2j} = Re C_ij, C''_{2i,2j+1} = Im C_ij, C''_{2i+1,2j} = -Im C_ij,
-// C''_{2i+1,2j+1} = Re C_ij (negated when neg). An m8n8k4 MMA takes exactly 8 rows, so each
-// warp streams its own 8-row tiles: it stages the tile's inputs in its own shared-memory slice,
-// runs the MMAs against the CTA's C'' and writes the tile's outputs; no CTA barrier in the loop.
-// A warp has staged all 8 rows before it writes any of them, so Y may alias one of the inputs.
+// C''_{2i+1,2j+1} = Re C_ij (negated when neg). Rows stream through shared memory in chunks of
+// kUpdChunk (one 8-row m8n8k4 tile per warp), double buffered with cp.async; a chunk is staged
+// completely before any of its rows is written, and a CTA owns its rows, so Y may alias one of
+// the inputs.
 constexpr int kUpdRows = 8;
 constexpr int kUpdThreads = 256;
 constexpr int kUpdWarps = kUpdThreads / 32;
+constexpr int kUpdChunk = kUpdRows * kUpdWarps;     // 64 rows per stage
 
-static __device__ __forceinline__ size_t update_smem_doubles(int P, int q) {
-  const int KPp = (2 * P + 3) / 4 * 4 + 4, NQ = (2 * q + 7) / 8 * 8;
-  return (size_t)KPp * NQ;
+__host__ __device__ __forceinline__ size_t update_smem_bytes(int P, int q, int elem_bytes) {
+  const size_t KPp = (2 * P + 3) / 4 * 4 + 4, NQ = (2 * q + 7) / 8 * 8;
+  return KPp * NQ * sizeof(double) + 2 * (size_t)kUpdChunk * P * elem_bytes;
 }
 
-static __device__ void update_rows(const BlockList<double>& A, const double2* const* C, int q,
-                                   long long r0, long long r1, double2* Y, long long ldy,
-                                   int accumulate, int neg, double* usm) {
+template <typename T>
+static __device__ void update_rows(const BlockList<T>& A, const double2* const* C, int q,
+                                   long long r0, long long r1, cplx<T>* Y, long long ldy,
+                                   int accumulate, int neg, unsigned char* smem) {
   const int P = A.total();
   const int KP = 2 * P;
   const int KPp = (KP + 3) / 4 * 4;
   const int NQ = (2 * q + 7) / 8 * 8;
-  double* sC = usm;
+  double* sC = reinterpret_cast<double*>(smem);
+  cplx<T>* stage0 = reinterpret_cast<cplx<T>*>(smem + (size_t)(KPp + 4) * NQ * sizeof(double));
+  cplx<T>* stage[2] = {stage0, stage0 + (size_t)kUpdChunk * P};
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const double sg = neg ? -1.0 : 1.0;
-  int off[3];
+  int off[3], kst[3];
   int tot = 0;
   for (int b = 0; b < A.nblk; ++b) { off[b] = tot; tot += A.cols[b]; }
   // KPp + 4 rows: a k step may run up to 3 rows past the last block (multiplied by zeros)
@@ -301,66 +307,140 @@ static __device__ void update_rows(const BlockList<double>& A, const double2* co
     sC[(2 * i + 1) * NQ + 2 * j] = -sg * c.y;
     sC[(2 * i + 1) * NQ + 2 * j + 1] = sg * c.x;
   }
-  __syncthreads();
+  for (int b = 0; b < A.nblk; ++b) kst[b] = off[b] * kUpdChunk;   // block start in a stage
   const int g = lane >> 2, t4 = lane & 3;
   const int NT = NQ / 8;
-  for (long long rb = r0 + (long long)warp * kUpdRows; rb < r1;
-       rb += (long long)kUpdWarps * kUpdRows) {
-    const long long rowg = rb + g;
-    const bool rok = rowg < r1;
-    double acc[6][2];
-#pragma unroll
-    for (int j = 0; j < 6; ++j) {
-      const int col = j * 4 + t4;
-      double2 y0 = make_double2(0.0, 0.0);
-      if (accumulate && j < NT && col < q && rok) y0 = Y[rowg * ldy + col];
-      acc[j][0] = y0.x; acc[j][1] = y0.y;
-    }
-    // A fragment of an m8n8k4 MMA: lane (g, t4) holds A'[row g][k0 + t4], i.e. the real or
-    // imaginary part of one complex element of its row -- read straight from global memory.
-    int kbase = 0;
+  const long long nrows = r1 - r0;
+  const int nchunks = (int)((nrows + kUpdChunk - 1) / kUpdChunk);
+  // the flat copy of gram_copy_rows with kUpdChunk rows per block run
+  auto stage_rows = [&](long long r, int nr, cplx<T>* dst) {
     for (int b = 0; b < A.nblk; ++b) {
-      const double* __restrict__ src =
-          reinterpret_cast<const double*>(A.p[b]) + (rok ? rowg : rb) * 2 * A.ld[b];
-      const int kb = 2 * A.cols[b];
-      for (int k = 0; k < kb; k += 4) {
-        const double a = (rok && k + t4 < kb) ? src[k + t4] : 0.0;
-        const int kr = kbase + k + t4 - t4;   // row block of C'' for this k step
-#pragma unroll
-        for (int j = 0; j < 6; ++j)
-          if (j < NT) dmma(acc[j][0], acc[j][1], a, sC[(kr + t4) * NQ + j * 8 + g]);
+      const int cols = A.cols[b];
+      const int units = nr * cols;
+      const cplx<T>* src = A.p[b] + r * A.ld[b];
+      cplx<T>* d = dst + kst[b];
+      for (int u = threadIdx.x; u < units; u += blockDim.x) {
+        const int rr = A.ld[b] == cols ? 0 : u / cols;
+        const cplx<T>* gp = A.ld[b] == cols ? src + u : src + (long long)rr * A.ld[b] + (u - rr * cols);
+        const unsigned sa = (unsigned)__cvta_generic_to_shared(d + u);
+        if (sizeof(cplx<T>) == 16)
+          asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" :: "r"(sa), "l"(gp) : "memory");
+        else
+          asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" :: "r"(sa), "l"(gp) : "memory");
       }
-      kbase += kb;
     }
+  };
+  if (nchunks > 0) stage_rows(r0, (int)min((long long)kUpdChunk, nrows), stage[0]);
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+  for (int ch = 0; ch < nchunks; ++ch) {
+    const long long rc = r0 + (long long)ch * kUpdChunk;
+    const int rows = (int)min((long long)kUpdChunk, r1 - rc);
+    if (ch + 1 < nchunks) {
+      const long long rn = rc + kUpdChunk;
+      stage_rows(rn, (int)min((long long)kUpdChunk, r1 - rn), stage[(ch + 1) & 1]);
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+    __syncthreads();
+    const int tr = warp * kUpdRows;             // this warp's 8-row tile in the chunk
+    if (tr < rows) {
+      const T* sr = reinterpret_cast<const T*>(stage[ch & 1]);
+      const int row = tr + g;
+      const bool rok = row < rows;
+      const long long rowg = rc + row;
+      double acc[6][2];
 #pragma unroll
-    for (int j = 0; j < 6; ++j) {
-      const int col = j * 4 + t4;
-      if (j < NT && col < q && rok) Y[rowg * ldy + col] = make_double2(acc[j][0], acc[j][1]);
+      for (int j = 0; j < 6; ++j) {
+        const int col = j * 4 + t4;
+        cplx<T> y0 = czero<T>();
+        if (accumulate && j < NT && col < q && rok) y0 = Y[rowg * ldy + col];
+        acc[j][0] = (double)y0.x; acc[j][1] = (double)y0.y;
+      }
+      // A fragment of an m8n8k4 MMA: lane (g, t4) holds A'[row g][k0 + t4]
+      int kbase = 0;
+      for (int b = 0; b < A.nblk; ++b) {
+        const int kb = 2 * A.cols[b];
+        const T* rs = sr + 2 * kst[b] + (rok ? row : 0) * kb;
+        for (int k = 0; k < kb; k += 4) {
+          const double a = (rok && k + t4 < kb) ? (double)rs[k + t4] : 0.0;
+          const double* cr = sC + (kbase + k + t4) * NQ + g;
+#pragma unroll
+          for (int j = 0; j < 6; ++j)
+            if (j < NT) dmma(acc[j][0], acc[j][1], a, cr[j * 8]);
+        }
+        kbase += kb;
+      }
+#pragma unroll
+      for (int j = 0; j < 6; ++j) {
+        const int col = j * 4 + t4;
+        if (j < NT && col < q && rok) Y[rowg * ldy + col] = mk<T>((T)acc[j][0], (T)acc[j][1]);
+      }
     }
+    __syncthreads();                 // the stage is overwritten by the copy two chunks on
   }
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
 
 // ---------------------------------------------------------------------------------------------
 // Gram core: partial C' = A'^T B' (real views: row r, column 2c + {re, im}) of rows [r0, r1) on
-// the FP64 MMA units. Each warp owns a rectangle of MR x MC 8x8 tiles of C' and a slice of the
-// rows; it loads its m8n8k4 fragments straight from global memory (lane (g, t4) of a k step
-// reads row k0 + t4, real column 8 tile + g: eight lanes cover 64 contiguous bytes) and keeps
-// its tiles in registers, so the row loop has no barrier. The row slices of a tile rectangle are
-// summed in shared memory in a fixed order at the end (deterministic), giving one RP x RQ
-// partial per CTA.
+// the FP64 MMA units (mma.sync.m8n8k4.f64; the tcgen05 family has no f64 kind). Rows stream
+// through shared memory in chunks of kGramRows, double buffered with cp.async: every block of
+// the two lists is copied as a flat run of chunk-rows x cols complex values (the engine's blocks
+// are compact, ld = cols; other leading dimensions are handled row by row). Each warp owns a
+// rectangle of MR x MC 8x8 tiles of C' and a slice of the chunk's 4-row k steps, reads its
+// m8n8k4 fragments from shared memory (lane (g, t4): row k0 + t4, real column 8 tile + g) and
+// keeps its tiles in registers. The row slices of a rectangle are summed in shared memory in a
+// fixed order at the end (deterministic), giving one RP x RQ partial per CTA. complex64 blocks
+// are staged as they are and widened to FP64 in the fragment loads.
 // ---------------------------------------------------------------------------------------------
 constexpr int kGramCtaThreads = 256;
+constexpr int kGramRows = 32;       // rows per shared-memory chunk (a multiple of 4)
 
-static __device__ __forceinline__ size_t gram_smem_bytes(int P, int Q) {
-  const int RP = (2 * P + 7) / 8 * 8, RQ = (2 * Q + 7) / 8 * 8;
-  return (size_t)RP * RQ * sizeof(double);
+__host__ __device__ __forceinline__ size_t gram_smem_bytes(int P, int Q, int elem_bytes) {
+  const size_t RP = (2 * P + 7) / 8 * 8, RQ = (2 * Q + 7) / 8 * 8;
+  const size_t stage = (size_t)kGramRows * (P + Q) * 2 * elem_bytes;
+  const size_t red = RP * RQ * sizeof(double);
+  const size_t st2 = 2 * stage;
+  return st2 > red ? st2 : red;
+}
+
+template <typename T>
+__device__ __forceinline__ void gram_copy_rows(const BlockList<T>& L, long long r, int nrows,
+                                               cplx<T>* dst) {
+  int off = 0;
+  for (int b = 0; b < L.nblk; ++b) {
+    const int cols = L.cols[b];
+    const int units = nrows * cols;
+    const cplx<T>* src = L.p[b] + r * L.ld[b];
+    cplx<T>* d = dst + (long long)off * kGramRows;
+    if (L.ld[b] == cols) {
+      for (int u = threadIdx.x; u < units; u += blockDim.x) {
+        const unsigned sa = (unsigned)__cvta_generic_to_shared(d + u);
+        if (sizeof(cplx<T>) == 16)
+          asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" :: "r"(sa), "l"(src + u) : "memory");
+        else
+          asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" :: "r"(sa), "l"(src + u) : "memory");
+      }
+    } else {
+      for (int u = threadIdx.x; u < units; u += blockDim.x) {
+        const int rr = u / cols, c = u - rr * cols;
+        const unsigned sa = (unsigned)__cvta_generic_to_shared(d + u);
+        const cplx<T>* g = src + (long long)rr * L.ld[b] + c;
+        if (sizeof(cplx<T>) == 16)
+          asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" :: "r"(sa), "l"(g) : "memory");
+        else
+          asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" :: "r"(sa), "l"(g) : "memory");
+      }
+    }
+    off += cols;
+  }
 }
 
 // tile rectangles: tile rows split in groups of MR, tile columns in groups of MC
-template <int MR, int MC>
-static __device__ void gram_core(const BlockList<double>& A, const BlockList<double>& B,
+template <int MR, int MC, typename T>
+static __device__ void gram_core(const BlockList<T>& A, const BlockList<T>& B,
                                  long long r0, long long r1, double* __restrict__ out,
-                                 double* gsm) {
+                                 unsigned char* smem) {
   const int P = A.total(), Q = B.total();
   const int RP = (2 * P + 7) / 8 * 8, RQ = (2 * Q + 7) / 8 * 8;
   const int TR = RP / 8, TC = RQ / 8;
@@ -373,68 +453,86 @@ static __device__ void gram_core(const BlockList<double>& A, const BlockList<dou
   const int rect = warp % G, slice = warp / G;
   const bool active_warp = slice < slices;
   const int tr0 = (rect / GC) * MR, tc0 = (rect % GC) * MC;
-  // per tile: block index (-1: outside P / Q) and the real column inside that block's row
-  int ba[MR], ca[MR], bb[MC], cb[MC];
+  // stage layout: per list, per block, kGramRows x cols complex values; A's blocks first
+  cplx<T>* stage[2];
+  stage[0] = reinterpret_cast<cplx<T>*>(smem);
+  stage[1] = stage[0] + (size_t)kGramRows * (P + Q);
+  // per tile: the real offset of its column inside a staged row block (-1: outside P / Q)
+  // as (block start in complex columns * kGramRows, block width, real column in the row)
+  int sa_off[MR], sa_w[MR], sa_c[MR], sb_off[MC], sb_w[MC], sb_c[MC];
 #pragma unroll
   for (int i = 0; i < MR; ++i) {
     const int col = (tr0 + i) * 8 + g;           // real column of A'
-    int c = col >> 1, blk = 0;
-    while (blk < A.nblk - 1 && c >= A.cols[blk]) { c -= A.cols[blk]; ++blk; }
+    int c = col >> 1, blk = 0, start = 0;
+    while (blk < A.nblk - 1 && c >= A.cols[blk]) { c -= A.cols[blk]; start += A.cols[blk]; ++blk; }
     const bool ok = active_warp && tr0 + i < TR && col < 2 * P;
-    ba[i] = ok ? blk : -1;
-    ca[i] = 2 * c + (col & 1);
+    sa_off[i] = ok ? start * kGramRows : -1;
+    sa_w[i] = A.cols[blk];
+    sa_c[i] = 2 * c + (col & 1);
   }
 #pragma unroll
   for (int j = 0; j < MC; ++j) {
     const int col = (tc0 + j) * 8 + g;
-    int c = col >> 1, blk = 0;
-    while (blk < B.nblk - 1 && c >= B.cols[blk]) { c -= B.cols[blk]; ++blk; }
+    int c = col >> 1, blk = 0, start = 0;
+    while (blk < B.nblk - 1 && c >= B.cols[blk]) { c -= B.cols[blk]; start += B.cols[blk]; ++blk; }
     const bool ok = active_warp && tc0 + j < TC && col < 2 * Q;
-    bb[j] = ok ? blk : -1;
-    cb[j] = 2 * c + (col & 1);
+    sb_off[j] = ok ? (P + start) * kGramRows : -1;
+    sb_w[j] = B.cols[blk];
+    sb_c[j] = 2 * c + (col & 1);
   }
-  const double* A0 = reinterpret_cast<const double*>(A.p[0]);
-  const double* A1 = reinterpret_cast<const double*>(A.nblk > 1 ? A.p[1] : A.p[0]);
-  const double* A2 = reinterpret_cast<const double*>(A.nblk > 2 ? A.p[2] : A.p[0]);
-  const double* B0 = reinterpret_cast<const double*>(B.p[0]);
-  const double* B1 = reinterpret_cast<const double*>(B.nblk > 1 ? B.p[1] : B.p[0]);
-  const double* B2 = reinterpret_cast<const double*>(B.nblk > 2 ? B.p[2] : B.p[0]);
-  const long long la0 = 2 * A.ld[0], la1 = A.nblk > 1 ? 2 * A.ld[1] : 0, la2 = A.nblk > 2 ? 2 * A.ld[2] : 0;
-  const long long lb0 = 2 * B.ld[0], lb1 = B.nblk > 1 ? 2 * B.ld[1] : 0, lb2 = B.nblk > 2 ? 2 * B.ld[2] : 0;
   double acc[MR][MC][2];
 #pragma unroll
   for (int i = 0; i < MR; ++i)
 #pragma unroll
     for (int j = 0; j < MC; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
-  if (active_warp) {
-#pragma unroll 2
-    for (long long k0 = r0 + 4LL * slice; k0 < r1; k0 += 4LL * slices) {
-      const long long row = k0 + t4;
-      const bool ok = row < r1;
-      const double* ra0 = A0 + row * la0;
-      const double* ra1 = A1 + row * la1;
-      const double* ra2 = A2 + row * la2;
-      const double* rb0 = B0 + row * lb0;
-      const double* rb1 = B1 + row * lb1;
-      const double* rb2 = B2 + row * lb2;
-      double a[MR], b[MC];
-#pragma unroll
-      for (int i = 0; i < MR; ++i) {
-        const double* base = ba[i] == 0 ? ra0 : (ba[i] == 1 ? ra1 : ra2);
-        a[i] = (ok && ba[i] >= 0) ? __ldg(base + ca[i]) : 0.0;
-      }
-#pragma unroll
-      for (int j = 0; j < MC; ++j) {
-        const double* base = bb[j] == 0 ? rb0 : (bb[j] == 1 ? rb1 : rb2);
-        b[j] = (ok && bb[j] >= 0) ? __ldg(base + cb[j]) : 0.0;
-      }
-#pragma unroll
-      for (int i = 0; i < MR; ++i)
-#pragma unroll
-        for (int j = 0; j < MC; ++j) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
-    }
+
+  const long long nrows = r1 - r0;
+  const int nchunks = (int)((nrows + kGramRows - 1) / kGramRows);
+  if (nchunks > 0) {
+    const int n0 = (int)min((long long)kGramRows, nrows);
+    gram_copy_rows(A, r0, n0, stage[0]);
+    gram_copy_rows(B, r0, n0, stage[0] + (size_t)P * kGramRows);
   }
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+  for (int ch = 0; ch < nchunks; ++ch) {
+    const long long rc = r0 + (long long)ch * kGramRows;
+    const int rows = (int)min((long long)kGramRows, r1 - rc);
+    if (ch + 1 < nchunks) {
+      const long long rn = rc + kGramRows;
+      const int nn = (int)min((long long)kGramRows, r1 - rn);
+      cplx<T>* st = stage[(ch + 1) & 1];
+      gram_copy_rows(A, rn, nn, st);
+      gram_copy_rows(B, rn, nn, st + (size_t)P * kGramRows);
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+    __syncthreads();
+    const T* sr = reinterpret_cast<const T*>(stage[ch & 1]);
+    if (active_warp) {
+      for (int k0 = 4 * slice; k0 < rows; k0 += 4 * slices) {
+        const int row = k0 + t4;
+        const bool ok = row < rows;
+        double a[MR], b[MC];
+#pragma unroll
+        for (int i = 0; i < MR; ++i)
+          a[i] = (ok && sa_off[i] >= 0)
+                     ? (double)sr[2 * sa_off[i] + row * 2 * sa_w[i] + sa_c[i]] : 0.0;
+#pragma unroll
+        for (int j = 0; j < MC; ++j)
+          b[j] = (ok && sb_off[j] >= 0)
+                     ? (double)sr[2 * sb_off[j] + row * 2 * sb_w[j] + sb_c[j]] : 0.0;
+#pragma unroll
+        for (int i = 0; i < MR; ++i)
+#pragma unroll
+          for (int j = 0; j < MC; ++j) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+      }
+    }
+    __syncthreads();                 // the stage is overwritten by the copy two chunks on
+  }
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+  __syncthreads();
   // fixed-order sum of the row slices of each rectangle
+  double* gsm = reinterpret_cast<double*>(smem);
   for (int e = threadIdx.x; e < RP * RQ; e += blockDim.x) gsm[e] = 0.0;
   __syncthreads();
   for (int sl = 0; sl < slices; ++sl) {

@@ -20,6 +20,9 @@ int launch_apply(const qdkp_operator* op, const void* X, int64_t ldx, void* Y, i
 constexpr int kERowsPerCta = 512;    // rows per CTA of the row kernels
 constexpr int kENormRows = 2048;     // rows per CTA of the norm kernel
 constexpr int kEGramSplit = 16;
+// Gram CTAs per slot: ceil(n / 256) up to this many. The split depends only on the slot's own
+// size, so the order of every Gram sum -- and so the result -- is the same alone and in a mix.
+constexpr int kEGramMaxParts = 296;
 
 enum GramWhich { GR_XR = 0, GR_RR, GR_PP, GR_WW, GR_WAW, GR_BA, GR_BB };
 enum UpdWhich { UP_RPROJ = 0, UP_RNORM, UP_PNORM, UP_APNORM, UP_PNEW, UP_APNEW, UP_XNEW, UP_AXNEW };
@@ -28,13 +31,11 @@ enum RowWhich { RW_COPYBEST = 0, RW_RESID, RW_GATHERP };
 // ---------------------------------------------------------------------------------------------
 // residual norms of A X - X lambda: partials per CTA, reduced in the decision kernel
 // ---------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(kTallThreads)
-e_norm_kernel(const ESlot* __restrict__ S, int ns) {
-  const int k = slot_of(S, ns, blockIdx.x, &ESlot::norm0);
-  const ESlot& d = S[k];
+template <typename T>
+__device__ __forceinline__ void e_norm_body(const ESlot& d, int part) {
   const EState* st = d.st;
-  if (!st->running) return;
-  const int part = blockIdx.x - d.norm0;
+  const cplx<T>* AX = blk<T>(d.AX);
+  const cplx<T>* X = blk<T>(d.X);
   const int m = d.m;
   const long long r0 = (long long)part * kENormRows;
   const long long r1 = min(d.n, r0 + kENormRows);
@@ -45,9 +46,9 @@ e_norm_kernel(const ESlot* __restrict__ S, int ns) {
 #pragma unroll
     for (int j = 0; j < kMaxBlock; ++j) {
       if (j < m) {
-        const double2 a = d.AX[r * m + j], x = d.X[r * m + j];
+        const cplx<T> a = AX[r * m + j], x = X[r * m + j];
         const double l = st->lam[j];
-        const double re = a.x - l * x.x, im = a.y - l * x.y;
+        const double re = (double)a.x - l * (double)x.x, im = (double)a.y - l * (double)x.y;
         acc[j] = fma(re, re, fma(im, im, acc[j]));
       }
     }
@@ -68,6 +69,15 @@ e_norm_kernel(const ESlot* __restrict__ S, int ns) {
     for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w][threadIdx.x];
     d.npart[(long long)part * m + threadIdx.x] = s;
   }
+}
+
+__global__ void __launch_bounds__(kTallThreads)
+e_norm_kernel(const ESlot* __restrict__ S, int ns) {
+  const int k = slot_of(S, ns, blockIdx.x, &ESlot::norm0);
+  const ESlot& d = S[k];
+  if (!d.st->running) return;
+  if (d.prec == QDKP_C64) e_norm_body<float>(d, blockIdx.x - d.norm0);
+  else e_norm_body<double>(d, blockIdx.x - d.norm0);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -114,8 +124,7 @@ __global__ void e_decide_kernel(const ESlot* __restrict__ S) {
   }
   st->ma = ma;
   if (ma == 0) { st->running = 0; st->status = QDKP_LOBPCG_CONVERGED; return; }
-  const double myeps = 1.4901161193847656e-08;   // sqrt(eps) for complex128
-  st->explicit_gram = !(mx > myeps && !st->explicit_gram);
+  st->explicit_gram = !(mx > d.sqrt_eps && !st->explicit_gram);
   st->idle = 0;
   st->skip_p = st->iter == 0 ? 1 : 0;
 }
@@ -123,87 +132,110 @@ __global__ void e_decide_kernel(const ESlot* __restrict__ S) {
 // ---------------------------------------------------------------------------------------------
 // row kernels: copy of the best iterate, residual gather, P gather
 // ---------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(kTallThreads)
-e_row_kernel(const ESlot* __restrict__ S, int ns, int which) {
-  const int k = slot_of(S, ns, blockIdx.x, &ESlot::row0);
-  const ESlot& d = S[k];
+template <typename T>
+__device__ __forceinline__ void e_row_body(const ESlot& d, int which, long long r0,
+                                           long long r1) {
   const EState* st = d.st;
   const int m = d.m;
-  if (which == RW_COPYBEST) { if (!st->copy_best) return; }
-  else if (st->idle || (which == RW_GATHERP && st->skip_p)) return;
-  const long long r0 = (long long)(blockIdx.x - d.row0) * d.rows_per_cta;
-  const long long r1 = min(d.n, r0 + d.rows_per_cta);
   const int ma = st->ma;
+  const cplx<T>* X = blk<T>(d.X);
   if (which == RW_COPYBEST) {
-    for (long long e = r0 * m + threadIdx.x; e < r1 * m; e += blockDim.x) d.best[e] = d.X[e];
+    cplx<T>* best = blk<T>(d.best);
+    for (long long e = r0 * m + threadIdx.x; e < r1 * m; e += blockDim.x) best[e] = X[e];
   } else if (which == RW_RESID) {
+    const cplx<T>* AX = blk<T>(d.AX);
+    cplx<T>* Ra = blk<T>(d.Ra);
     for (long long e = r0 * ma + threadIdx.x; e < r1 * ma; e += blockDim.x) {
       const long long r = e / ma;
       const int c = (int)(e - r * ma);
       const int j = st->idx[c];
       const double l = st->lam[j];
-      const double2 a = d.AX[r * m + j], x = d.X[r * m + j];
-      d.Ra[e] = make_double2(a.x - l * x.x, a.y - l * x.y);
+      const cplx<T> a = AX[r * m + j], x = X[r * m + j];
+      Ra[e] = mk<T>((T)((double)a.x - l * (double)x.x), (T)((double)a.y - l * (double)x.y));
     }
   } else {
+    const cplx<T>* P = blk<T>(d.P);
+    const cplx<T>* AP = blk<T>(d.AP);
+    cplx<T>* Pa = blk<T>(d.Pa);
+    cplx<T>* APa = blk<T>(d.APa);
     for (long long e = r0 * ma + threadIdx.x; e < r1 * ma; e += blockDim.x) {
       const long long r = e / ma;
       const int c = (int)(e - r * ma);
       const int j = st->idx[c];
-      d.Pa[e] = d.P[r * m + j];
-      d.APa[e] = d.AP[r * m + j];
+      Pa[e] = P[r * m + j];
+      APa[e] = AP[r * m + j];
     }
   }
+}
+
+__global__ void __launch_bounds__(kTallThreads)
+e_row_kernel(const ESlot* __restrict__ S, int ns, int which) {
+  const int k = slot_of(S, ns, blockIdx.x, &ESlot::row0);
+  const ESlot& d = S[k];
+  const EState* st = d.st;
+  if (which == RW_COPYBEST) { if (!st->copy_best) return; }
+  else if (st->idle || (which == RW_GATHERP && st->skip_p)) return;
+  const long long r0 = (long long)(blockIdx.x - d.row0) * d.rows_per_cta;
+  const long long r1 = min(d.n, r0 + d.rows_per_cta);
+  if (d.prec == QDKP_C64) e_row_body<float>(d, which, r0, r1);
+  else e_row_body<double>(d, which, r0, r1);
 }
 
 // ---------------------------------------------------------------------------------------------
 // Gram products, multi-slot (same FP64 MMA scheme as gram_partial_kernel)
 // ---------------------------------------------------------------------------------------------
-__device__ bool gram_lists(const ESlot& d, int which, BlockList<double>& A, BlockList<double>& B,
+template <typename T>
+__device__ bool gram_lists(const ESlot& d, int which, BlockList<T>& A, BlockList<T>& B,
                            double2*& out) {
   const EState* st = d.st;
   if (st->idle) return false;
   const int m = d.m, ma = st->ma, mp = st->mp;
-  auto set1 = [](BlockList<double>& L, const double2* p, int c) {
+  auto set1 = [](BlockList<T>& L, const cplx<T>* p, int c) {
     L.nblk = 1; L.p[0] = p; L.ld[0] = c; L.cols[0] = c;
   };
+  const cplx<T>* X = blk<T>(d.X);
+  const cplx<T>* AX = blk<T>(d.AX);
+  const cplx<T>* Ra = blk<T>(d.Ra);
+  const cplx<T>* ARa = blk<T>(d.ARa);
+  const cplx<T>* Pa = blk<T>(d.Pa);
+  const cplx<T>* APa = blk<T>(d.APa);
   switch (which) {
-    case GR_XR: set1(A, d.X, m); set1(B, d.Ra, ma); out = d.W; return true;
-    case GR_RR: set1(A, d.Ra, ma); set1(B, d.Ra, ma); out = d.G; return true;
+    case GR_XR: set1(A, X, m); set1(B, Ra, ma); out = d.W; return true;
+    case GR_RR: set1(A, Ra, ma); set1(B, Ra, ma); out = d.G; return true;
     case GR_PP:
       if (st->skip_p) return false;
-      set1(A, d.Pa, ma); set1(B, d.Pa, ma); out = d.G; return true;
+      set1(A, Pa, ma); set1(B, Pa, ma); out = d.G; return true;
     case GR_BA:      // non-explicit: [X | R | P]^H [AR | AP]
       if (st->explicit_gram) return false;
       A.nblk = mp ? 3 : 2;
-      A.p[0] = d.X; A.ld[0] = m; A.cols[0] = m;
-      A.p[1] = d.Ra; A.ld[1] = ma; A.cols[1] = ma;
-      A.p[2] = d.Pa; A.ld[2] = ma; A.cols[2] = mp;
+      A.p[0] = X; A.ld[0] = m; A.cols[0] = m;
+      A.p[1] = Ra; A.ld[1] = ma; A.cols[1] = ma;
+      A.p[2] = Pa; A.ld[2] = ma; A.cols[2] = mp;
       B.nblk = mp ? 2 : 1;
-      B.p[0] = d.ARa; B.ld[0] = ma; B.cols[0] = ma;
-      B.p[1] = d.APa; B.ld[1] = ma; B.cols[1] = mp;
+      B.p[0] = ARa; B.ld[0] = ma; B.cols[0] = ma;
+      B.p[1] = APa; B.ld[1] = ma; B.cols[1] = mp;
       out = d.gT;
       return true;
     case GR_BB:      // non-explicit: [X | R]^H P
       if (st->explicit_gram || mp == 0) return false;
       A.nblk = 2;
-      A.p[0] = d.X; A.ld[0] = m; A.cols[0] = m;
-      A.p[1] = d.Ra; A.ld[1] = ma; A.cols[1] = ma;
-      set1(B, d.Pa, mp);
+      A.p[0] = X; A.ld[0] = m; A.cols[0] = m;
+      A.p[1] = Ra; A.ld[1] = ma; A.cols[1] = ma;
+      set1(B, Pa, mp);
       B.ld[0] = ma;
       out = d.gS;
       return true;
     default: {       // explicit Gram mode: the full W^H W and W^H AW
       if (!st->explicit_gram) return false;
       A.nblk = mp ? 3 : 2;
-      A.p[0] = d.X; A.ld[0] = m; A.cols[0] = m;
-      A.p[1] = d.Ra; A.ld[1] = ma; A.cols[1] = ma;
-      A.p[2] = d.Pa; A.ld[2] = ma; A.cols[2] = mp;
+      A.p[0] = X; A.ld[0] = m; A.cols[0] = m;
+      A.p[1] = Ra; A.ld[1] = ma; A.cols[1] = ma;
+      A.p[2] = Pa; A.ld[2] = ma; A.cols[2] = mp;
       if (which == GR_WW) { B = A; out = d.gS; return true; }
       B.nblk = A.nblk;
-      B.p[0] = d.AX; B.ld[0] = m; B.cols[0] = m;
-      B.p[1] = d.ARa; B.ld[1] = ma; B.cols[1] = ma;
-      B.p[2] = d.APa; B.ld[2] = ma; B.cols[2] = mp;
+      B.p[0] = AX; B.ld[0] = m; B.cols[0] = m;
+      B.p[1] = ARa; B.ld[1] = ma; B.cols[1] = ma;
+      B.p[2] = APa; B.ld[2] = ma; B.cols[2] = mp;
       out = d.gT;
       return true;
     }
@@ -215,25 +247,33 @@ __device__ bool gram_lists(const ESlot& d, int which, BlockList<double>& A, Bloc
 template <int MR, int MC>
 __global__ void __launch_bounds__(512)
 e_gram_kernel(const ESlot* __restrict__ S, int ns, int which, int m_only) {
-  extern __shared__ double gsm_e[];
+  extern __shared__ __align__(16) unsigned char gsm_e[];
   const int k = slot_of(S, ns, blockIdx.x, &ESlot::gram0);
   const ESlot& d = S[k];
   if (d.m != m_only) return;
-  BlockList<double> A, B;
-  double2* out;
-  if (!gram_lists(d, which, A, B, out)) return;
   const int part = blockIdx.x - d.gram0;
-  const int RP = (2 * A.total() + 7) / 8 * 8, RQ = (2 * B.total() + 7) / 8 * 8;
   const long long r0 = (long long)part * d.rows_per_gpart;
-  gram_core<MR, MC>(A, B, r0, min(d.n, r0 + d.rows_per_gpart),
-                    d.gpart + (long long)part * RP * RQ, gsm_e);
+  double2* out;
+  if (d.prec == QDKP_C64) {
+    BlockList<float> A, B;
+    if (!gram_lists<float>(d, which, A, B, out)) return;
+    const int RP = (2 * A.total() + 7) / 8 * 8, RQ = (2 * B.total() + 7) / 8 * 8;
+    gram_core<MR, MC>(A, B, r0, min(d.n, r0 + d.rows_per_gpart),
+                      d.gpart + (long long)part * RP * RQ, gsm_e);
+  } else {
+    BlockList<double> A, B;
+    if (!gram_lists<double>(d, which, A, B, out)) return;
+    const int RP = (2 * A.total() + 7) / 8 * 8, RQ = (2 * B.total() + 7) / 8 * 8;
+    gram_core<MR, MC>(A, B, r0, min(d.n, r0 + d.rows_per_gpart),
+                      d.gpart + (long long)part * RP * RQ, gsm_e);
+  }
 }
 
 __global__ void e_gram_reduce1(const ESlot* __restrict__ S, int which) {
   const ESlot& d = S[blockIdx.z];
-  BlockList<double> A, B;
+  BlockList<double> A, B;       // column counts only (the block pointers are not read here)
   double2* out;
-  if (!gram_lists(d, which, A, B, out)) return;
+  if (!gram_lists<double>(d, which, A, B, out)) return;
   const int P = A.total(), Q = B.total();
   const int RP = (2 * P + 7) / 8 * 8, RQ = (2 * Q + 7) / 8 * 8;
   const int elems = RP * RQ;
@@ -248,9 +288,9 @@ __global__ void e_gram_reduce1(const ESlot* __restrict__ S, int which) {
 
 __global__ void e_gram_reduce2(const ESlot* __restrict__ S, int which) {
   const ESlot& d = S[blockIdx.y];
-  BlockList<double> A, B;
+  BlockList<double> A, B;       // column counts only (the block pointers are not read here)
   double2* out;
-  if (!gram_lists(d, which, A, B, out)) return;
+  if (!gram_lists<double>(d, which, A, B, out)) return;
   const int P = A.total(), Q = B.total();
   const int RP = (2 * P + 7) / 8 * 8, RQ = (2 * Q + 7) / 8 * 8;
   const int elems = RP * RQ;
@@ -270,50 +310,58 @@ __global__ void e_gram_reduce2(const ESlot* __restrict__ S, int which) {
 // ---------------------------------------------------------------------------------------------
 // block updates, multi-slot (FP64 MMA, rows staged through shared memory: in-place safe)
 // ---------------------------------------------------------------------------------------------
-__device__ bool upd_lists(const ESlot& d, int which, BlockList<double>& A, const double2* C[3],
-                          int& q, double2*& Y, int& accumulate, int& neg) {
+template <typename T>
+__device__ bool upd_lists(const ESlot& d, int which, BlockList<T>& A, const double2* C[3],
+                          int& q, cplx<T>*& Y, int& accumulate, int& neg) {
   const EState* st = d.st;
   if (st->idle) return false;
   const int m = d.m, ma = st->ma, mp = st->mp;
   accumulate = 0; neg = 0;
-  auto set = [&](int i, const double2* p, int ld, int c, const double2* cf) {
-    A.p[i] = p; A.ld[i] = ld; A.cols[i] = c; C[i] = cf;
+  auto set = [&](int i, double2* p, int ld, int c, const double2* cf) {
+    A.p[i] = blk<T>(p); A.ld[i] = ld; A.cols[i] = c; C[i] = cf;
   };
   switch (which) {
-    case UP_RPROJ: A.nblk = 1; set(0, d.X, m, m, d.W); q = ma; Y = d.Ra; accumulate = 1; neg = 1; return true;
-    case UP_RNORM: A.nblk = 1; set(0, d.Ra, ma, ma, d.U); q = ma; Y = d.Ra; return true;
+    case UP_RPROJ: A.nblk = 1; set(0, d.X, m, m, d.W); q = ma; Y = blk<T>(d.Ra); accumulate = 1; neg = 1; return true;
+    case UP_RNORM: A.nblk = 1; set(0, d.Ra, ma, ma, d.U); q = ma; Y = blk<T>(d.Ra); return true;
     case UP_PNORM:
       if (st->skip_pnorm) return false;
-      A.nblk = 1; set(0, d.Pa, ma, ma, d.U); q = ma; Y = d.Pa; return true;
+      A.nblk = 1; set(0, d.Pa, ma, ma, d.U); q = ma; Y = blk<T>(d.Pa); return true;
     case UP_APNORM:
       if (st->skip_pnorm) return false;
-      A.nblk = 1; set(0, d.APa, ma, ma, d.U); q = ma; Y = d.APa; return true;
+      A.nblk = 1; set(0, d.APa, ma, ma, d.U); q = ma; Y = blk<T>(d.APa); return true;
     case UP_PNEW:
       A.nblk = mp ? 2 : 1; set(0, d.Ra, ma, ma, d.Cr); set(1, d.Pa, ma, mp, d.Cp);
-      q = m; Y = d.P; return true;
+      q = m; Y = blk<T>(d.P); return true;
     case UP_APNEW:
       A.nblk = mp ? 2 : 1; set(0, d.ARa, ma, ma, d.Cr); set(1, d.APa, ma, mp, d.Cp);
-      q = m; Y = d.AP; return true;
+      q = m; Y = blk<T>(d.AP); return true;
     case UP_XNEW:
-      A.nblk = 2; set(0, d.X, m, m, d.Cx); set(1, d.P, m, m, d.Im); q = m; Y = d.X; return true;
+      A.nblk = 2; set(0, d.X, m, m, d.Cx); set(1, d.P, m, m, d.Im); q = m; Y = blk<T>(d.X); return true;
     default:
-      A.nblk = 2; set(0, d.AX, m, m, d.Cx); set(1, d.AP, m, m, d.Im); q = m; Y = d.AX; return true;
+      A.nblk = 2; set(0, d.AX, m, m, d.Cx); set(1, d.AP, m, m, d.Im); q = m; Y = blk<T>(d.AX); return true;
   }
 }
 
 __global__ void __launch_bounds__(kUpdThreads)
 e_update_kernel(const ESlot* __restrict__ S, int ns, int which) {
-  extern __shared__ double usm_e[];
+  extern __shared__ __align__(16) unsigned char usm_e[];
   const int k = slot_of(S, ns, blockIdx.x, &ESlot::row0);
   const ESlot& d = S[k];
-  BlockList<double> A;
   const double2* Cf[3];
   int q, accumulate, neg;
-  double2* Y;
-  if (!upd_lists(d, which, A, Cf, q, Y, accumulate, neg)) return;
   const long long r0 = (long long)(blockIdx.x - d.row0) * d.rows_per_cta;
   const long long r1 = min(d.n, r0 + d.rows_per_cta);
-  update_rows(A, Cf, q, r0, r1, Y, (long long)q, accumulate, neg, usm_e);
+  if (d.prec == QDKP_C64) {
+    BlockList<float> A;
+    float2* Y;
+    if (!upd_lists<float>(d, which, A, Cf, q, Y, accumulate, neg)) return;
+    update_rows(A, Cf, q, r0, r1, Y, (long long)q, accumulate, neg, usm_e);
+  } else {
+    BlockList<double> A;
+    double2* Y;
+    if (!upd_lists<double>(d, which, A, Cf, q, Y, accumulate, neg)) return;
+    update_rows(A, Cf, q, r0, r1, Y, (long long)q, accumulate, neg, usm_e);
+  }
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -462,14 +510,14 @@ struct SlotLayout {
   long long rows_per_gpart;
 };
 
-SlotLayout slot_layout(int64_t n, int m) {
+SlotLayout slot_layout(int64_t n, int m, int prec) {
   SlotLayout L;
-  L.blk = align256((size_t)n * m * sizeof(double2));
+  L.blk = align256((size_t)n * m * (prec == QDKP_C64 ? sizeof(float2) : sizeof(double2)));
   L.small = align256((size_t)(3 * m) * (3 * m) * sizeof(double2));
   L.nparts = (int)((n + kENormRows - 1) / kENormRows);
   L.npart = align256((size_t)L.nparts * m * sizeof(double));
   long long parts = (n + 255) / 256;
-  if (parts > 296) parts = 296;
+  if (parts > kEGramMaxParts) parts = kEGramMaxParts;
   if (parts < 1) parts = 1;
   long long rpp = (n + parts - 1) / parts;
   rpp = (rpp + 3) / 4 * 4;
@@ -490,38 +538,82 @@ struct qdkp_engine {
   int max_slots = 0;
   std::vector<qdkp::SlotHost> slots;
   qdkp::ESlot* d_slots = nullptr;      // compact array of the used slots
-  qdkp::HXSlot* d_hx = nullptr;        // 4 x max_slots H.X descriptors
+  qdkp::HXSlot* d_hx = nullptr;        // [precision][phase][slot]: 2 x 4 x max_slots H.X descriptors
   int* d_one = nullptr;                // constant 1 (skip flag)
   std::vector<int> order;              // slot ids in compact order
-  int ns = 0, norm_ctas = 0, gram_ctas = 0, row_ctas = 0, hx_tiles = 0, S_max = 32;
+  int ns = 0, norm_ctas = 0, gram_ctas = 0, row_ctas = 0;
+  int hx_ns[2] = {0, 0}, hx_tiles[2] = {0, 0};   // per precision (QDKP_C128, QDKP_C64)
   int maxT = 2, m_max = 1;
   std::vector<int> widths;             // distinct block widths among the used slots
   bool dirty = true;
+  // CUDA graph of `graph_ticks` ticks over the current slot layout, replayed by
+  // qdkp_engine_step on the engine's own stream (ordered after the caller's stream by events)
+  cudaStream_t gstream = nullptr;
+  cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+  cudaGraphExec_t graph = nullptr;
+  int graph_ticks = 0;
+  bool use_graph = true;
+  long long launches_per_tick = 0;     // kernels one tick launches (graph replays count them)
 };
 
 namespace qdkp {
 namespace {
 
-int apply_folded(const SlotHost& h, const double2* V, int c, double2* out, cudaStream_t st) {
+// Host helpers on a slot's tall blocks, in the slot's precision (the block pointers are typed
+// double2 in ESlot and hold complex64 values for a QDKP_C64 slot).
+int apply_folded(const SlotHost& h, const void* V, int c, void* out, cudaStream_t st) {
   const ESlot& d = h.d;
   if (h.prm.folded) {
-    int rc = launch_apply(h.op, V, c, d.T, c, c, h.prm.sigma, 1, QDKP_C128, st);
+    int rc = launch_apply(h.op, V, c, d.T, c, c, h.prm.sigma, 1, d.prec, st);
     if (rc) return rc;
-    return launch_apply(h.op, d.T, c, out, c, c, h.prm.sigma, 1, QDKP_C128, st);
+    return launch_apply(h.op, d.T, c, out, c, c, h.prm.sigma, 1, d.prec, st);
   }
-  return launch_apply(h.op, V, c, out, c, c, 0.0, 0, QDKP_C128, st);
+  return launch_apply(h.op, V, c, out, c, c, 0.0, 0, d.prec, st);
 }
 
-BlockList<double> one(const double2* p, int c) {
-  BlockList<double> L;
-  L.nblk = 1; L.p[0] = p; L.ld[0] = c; L.cols[0] = c;
+template <typename T>
+BlockList<T> one(const void* p, int c) {
+  BlockList<T> L;
+  L.nblk = 1; L.p[0] = static_cast<const cplx<T>*>(p); L.ld[0] = c; L.cols[0] = c;
   return L;
 }
 
-int gram1(const SlotHost& h, const double2* A, const double2* B, int m, double2* out,
+int gram1(const SlotHost& h, const void* A, const void* B, int m, double2* out,
           cudaStream_t st) {
   const size_t elems = h.gpart_doubles / 2;
-  return launch_gram(one(A, m), one(B, m), h.d.n, reinterpret_cast<double2*>(h.d.gpart), elems, out, st);
+  double2* part = reinterpret_cast<double2*>(h.d.gpart);
+  if (h.d.prec == QDKP_C64)
+    return launch_gram(one<float>(A, m), one<float>(B, m), h.d.n, part, elems, out, st);
+  return launch_gram(one<double>(A, m), one<double>(B, m), h.d.n, part, elems, out, st);
+}
+
+// Y (n x q) = A (n x m) C (m x q)
+int update1(const SlotHost& h, const void* A, int m, const double2* C, int q, void* Y,
+            cudaStream_t st) {
+  const double2* Cs[1] = {C};
+  if (h.d.prec == QDKP_C64)
+    return launch_update(one<float>(A, m), Cs, q, h.d.n, static_cast<float2*>(Y), q, 0, st);
+  return launch_update(one<double>(A, m), Cs, q, h.d.n, static_cast<double2*>(Y), q, 0, st);
+}
+
+// out[j] = sum_r |A[r, j] - lambda_j B[r, j]|^2, summed on the device into out (device)
+int colnorm1(const SlotHost& h, const void* A, const void* B, const double* lam, int m,
+             double* out, cudaStream_t st) {
+  const ESlot& d = h.d;
+  if (d.prec == QDKP_C64)
+    return launch_colnorm2<float>(static_cast<const float2*>(A), m, static_cast<const float2*>(B),
+                                  m, lam, m, d.n, d.npart, d.nparts, out, st);
+  return launch_colnorm2<double>(static_cast<const double2*>(A), m,
+                                 static_cast<const double2*>(B), m, lam, m, d.n, d.npart,
+                                 d.nparts, out, st);
+}
+
+int copy1(const SlotHost& h, const void* src, int m, void* dst, cudaStream_t st) {
+  if (h.d.prec == QDKP_C64)
+    return launch_copy<float, float>(static_cast<const float2*>(src), m, m, h.d.n,
+                                     static_cast<float2*>(dst), m, st);
+  return launch_copy<double, double>(static_cast<const double2*>(src), m, m, h.d.n,
+                                     static_cast<double2*>(dst), m, st);
 }
 
 int read_sync(void* host, const void* dev, size_t bytes, cudaStream_t st) {
@@ -532,9 +624,11 @@ int read_sync(void* host, const void* dev, size_t bytes, cudaStream_t st) {
 
 int rebuild(qdkp_engine* e, cudaStream_t st) {
   std::vector<ESlot> compact;
-  std::vector<HXSlot> hx(4 * (size_t)e->max_slots);
+  std::vector<HXSlot> hx(8 * (size_t)e->max_slots);
   e->order.clear();
-  int norm0 = 0, gram0 = 0, row0 = 0, tile0 = 0, S_max = 32, m_max = 1;
+  int norm0 = 0, gram0 = 0, row0 = 0, m_max = 1;
+  int tile0[2] = {0, 0}, kp[2] = {0, 0};
+
   for (int i = 0; i < e->max_slots; ++i) {
     SlotHost& h = e->slots[i];
     if (!h.used) continue;
@@ -543,20 +637,20 @@ int rebuild(qdkp_engine* e, cudaStream_t st) {
     d.gram0 = gram0; gram0 += d.gparts;
     d.row0 = row0; row0 += (int)((d.n + d.rows_per_cta - 1) / d.rows_per_cta);
     h.d = d;
-    const int k = (int)compact.size();
     compact.push_back(d);
+    const int pi = d.prec == QDKP_C64 ? 1 : 0;
+    const int k = kp[pi]++;
     e->order.push_back(i);
     const qdkp_operator* op = h.op;
-    const int S = apply_tile_sites(d.m);
-    S_max = std::max(S_max, S);
     m_max = std::max(m_max, d.m);
-    const int tiles = (int)((op->n_sites + S - 1) / S);
-    const double sign = (op->flags & QDKP_NEGATE) ? -1.0 : 1.0;
+    const int tiles = apply_tiles(op->n_sites, d.m);
     for (int t = 0; t < 4; ++t) {
       HXSlot x{};
-      x.F = op->fields64; x.N = op->n_sites;
-      x.nx = op->nx; x.ny = op->ny; x.nz = op->nz; x.flags = op->flags;
-      x.S = S; x.tile0 = tile0; x.h = op->h; x.sign = sign;
+      x.rec = pi ? (const void*)op->rec32 : (const void*)op->rec64;
+      x.msk = op->nbmask; x.N = (int)op->n_sites;
+      x.sx = op->ny * op->nz; x.sy = op->nz;
+      x.nzp = op->nzp; x.NP = op->nx * op->ny * op->nzp;
+      x.tile0 = tile0[pi]; x.cb = apply_cb_weight(op);
       x.sigma = h.prm.sigma;
       x.shifted = h.prm.folded ? 1 : 0;
       const bool recompute = t < 2;
@@ -572,13 +666,14 @@ int rebuild(qdkp_engine* e, cudaStream_t st) {
         x.Y = recompute ? (void*)d.AX : (void*)d.ARa;
         x.skip = (t == 1 || t == 3) ? e->d_one : skipflag;
       }
-      hx[(size_t)t * e->max_slots + k] = x;
+      hx[((size_t)pi * 4 + t) * e->max_slots + k] = x;
     }
-    tile0 += tiles;
+    tile0[pi] += tiles;
   }
   e->ns = (int)compact.size();
-  e->norm_ctas = norm0; e->gram_ctas = gram0; e->row_ctas = row0; e->hx_tiles = tile0;
-  e->S_max = S_max; e->m_max = m_max;
+  e->norm_ctas = norm0; e->gram_ctas = gram0; e->row_ctas = row0;
+  for (int pi = 0; pi < 2; ++pi) { e->hx_ns[pi] = kp[pi]; e->hx_tiles[pi] = tile0[pi]; }
+  e->m_max = m_max;
   e->widths.clear();
   for (const ESlot& d : compact)
     if (std::find(e->widths.begin(), e->widths.end(), d.m) == e->widths.end()) e->widths.push_back(d.m);
@@ -603,7 +698,7 @@ int launch_gram_multi(qdkp_engine* e, int which, cudaStream_t st) {
     if (which == GR_BA) { P = 3 * m; Q = 2 * m; }
     else if (which == GR_BB) { P = 2 * m; Q = m; }
     else if (which == GR_WW || which == GR_WAW) { P = 3 * m; Q = 3 * m; }
-    const size_t smem = (size_t)((2 * P + 7) / 8 * 8) * ((2 * Q + 7) / 8 * 8) * sizeof(double);
+    const size_t smem = gram_smem_bytes(P, Q, (int)sizeof(double2));
     int MR, MC, threads;
     gram_shape(P, Q, MR, MC, threads);
     if (MR == 3 && MC == 3) e_gram_kernel<3, 3><<<e->gram_ctas, threads, smem, st>>>(e->d_slots, e->ns, which, m);
@@ -622,12 +717,21 @@ int launch_gram_multi(qdkp_engine* e, int which, cudaStream_t st) {
 }
 
 int launch_update_multi(qdkp_engine* e, int which, cudaStream_t st) {
-  const int P = 2 * e->m_max;
-  const int KPp = (2 * P + 3) / 4 * 4, NQ = (2 * e->m_max + 7) / 8 * 8;
-  const size_t smem = ((size_t)KPp * NQ + (size_t)4 * NQ) * sizeof(double);
+  const size_t smem = update_smem_bytes(2 * e->m_max, e->m_max, (int)sizeof(double2));
   e_update_kernel<<<e->row_ctas, kUpdThreads, smem, st>>>(e->d_slots, e->ns, which);
   count_launch();
   QDKP_CUDA_TRY(cudaGetLastError());
+  return QDKP_OK;
+}
+
+// one H.X phase of a tick: a multi-slot launch per precision present
+int launch_hx_phase(qdkp_engine* e, int phase, cudaStream_t st) {
+  for (int pi = 0; pi < 2; ++pi) {
+    if (!e->hx_ns[pi]) continue;
+    int rc = launch_apply_multi(e->d_hx + ((size_t)pi * 4 + phase) * e->max_slots, e->hx_ns[pi],
+                                e->hx_tiles[pi], pi ? QDKP_C64 : QDKP_C128, st);
+    if (rc) return rc;
+  }
   return QDKP_OK;
 }
 
@@ -644,8 +748,8 @@ int tick(qdkp_engine* e, cudaStream_t st) {
   e_row_kernel<<<e->row_ctas, kTallThreads, 0, st>>>(e->d_slots, ns, RW_RESID);
   count_launch(4);
   QDKP_CUDA_TRY(cudaGetLastError());
-  ETRY(launch_apply_multi(e->d_hx + 0 * e->max_slots, ns, e->hx_tiles, e->S_max, QDKP_C128, st));
-  ETRY(launch_apply_multi(e->d_hx + 1 * e->max_slots, ns, e->hx_tiles, e->S_max, QDKP_C128, st));
+  ETRY(launch_hx_phase(e, 0, st));
+  ETRY(launch_hx_phase(e, 1, st));
   e_row_kernel<<<e->row_ctas, kTallThreads, 0, st>>>(e->d_slots, ns, RW_GATHERP);
   count_launch();
   ETRY(launch_gram_multi(e, GR_XR, st));
@@ -654,8 +758,8 @@ int tick(qdkp_engine* e, cudaStream_t st) {
   e_rchol_kernel<<<ns, kSmallThreads, small_smem, st>>>(e->d_slots);
   count_launch();
   ETRY(launch_update_multi(e, UP_RNORM, st));
-  ETRY(launch_apply_multi(e->d_hx + 2 * e->max_slots, ns, e->hx_tiles, e->S_max, QDKP_C128, st));
-  ETRY(launch_apply_multi(e->d_hx + 3 * e->max_slots, ns, e->hx_tiles, e->S_max, QDKP_C128, st));
+  ETRY(launch_hx_phase(e, 2, st));
+  ETRY(launch_hx_phase(e, 3, st));
   ETRY(launch_gram_multi(e, GR_PP, st));
   e_pchol_kernel<<<ns, kSmallThreads, small_smem, st>>>(e->d_slots);
   count_launch();
@@ -679,6 +783,45 @@ int tick(qdkp_engine* e, cudaStream_t st) {
 }  // namespace
 }  // namespace qdkp
 
+namespace qdkp {
+
+static void drop_graph(qdkp_engine* e) {
+  if (e->graph) cudaGraphExecDestroy(e->graph);
+  e->graph = nullptr;
+  e->graph_ticks = 0;
+}
+
+// Capture `ticks` ticks of the current layout into e->graph (on the engine's stream).
+static int capture_ticks(qdkp_engine* e, int ticks) {
+  drop_graph(e);
+  QDKP_CUDA_TRY(cudaStreamBeginCapture(e->gstream, cudaStreamCaptureModeThreadLocal));
+  int rc = QDKP_OK;
+  const long long l0 = launches_so_far();
+  for (int t = 0; t < ticks && rc == QDKP_OK; ++t) rc = tick(e, e->gstream);
+  // captured launches are not executions: take them back off the counter
+  const long long captured = launches_so_far() - l0;
+  count_launch((int)-captured);
+  e->launches_per_tick = ticks ? captured / ticks : 0;
+  cudaGraph_t g = nullptr;
+  const cudaError_t ce = cudaStreamEndCapture(e->gstream, &g);
+  if (rc != QDKP_OK) { if (g) cudaGraphDestroy(g); return rc; }
+  if (ce != cudaSuccess) {
+    set_error(std::string("engine graph capture: ") + cudaGetErrorString(ce));
+    return QDKP_ERR_CUDA;
+  }
+  const cudaError_t ie = cudaGraphInstantiate(&e->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (ie != cudaSuccess) {
+    e->graph = nullptr;
+    set_error(std::string("engine graph instantiate: ") + cudaGetErrorString(ie));
+    return QDKP_ERR_CUDA;
+  }
+  e->graph_ticks = ticks;
+  return QDKP_OK;
+}
+
+}  // namespace qdkp
+
 using namespace qdkp;
 
 extern "C" {
@@ -691,12 +834,18 @@ int qdkp_engine_create(int max_slots, int device, qdkp_engine** out) {
   e->max_slots = max_slots;
   e->slots.resize(max_slots);
   cudaError_t err = cudaMalloc(&e->d_slots, sizeof(ESlot) * max_slots);
-  if (err == cudaSuccess) err = cudaMalloc(&e->d_hx, sizeof(HXSlot) * 4 * max_slots);
+  if (err == cudaSuccess) err = cudaMalloc(&e->d_hx, sizeof(HXSlot) * 8 * max_slots);
   if (err == cudaSuccess) err = cudaMalloc(&e->d_one, sizeof(int));
   if (err == cudaSuccess) { const int one = 1; err = cudaMemcpy(e->d_one, &one, sizeof(int), cudaMemcpyHostToDevice); }
+  if (err == cudaSuccess) err = cudaStreamCreateWithFlags(&e->gstream, cudaStreamNonBlocking);
+  if (err == cudaSuccess) err = cudaEventCreateWithFlags(&e->ev_in, cudaEventDisableTiming);
+  if (err == cudaSuccess) err = cudaEventCreateWithFlags(&e->ev_out, cudaEventDisableTiming);
   if (err != cudaSuccess) {
     set_error(std::string("engine tables: ") + cudaGetErrorString(err));
     cudaFree(e->d_slots); cudaFree(e->d_hx); cudaFree(e->d_one);
+    if (e->gstream) cudaStreamDestroy(e->gstream);
+    if (e->ev_in) cudaEventDestroy(e->ev_in);
+    if (e->ev_out) cudaEventDestroy(e->ev_out);
     delete e;
     return QDKP_ERR_CUDA;
   }
@@ -716,6 +865,10 @@ int qdkp_engine_create(int max_slots, int device, qdkp_engine** out) {
 int qdkp_engine_destroy(qdkp_engine* e) {
   if (!e) return QDKP_OK;
   cudaSetDevice(e->device);
+  drop_graph(e);
+  if (e->gstream) { cudaStreamSynchronize(e->gstream); cudaStreamDestroy(e->gstream); }
+  if (e->ev_in) cudaEventDestroy(e->ev_in);
+  if (e->ev_out) cudaEventDestroy(e->ev_out);
   cudaFree(e->d_slots);
   cudaFree(e->d_hx);
   cudaFree(e->d_one);
@@ -725,7 +878,8 @@ int qdkp_engine_destroy(qdkp_engine* e) {
 
 size_t qdkp_engine_slot_workspace_size(const qdkp_operator* op, const qdkp_lobpcg_params* prm) {
   if (!op || !prm || prm->block < 1 || prm->block > kMaxBlock) return 0;
-  return slot_layout((int64_t)op->n_bands * op->n_sites, prm->block).total;
+  if (prm->precision != QDKP_C128 && prm->precision != QDKP_C64) return 0;
+  return slot_layout((int64_t)op->n_bands * op->n_sites, prm->block, prm->precision).total;
 }
 
 int qdkp_engine_admit(qdkp_engine* e, const qdkp_operator* op, const qdkp_lobpcg_params* prm,
@@ -733,13 +887,14 @@ int qdkp_engine_admit(qdkp_engine* e, const qdkp_operator* op, const qdkp_lobpcg
   QDKP_CHECK_ARG(e && op && prm && X0 && ws && slot_out, "NULL argument");
   QDKP_CHECK_ARG(op->n_bands == 8, "the batched engine serves eight-band operators");
   QDKP_CHECK_ARG(prm->block >= 1 && prm->block <= kMaxBlock, "block must be in [1, 24]");
-  QDKP_CHECK_ARG(prm->precision == QDKP_C128, "the engine computes in complex128");
+  QDKP_CHECK_ARG(prm->precision == QDKP_C128 || prm->precision == QDKP_C64,
+                 "precision must be QDKP_C128 or QDKP_C64");
   QDKP_CHECK_ARG(op->device == e->device, "operator lives on another device");
   const int64_t n = (int64_t)op->n_bands * op->n_sites;
   const int m = prm->block;
   QDKP_CHECK_ARG(n >= 5 * m, "problem too small for LOBPCG");
   QDKP_CHECK_ARG(n * m < (int64_t(1) << 31), "n * block must stay below 2^31 elements");
-  const SlotLayout L = slot_layout(n, m);
+  const SlotLayout L = slot_layout(n, m, prm->precision);
   if (ws_bytes < L.total) { set_error("engine slot workspace too small"); return QDKP_ERR_WORKSPACE; }
   int id = -1;
   for (int i = 0; i < e->max_slots; ++i) if (!e->slots[i].used) { id = i; break; }
@@ -768,6 +923,9 @@ int qdkp_engine_admit(qdkp_engine* e, const qdkp_operator* op, const qdkp_lobpcg
   d.gpart = (double*)take(L.gpart);
   h.gpart_doubles = L.gpart / sizeof(double);
   d.n = n; d.m = m; d.folded = prm->folded;
+  d.prec = prm->precision;
+  d.sqrt_eps = d.prec == QDKP_C64 ? std::sqrt((double)std::numeric_limits<float>::epsilon())
+                                  : std::sqrt(std::numeric_limits<double>::epsilon());
   d.tol = prm->tol > 0 ? prm->tol : std::sqrt(std::numeric_limits<double>::epsilon()) * (double)n;
   d.maxiter = prm->maxiter;
   d.restart_control = prm->restart_control > 0 ? prm->restart_control : 20;
@@ -776,27 +934,25 @@ int qdkp_engine_admit(qdkp_engine* e, const qdkp_operator* op, const qdkp_lobpcg
   int rc;
 #define ATRY(x) do { rc = (x); if (rc != QDKP_OK) return rc; } while (0)
   // X = orthonormalise(X0) (lobpcg.py:620-630)
-  ATRY(launch_copy((const double2*)X0, m, m, n, d.X, m, st));
+  if (d.prec == QDKP_C64)
+    ATRY((launch_copy<double, float>(static_cast<const double2*>(X0), m, m, n,
+                                     reinterpret_cast<float2*>(d.X), m, st)));
+  else
+    ATRY(launch_copy(static_cast<const double2*>(X0), m, m, n, d.X, m, st));
   ATRY(gram1(h, d.X, d.X, m, d.G, st));
   ATRY(launch_chol_inv(d.G, m, d.U, (int*)d.w, st));
   int stat = 0;
   ATRY(read_sync(&stat, d.w, sizeof(int), st));
   if (stat) { set_error("Linearly dependent initial approximations"); return QDKP_ERR_NUMERIC; }
-  {
-    const double2* C[1] = {d.U};
-    ATRY(launch_update(one(d.X, m), C, m, n, d.X, m, 0, st));
-  }
+  ATRY(update1(h, d.X, m, d.U, m, d.X, st));
   // initial Ritz vectors (lobpcg.py:633-660)
   ATRY(apply_folded(h, d.X, m, d.AX, st));
   ATRY(gram1(h, d.X, d.AX, m, d.gT, st));
   ATRY(launch_eigh(d.gT, nullptr, m, d.w, d.E, d.scr, (int*)d.G, st));
   ATRY(read_sync(&stat, d.G, sizeof(int), st));
   if (stat) { set_error("initial Rayleigh-Ritz failed"); return QDKP_ERR_NUMERIC; }
-  {
-    const double2* C[1] = {d.E};
-    ATRY(launch_update(one(d.X, m), C, m, n, d.X, m, 0, st));
-    ATRY(launch_update(one(d.AX, m), C, m, n, d.AX, m, 0, st));
-  }
+  ATRY(update1(h, d.X, m, d.E, m, d.X, st));
+  ATRY(update1(h, d.AX, m, d.E, m, d.AX, st));
   std::vector<double> w(m);
   ATRY(read_sync(w.data(), d.w, m * sizeof(double), st));
   EState s0{};
@@ -821,11 +977,38 @@ int qdkp_engine_step(qdkp_engine* e, int ticks, void* stream) {
   QDKP_CHECK_ARG(e && ticks >= 0, "bad arguments");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   QDKP_CUDA_TRY(cudaSetDevice(e->device));
-  if (e->dirty) { int rc = rebuild(e, st); if (rc) return rc; }
-  for (int t = 0; t < ticks; ++t) {
-    int rc = tick(e, st);
+  if (e->dirty) {
+    drop_graph(e);
+    int rc = rebuild(e, st);
     if (rc) return rc;
   }
+  if (ticks == 0 || e->ns == 0) return QDKP_OK;
+  if (!e->use_graph) {
+    for (int t = 0; t < ticks; ++t) {
+      int rc = tick(e, st);
+      if (rc) return rc;
+    }
+    return QDKP_OK;
+  }
+  // the tick sequence is fixed for a slot layout: replay it as one graph launch
+  if (!e->graph || e->graph_ticks != ticks) {
+    QDKP_CUDA_TRY(cudaStreamSynchronize(st));   // descriptor uploads of rebuild() landed
+    int rc = capture_ticks(e, ticks);
+    if (rc) return rc;
+  }
+  QDKP_CUDA_TRY(cudaEventRecord(e->ev_in, st));
+  QDKP_CUDA_TRY(cudaStreamWaitEvent(e->gstream, e->ev_in, 0));
+  QDKP_CUDA_TRY(cudaGraphLaunch(e->graph, e->gstream));
+  count_launch(e->launches_per_tick * ticks);
+  QDKP_CUDA_TRY(cudaEventRecord(e->ev_out, e->gstream));
+  QDKP_CUDA_TRY(cudaStreamWaitEvent(st, e->ev_out, 0));
+  return QDKP_OK;
+}
+
+int qdkp_engine_set_graphs(qdkp_engine* e, int enable) {
+  QDKP_CHECK_ARG(e != nullptr, "NULL engine");
+  e->use_graph = enable != 0;
+  if (!e->use_graph) drop_graph(e);
   return QDKP_OK;
 }
 
@@ -865,14 +1048,14 @@ int qdkp_engine_retire(qdkp_engine* e, int slot, double* lambda_out, void* V,
   // residuals of the last iterate; it becomes the best one if it improved (lobpcg.py:975-995)
   double* dl = d.w;
   QDKP_CUDA_TRY(cudaMemcpyAsync(dl, lam.data(), m * sizeof(double), cudaMemcpyHostToDevice, st));
-  RTRY(launch_colnorm2(d.AX, m, d.X, m, dl, m, n, d.npart, d.nparts, d.gpart, st));
+  RTRY(colnorm1(h, d.AX, d.X, dl, m, d.gpart, st));
   RTRY(read_sync(rn2.data(), d.gpart, m * sizeof(double), st));
   double mean = 0.0;
   for (int j = 0; j < m; ++j) mean += std::sqrt(std::fabs(rn2[j]));
   mean /= m;
   int best_iter = s.best_iter;
   if (s.status != QDKP_LOBPCG_NONFINITE && mean < s.smallest) {
-    RTRY(launch_copy(d.X, m, m, n, d.best, m, st));
+    RTRY(copy1(h, d.X, m, d.best, st));
     best_iter = s.iter + 1;
   }
   // final Rayleigh-Ritz on the best iterate (lobpcg.py:1009-1060)
@@ -898,12 +1081,15 @@ int qdkp_engine_retire(qdkp_engine* e, int slot, double* lambda_out, void* V,
   RTRY(read_sync(&stat, d.G, sizeof(int), st));
   if (stat) { set_error("eigh has failed in lobpcg postprocessing"); return QDKP_ERR_NUMERIC; }
   RTRY(read_sync(lam.data(), d.w, m * sizeof(double), st));
-  {
-    const double2* C[1] = {d.E};
-    RTRY(launch_update(one(d.best, m), C, m, n, (double2*)V, m, 0, st));
-    RTRY(launch_update(one(d.AX, m), C, m, n, d.AX, m, 0, st));
-  }
-  RTRY(launch_colnorm2(d.AX, m, (const double2*)V, m, d.w, m, n, d.npart, d.nparts, d.gpart, st));
+  // Ritz vectors of the best iterate; a complex64 slot forms them in its own precision (in the
+  // free folded scratch T) and widens them into the caller's complex128 V
+  void* Vs = d.prec == QDKP_C64 ? static_cast<void*>(d.T) : V;
+  RTRY(update1(h, d.best, m, d.E, m, Vs, st));
+  RTRY(update1(h, d.AX, m, d.E, m, d.AX, st));
+  RTRY(colnorm1(h, d.AX, Vs, d.w, m, d.gpart, st));
+  if (d.prec == QDKP_C64)
+    RTRY((launch_copy<float, double>(reinterpret_cast<const float2*>(d.T), m, m, n,
+                                     static_cast<double2*>(V), m, st)));
   RTRY(read_sync(rn2.data(), d.gpart, m * sizeof(double), st));
   bool all = true;
   for (int j = 0; j < m; ++j) {

@@ -29,9 +29,14 @@ struct EState {
 };
 
 // Per-slot constant descriptor (built on the host at admission, device resident).
+// The tall blocks (X ... T) hold complex128 or, for a complex64 slot (prec = QDKP_C64), complex64
+// values; they are declared double2 and reinterpreted through blk<T>(). Everything small (Gram
+// matrices, Ritz coefficients, residual norms) is FP64 in both cases.
 struct ESlot {
   long long n;          // rows (8 N)
   int m;                // block width
+  int prec;             // QDKP_C128 or QDKP_C64: arithmetic of the tall blocks and of H.X
+  double sqrt_eps;      // sqrt(machine epsilon) of that arithmetic (explicit Gram switch)
   int folded;
   double tol;
   int maxiter;
@@ -48,6 +53,9 @@ struct ESlot {
   int rows_per_cta;     // rows per CTA in the row kernels (gather, update)
   EState* st;
 };
+
+template <typename T>
+__device__ __forceinline__ cplx<T>* blk(double2* p) { return reinterpret_cast<cplx<T>*>(p); }
 
 __device__ __forceinline__ int slot_of(const ESlot* __restrict__ S, int ns, int b,
                                        int ESlot::*first) {

@@ -12,417 +12,1017 @@
 // The block layout of those pieces is Pryor's table (kp_pryor.py:244-301) with the lower
 // triangle the adjoint of the upper (kp_pryor.py:216-241).
 //
-// Work split: a CTA owns S consecutive sites. Phase 1 builds one coefficient record per site
-// into shared memory (face-averaged stencil weights, first-order face weights, the local
-// block), reading the 15 raw fields of the site and its six face neighbours. Phase 2 gives each
-// thread (site, column) items: it loads the eight band components of the site, its six faces
-// and twelve edges for that column, and accumulates all eight output bands in registers.
+// Two kernels:
+//   kp_record_kernel  once per operator (and per band-edge update): folds the 15 raw per-site
+//                     fields into a per-site record of stencil weights (local block, the three
+//                     "+" faces, the twelve edge weights) and a neighbour mask. The record is
+//                     kept in FP64 and FP32; the sign of the hole convention / negation is
+//                     folded in, so the apply kernel never branches on it.
+//   kp_apply_kernel   one thread per (site, column): loads the eight band components of the
+//                     site, its six faces and twelve edges (valence bands only) for that
+//                     column, and accumulates all eight output bands in registers. A "-" face
+//                     reads its weights from the neighbour's "+" face (the face weights are
+//                     symmetric; the first-order ones change sign). The edge terms of a plane
+//                     are summed with their scalar weights first and the constant band-mixing
+//                     matrix of that plane is applied once.
 #include <algorithm>
+#include <type_traits>
 
 #include "qdkp_common.cuh"
 
 namespace qdkp {
 
-enum RecSlot {
-  R_A = 0, R_P, R_Q, R_RRE, R_RIM, R_SRE, R_SIM, R_DL,
-  R_T1 = 8,     // -G t1 per face (x+, x-, y+, y-, z+, z-): P kinetic
-  R_T2 = 14,    // -G t2 per face: Q and R kinetic
-  R_G3 = 20,    // gamma3 at the face neighbour (cross terms)
-  R_SU = 26,    // (cu_p + cu_q) / 4h, signed by the face direction: U
-  R_SVR = 32,   // (cv_p + cv_q) / 4h, signed, real part: V
-  R_SVI = 38,   // imaginary part
-  R_COUNT = 44
+// Record layout: entry k of site (ix, iy, iz) at rec[k * NP + (ix * ny + iy) * nzp + iz], with z
+// padded to nzp = a multiple of 4 (zeros in the padding) so that a z-run of a tile row starts on
+// a 16-byte boundary for the staged kernel's copies; NP = nx ny nzp.
+enum RecEntry {
+  K_A = 0,      // sign (Ec + 6 G / h^2): conduction diagonal
+  K_A2,         // sign (-P + Q): LH/HH diagonals of rows 2, 5
+  K_A3,         // sign (-P - Q): rows 3, 4
+  K_A6,         // sign (-P - Delta): split-off rows 6, 7
+  K_Q2,         // sign sqrt2 Q
+  K_RRE, K_RIM, K_SRE, K_SIM,
+  K_FACE = 9,   // per face f (x+, x-, y+, y-, z+, z-): K_FACE + 5f + {0 kp, 1 k2, 2 su, 3 svr, 4 svi}
+  K_EDGE = 39,  // per plane pl (xy, zx, zy) and edge e: K_EDGE + 4 pl + e
+  K_COUNT = 51
 };
 
-template <typename T>
-struct ApplyArgs {
-  const T* __restrict__ F;   // F_COUNT * N
-  const cplx<T>* __restrict__ X;
-  cplx<T>* __restrict__ Y;
-  long long N, ldx, ldy;
-  int nx, ny, nz, m, flags, S;
-  T h, sigma, sign;          // sign = -1 for the hole convention
-  int shifted;
-};
-
-template <typename T>
-__device__ __forceinline__ void first_order_coefs(const T* __restrict__ F, long long N,
-                                                  long long q, bool inter, T cu[3],
-                                                  cplx<T> cv[3]) {
-  const T r3 = T(0.57735026918962576451), r6 = T(0.40824829046386301637);
-  const T P0 = F[F_P0 * N + q];
+// ---------------------------------------------------------------------------------------------
+// Record construction (FP64, once per operator)
+// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ void first_order_coefs(const double* __restrict__ F, long long N,
+                                                  long long q, bool inter, double cu[3],
+                                                  double2 cv[3]) {
+  const double r3 = 0.57735026918962576451, r6 = 0.40824829046386301637;
+  const double P0 = F[F_P0 * N + q];
   if (inter) {
-    const T exx = F[F_EXX * N + q], eyy = F[F_EYY * N + q], ezz = F[F_EZZ * N + q];
-    const T exy = F[F_EXY * N + q], eyz = F[F_EYZ * N + q], ezx = F[F_EZX * N + q];
+    const double exx = F[F_EXX * N + q], eyy = F[F_EYY * N + q], ezz = F[F_EZZ * N + q];
+    const double exy = F[F_EXY * N + q], eyz = F[F_EYZ * N + q], ezx = F[F_EZX * N + q];
     cu[0] = -P0 * ezx * r3;
     cu[1] = -P0 * eyz * r3;
-    cu[2] = P0 * (T(1) - ezz) * r3;
-    cv[0] = mk<T>(P0 * (T(1) - exx) * r6, P0 * exy * r6);
-    cv[1] = mk<T>(-P0 * exy * r6, P0 * (eyy - T(1)) * r6);
-    cv[2] = mk<T>(-P0 * ezx * r6, P0 * eyz * r6);
+    cu[2] = P0 * (1.0 - ezz) * r3;
+    cv[0] = make_double2(P0 * (1.0 - exx) * r6, P0 * exy * r6);
+    cv[1] = make_double2(-P0 * exy * r6, P0 * (eyy - 1.0) * r6);
+    cv[2] = make_double2(-P0 * ezx * r6, P0 * eyz * r6);
   } else {
-    cu[0] = T(0); cu[1] = T(0); cu[2] = P0 * r3;
-    cv[0] = mk<T>(P0 * r6, T(0));
-    cv[1] = mk<T>(T(0), -P0 * r6);
-    cv[2] = czero<T>();
+    cu[0] = 0.0; cu[1] = 0.0; cu[2] = P0 * r3;
+    cv[0] = make_double2(P0 * r6, 0.0);
+    cv[1] = make_double2(0.0, -P0 * r6);
+    cv[2] = make_double2(0.0, 0.0);
   }
 }
 
-template <typename T, int NB>
-__device__ void build_record(const ApplyArgs<T>& a, long long s, T* rec, int S,
-                             unsigned* nbmask) {
-  const T* __restrict__ F = a.F;
-  const long long N = a.N;
-  const int iz = (int)(s % a.nz);
-  const long long t = s / a.nz;
-  const int iy = (int)(t % a.ny);
-  const int ix = (int)(t / a.ny);
-  const int coord[3] = {ix, iy, iz};
-  const int ext[3] = {a.nx, a.ny, a.nz};
-  const long long str[3] = {(long long)a.ny * a.nz, (long long)a.nz, 1LL};
-  const T G = T(kG);
-  const T ih2 = T(1) / (a.h * a.h);
-  const T i4h = T(1) / (T(4) * a.h);
-  const bool strain = (a.flags & QDKP_STRAIN) != 0;
-  const bool inter = NB == 8 && strain && (a.flags & QDKP_INTERBAND_STRAIN);
-
-  // neighbour mask: bit f (0..5) face x+, x-, y+, y-, z+, z-; bit 6 + 4 pl + e the in-plane
-  // edge e of plane pl (xy, zx, zy) with signs sa = e & 1 ? -1 : 1, sb = e & 2 ? -1 : 1
-  {
+__global__ void kp_record_kernel(const double* __restrict__ F, long long N, int nx, int ny,
+                                 int nz, int nzp, double h, int flags, int nb, double sign,
+                                 double* __restrict__ rec64, float* __restrict__ rec32,
+                                 unsigned* __restrict__ nbmask) {
+  const double G = kG;
+  const double ih2 = 1.0 / (h * h);
+  const double i4h = 1.0 / (4.0 * h);
+  const double i8h2 = 1.0 / (8.0 * h * h);
+  const double sq2 = 1.41421356237309504880, sq3 = 1.73205080756887729353;
+  const bool strain = (flags & QDKP_STRAIN) != 0;
+  const bool inter = nb == 8 && strain && (flags & QDKP_INTERBAND_STRAIN);
+  for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < N;
+       s += (long long)gridDim.x * blockDim.x) {
+    const int iz = (int)(s % nz);
+    const long long t = s / nz;
+    const int iy = (int)(t % ny);
+    const int ix = (int)(t / ny);
+    const int coord[3] = {ix, iy, iz};
+    const int ext[3] = {nx, ny, nz};
+    const long long str[3] = {(long long)ny * nz, (long long)nz, 1LL};
+    double r[K_COUNT];
+    // neighbour mask: bit f (0..5) face x+, x-, y+, y-, z+, z-; bit 6 + 4 pl + e the in-plane
+    // edge e of plane pl (xy, zx, zy) with signs sa = e & 1 ? -1 : 1, sb = e & 2 ? -1 : 1
     unsigned msk = 0;
     for (int ax = 0; ax < 3; ++ax) {
       if (coord[ax] + 1 < ext[ax]) msk |= 1u << (2 * ax);
       if (coord[ax] > 0) msk |= 1u << (2 * ax + 1);
     }
+    const double g1 = F[F_G1 * N + s], g2 = F[F_G2 * N + s];
+    double cu_p[3]; double2 cv_p[3];
+    if (nb == 8) first_order_coefs(F, N, s, inter, cu_p, cv_p);
+    double dk1 = 0.0, dk2[3];
+    for (int ax = 0; ax < 3; ++ax) {
+      double d1 = 0.0, d2 = 0.0;
+      for (int dir = 0; dir < 2; ++dir) {
+        const bool in = dir == 0 ? (coord[ax] + 1 < ext[ax]) : (coord[ax] > 0);
+        double kp = 0.0, k2 = 0.0, su = 0.0, svr = 0.0, svi = 0.0;
+        if (in) {
+          const long long q = dir == 0 ? s + str[ax] : s - str[ax];
+          const double t1 = (g1 + F[F_G1 * N + q]) * 0.5 * ih2;
+          const double t2 = (g2 + F[F_G2 * N + q]) * 0.5 * ih2;
+          d1 += t1; d2 += t2;
+          kp = -G * t1; k2 = -G * t2;
+          if (nb == 8) {
+            // symmetrised first derivative: (cu_p + cu_q) / 4h, signed by the face direction
+            double cu_q[3]; double2 cv_q[3];
+            first_order_coefs(F, N, q, inter, cu_q, cv_q);
+            const double sg = dir == 0 ? i4h : -i4h;
+            su = (cu_p[ax] + cu_q[ax]) * sg;
+            svr = (cv_p[ax].x + cv_q[ax].x) * sg;
+            svi = (cv_p[ax].y + cv_q[ax].y) * sg;
+          }
+        } else {  // hard wall: ghost term alpha_p / h^2 (kp_confined.py:133-137)
+          d1 += g1 * ih2; d2 += g2 * ih2;
+        }
+        const int kf = K_FACE + 5 * (2 * ax + dir);
+        r[kf + 0] = sign * kp;
+        r[kf + 1] = sign * k2;
+        r[kf + 2] = sign * su;
+        r[kf + 3] = sign * svr;
+        r[kf + 4] = sign * svi;
+      }
+      dk1 += d1; dk2[ax] = d2;
+    }
+    double Q = G * (dk2[0] + dk2[1] - 2.0 * dk2[2]);
+    double Rre = -sq3 * G * (dk2[0] - dk2[1]), Rim = 0.0, Sre = 0.0, Sim = 0.0;
+    if (strain) {
+      const double b = F[F_B * N + s], d = F[F_D * N + s];
+      const double exx = F[F_EXX * N + s], eyy = F[F_EYY * N + s], ezz = F[F_EZZ * N + s];
+      const double exy = F[F_EXY * N + s], eyz = F[F_EYZ * N + s], ezx = F[F_EZX * N + s];
+      Q += -(b / 2.0) * (exx + eyy - 2.0 * ezz);
+      Rre += (sq3 / 2.0) * b * (exx - eyy);
+      Rim += -d * exy;
+      Sre = -d * ezx;
+      Sim = d * eyz;
+    }
+    const double A = F[F_EC * N + s] + 6.0 * G * ih2;
+    const double P = -F[F_EV * N + s] + G * dk1;
+    const double Dl = F[F_DSO * N + s];
+    r[K_A] = sign * A;
+    r[K_A2] = sign * (-P + Q);
+    r[K_A3] = sign * (-P - Q);
+    r[K_A6] = sign * (-P - Dl);
+    r[K_Q2] = sign * sq2 * Q;
+    r[K_RRE] = sign * Rre; r[K_RIM] = sign * Rim;
+    r[K_SRE] = sign * Sre; r[K_SIM] = sign * Sim;
+    // cross(g3, a, b): coefficient of x(p + sa e_a + sb e_b) in the R / S slots is
+    // 2 sqrt3 G * (-(sa sb) / (8 h^2)) (g3(p + sa e_a) + g3(p + sb e_b))
     for (int pl = 0; pl < 3; ++pl) {
       const int ea = pl == 0 ? 0 : 2, eb = pl == 0 ? 1 : (pl == 1 ? 0 : 1);
       for (int e = 0; e < 4; ++e) {
-        const int ca = coord[ea] + ((e & 1) ? -1 : 1), cb = coord[eb] + ((e & 2) ? -1 : 1);
-        if (ca >= 0 && ca < ext[ea] && cb >= 0 && cb < ext[eb]) msk |= 1u << (6 + 4 * pl + e);
-      }
-    }
-    *nbmask = msk;
-  }
-  const T g1 = F[F_G1 * N + s], g2 = F[F_G2 * N + s];
-  T cu_p[3]; cplx<T> cv_p[3];
-  if (NB == 8) first_order_coefs<T>(F, N, s, inter, cu_p, cv_p);
-  T dk1 = T(0), dk2[3];
-#pragma unroll
-  for (int ax = 0; ax < 3; ++ax) {
-    T d1 = T(0), d2 = T(0);
-#pragma unroll
-    for (int dir = 0; dir < 2; ++dir) {
-      const int f = 2 * ax + dir;
-      const bool in = dir == 0 ? (coord[ax] + 1 < ext[ax]) : (coord[ax] > 0);
-      T t1n = T(0), t2n = T(0), g3n = T(0), su = T(0), svr = T(0), svi = T(0);
-      if (in) {
-        const long long q = dir == 0 ? s + str[ax] : s - str[ax];
-        const T t1 = (g1 + F[F_G1 * N + q]) * T(0.5) * ih2;
-        const T t2 = (g2 + F[F_G2 * N + q]) * T(0.5) * ih2;
-        d1 += t1; d2 += t2;
-        t1n = -G * t1; t2n = -G * t2;
-        g3n = F[F_G3 * N + q];
-        if (NB == 8) {
-          T cu_q[3]; cplx<T> cv_q[3];
-          first_order_coefs<T>(F, N, q, inter, cu_q, cv_q);
-          const T sg = dir == 0 ? T(1) : T(-1);
-          su = sg * (cu_p[ax] + cu_q[ax]) * i4h;
-          svr = sg * (cv_p[ax].x + cv_q[ax].x) * i4h;
-          svi = sg * (cv_p[ax].y + cv_q[ax].y) * i4h;
+        const int sa = (e & 1) ? -1 : 1, sb = (e & 2) ? -1 : 1;
+        const int ca = coord[ea] + sa, cb = coord[eb] + sb;
+        double c = 0.0;
+        if (ca >= 0 && ca < ext[ea] && cb >= 0 && cb < ext[eb]) {
+          msk |= 1u << (6 + 4 * pl + e);
+          const double ga = F[F_G3 * N + s + sa * str[ea]];
+          const double gb = F[F_G3 * N + s + sb * str[eb]];
+          c = 2.0 * sq3 * G * (-(double)(sa * sb) * i8h2) * (ga + gb);
         }
-      } else {  // hard wall: ghost term alpha_p / h^2 (kp_confined.py:133-137)
-        d1 += g1 * ih2; d2 += g2 * ih2;
+        r[K_EDGE + 4 * pl + e] = sign * c;
       }
-      rec[(R_T1 + f) * S] = t1n;
-      rec[(R_T2 + f) * S] = t2n;
-      rec[(R_G3 + f) * S] = g3n;
-      rec[(R_SU + f) * S] = su;
-      rec[(R_SVR + f) * S] = svr;
-      rec[(R_SVI + f) * S] = svi;
     }
-    dk1 += d1; dk2[ax] = d2;
+    const long long NP = (long long)nx * ny * nzp;
+    const long long sp = t * nzp + iz;
+    for (int k = 0; k < K_COUNT; ++k) {
+      rec64[k * NP + sp] = r[k];
+      rec32[k * NP + sp] = (float)r[k];
+    }
+    nbmask[s] = msk;
   }
-  const T sq3 = T(1.73205080756887729353);
-  T Q = G * (dk2[0] + dk2[1] - T(2) * dk2[2]);
-  T Rre = -sq3 * G * (dk2[0] - dk2[1]), Rim = T(0), Sre = T(0), Sim = T(0);
-  if (strain) {
-    const T b = F[F_B * N + s], d = F[F_D * N + s];
-    const T exx = F[F_EXX * N + s], eyy = F[F_EYY * N + s], ezz = F[F_EZZ * N + s];
-    const T exy = F[F_EXY * N + s], eyz = F[F_EYZ * N + s], ezx = F[F_EZX * N + s];
-    Q += -(b / T(2)) * (exx + eyy - T(2) * ezz);
-    Rre += (sq3 / T(2)) * b * (exx - eyy);
-    Rim += -d * exy;
-    Sre = -d * ezx;
-    Sim = d * eyz;
-  }
-  rec[R_A * S] = F[F_EC * N + s] + T(6) * G * ih2;
-  rec[R_P * S] = -F[F_EV * N + s] + G * dk1;
-  rec[R_Q * S] = Q;
-  rec[R_RRE * S] = Rre;
-  rec[R_RIM * S] = Rim;
-  rec[R_SRE * S] = Sre;
-  rec[R_SIM * S] = Sim;
-  rec[R_DL * S] = F[F_DSO * N + s];
 }
 
+// ---------------------------------------------------------------------------------------------
+// The stencil arithmetic, shared by the kernels below. `L` supplies the neighbour values of one
+// column (centre, face f = x+, x-, y+, y-, z+, z-, edge (pl, e)); `Rc` the site's record
+// entries (own(k); face(ax, dir, k): entry k of face (ax, dir)).
+// ---------------------------------------------------------------------------------------------
 template <int NB> __device__ __forceinline__ constexpr bool has_band(int b) {
   return NB == 8 ? true : (NB == 6 ? b >= 2 : (b >= 2 && b <= 5));
 }
 template <int NB> __device__ __forceinline__ constexpr int band_off() { return NB == 8 ? 0 : 2; }
 
-// x[b] = X[band b, site s + offset, column j] with xs = &X[0, s, j], bstr = N ldx (elements);
-// every offset fits 32 bits for the grids this library accepts (n ldx < 2^31).
-template <typename T, int NB, bool VB_ONLY>
-__device__ __forceinline__ void load_site(const cplx<T>* __restrict__ xs, int bstr, int off,
-                                          cplx<T> (&x)[8]) {
-#pragma unroll
-  for (int b = 0; b < 8; ++b) {
-    if (!has_band<NB>(b) || (VB_ONLY && b < 2)) { x[b] = czero<T>(); continue; }
-    x[b] = __ldg(xs + ((b - band_off<NB>()) * bstr + off));
-  }
-}
-
-template <typename T> struct ApplyOcc;
-template <> struct ApplyOcc<double> { static constexpr int kMinBlocks = 2; };
-template <> struct ApplyOcc<float> { static constexpr int kMinBlocks = 2; };
-
-template <typename T, int NB>
-__device__ __forceinline__ void apply_tile(const ApplyArgs<T>& a, long long s0, T* rec) {
-  const int S = a.S;
-  const int ns = (int)min((long long)S, a.N - s0);
-
-  unsigned* nbm = reinterpret_cast<unsigned*>(rec + R_COUNT * S);
-  for (int i = threadIdx.x; i < ns; i += blockDim.x)
-    build_record<T, NB>(a, s0 + i, rec + i, S, nbm + i);
-  __syncthreads();
-
-  const T G = T(kG);
-  const T ih2 = T(1) / (a.h * a.h);
+template <typename T, int NB, class L, class Rc>
+__device__ __forceinline__ void hx_math(const L& ld, const Rc& rc, unsigned msk, T shift, T cb,
+                                        cplx<T> (&y)[8]) {
   const T sq2 = T(1.41421356237309504880), sq3 = T(1.73205080756887729353);
   const T sq32 = T(1.22474487139158904910), isq2 = T(0.70710678118654752440);
-  const T i8h2 = T(1) / (T(8) * a.h * a.h);
   const T wQ[3] = {T(1), T(1), T(-2)};
   const T wR[3] = {-sq3, sq3, T(0)};
-  const int m = a.m;
-  const int items = ns * m;
+  cplx<T> x[8];
 
-  const int bstr = (int)(a.N * a.ldx);
-  const int ystr = (int)(a.N * a.ldy);
-  const int sx = a.ny * a.nz, sy = a.nz;
-  for (int it = threadIdx.x; it < items; it += blockDim.x) {
-    const int i = it / m;
-    const int j = it - i * m;
-    const long long s = s0 + i;
-    const T* r = rec + i;
-    const unsigned msk = nbm[i];
-    const cplx<T>* __restrict__ xs = a.X + (s * a.ldx + j);
-    const int str[3] = {sx * (int)a.ldx, sy * (int)a.ldx, (int)a.ldx};
-    cplx<T> y[8], x[8];
-
-    // ---- local block ------------------------------------------------------------------
-    // y = sign (H x) - sigma x is accumulated as sign (H x - sign sigma x): start from the
-    // shift term so the centre values need not stay live until the end.
-    load_site<T, NB, false>(xs, bstr, 0, x);
-    {
-      const T sh = a.shifted ? -a.sigma * a.sign : T(0);
+  // ---- local block (with the shift -sigma) -------------------------------------------
+  ld.centre(x);
 #pragma unroll
-      for (int b = 0; b < 8; ++b) y[b] = cscale(sh, x[b]);
+  for (int b = 0; b < 8; ++b) y[b] = cscale(shift, x[b]);
+  {
+    const T a2 = rc.own(K_A2), a3 = rc.own(K_A3), a6 = rc.own(K_A6), q2 = rc.own(K_Q2);
+    const cplx<T> Rr = mk<T>(rc.own(K_RRE), rc.own(K_RIM));
+    const cplx<T> Sx = mk<T>(rc.own(K_SRE), rc.own(K_SIM));
+    if (NB == 8) {
+      const T A = rc.own(K_A);
+      caxpy(y[0], A, x[0]); caxpy(y[1], A, x[1]);
     }
-    {
-      const T A = r[R_A * S], P = r[R_P * S], Q = r[R_Q * S], Dl = r[R_DL * S];
-      const cplx<T> R = mk<T>(r[R_RRE * S], r[R_RIM * S]);
-      const cplx<T> Sx = mk<T>(r[R_SRE * S], r[R_SIM * S]);
-      if (NB == 8) { caxpy(y[0], A, x[0]); caxpy(y[1], A, x[1]); }
-      caxpy(y[2], -P + Q, x[2]); cfmac(y[2], Sx, cscale(T(-1), x[3])); cfma(y[2], R, x[4]);
-      cfma(y[2], Sx, cscale(sq32, x[6])); caxpy(y[2], -sq2 * Q, x[7]);
-      cfma(y[3], Sx, cscale(T(-1), x[2])); caxpy(y[3], -P - Q, x[3]); cfma(y[3], R, x[5]);
-      cfma(y[3], R, cscale(-sq2, x[6])); cfma(y[3], Sx, cscale(isq2, x[7]));
-      cfmac(y[4], R, x[2]); caxpy(y[4], -P - Q, x[4]); cfmac(y[4], Sx, x[5]);
-      cfmac(y[4], Sx, cscale(isq2, x[6])); cfmac(y[4], R, cscale(sq2, x[7]));
-      cfmac(y[5], R, x[3]); cfma(y[5], Sx, x[4]); caxpy(y[5], -P + Q, x[5]);
-      caxpy(y[5], sq2 * Q, x[6]); cfmac(y[5], Sx, cscale(sq32, x[7]));
-      cfmac(y[6], Sx, cscale(sq32, x[2])); cfmac(y[6], R, cscale(-sq2, x[3]));
-      cfma(y[6], Sx, cscale(isq2, x[4])); caxpy(y[6], sq2 * Q, x[5]); caxpy(y[6], -P - Dl, x[6]);
-      caxpy(y[7], -sq2 * Q, x[2]); cfmac(y[7], Sx, cscale(isq2, x[3])); cfma(y[7], R, cscale(sq2, x[4]));
-      cfma(y[7], Sx, cscale(sq32, x[5])); caxpy(y[7], -P - Dl, x[7]);
-    }
+    const cplx<T> R2 = cscale(sq2, Rr), S32 = cscale(sq32, Sx), Si2 = cscale(isq2, Sx);
+    caxpy(y[2], a2, x[2]); cfmac(y[2], Sx, cscale(T(-1), x[3])); cfma(y[2], Rr, x[4]);
+    cfma(y[2], S32, x[6]); caxpy(y[2], -q2, x[7]);
+    cfma(y[3], Sx, cscale(T(-1), x[2])); caxpy(y[3], a3, x[3]); cfma(y[3], Rr, x[5]);
+    cfma(y[3], R2, cscale(T(-1), x[6])); cfma(y[3], Si2, x[7]);
+    cfmac(y[4], Rr, x[2]); caxpy(y[4], a3, x[4]); cfmac(y[4], Sx, x[5]);
+    cfmac(y[4], Si2, x[6]); cfmac(y[4], R2, x[7]);
+    cfmac(y[5], Rr, x[3]); cfma(y[5], Sx, x[4]); caxpy(y[5], a2, x[5]);
+    caxpy(y[5], q2, x[6]); cfmac(y[5], S32, x[7]);
+    cfmac(y[6], S32, x[2]); cfmac(y[6], R2, cscale(T(-1), x[3]));
+    cfma(y[6], Si2, x[4]); caxpy(y[6], q2, x[5]); caxpy(y[6], a6, x[6]);
+    caxpy(y[7], -q2, x[2]); cfmac(y[7], Si2, x[3]); cfma(y[7], R2, x[4]);
+    cfma(y[7], S32, x[5]); caxpy(y[7], a6, x[7]);
+  }
 
-    // ---- six face neighbours ------------------------------------------------------------
+  // ---- six face neighbours ------------------------------------------------------------
 #pragma unroll
-    for (int f = 0; f < 6; ++f) {
-      const int ax = f >> 1, dir = f & 1;
-      if (!(msk & (1u << f))) continue;
-      load_site<T, NB, false>(xs, bstr, dir == 0 ? str[ax] : -str[ax], x);
-      const T kp = r[(R_T1 + f) * S], k2 = r[(R_T2 + f) * S];
-      const T kq = wQ[ax] * k2, kr = wR[ax] * k2;
-      if (NB == 8) { caxpy(y[0], -G * ih2, x[0]); caxpy(y[1], -G * ih2, x[1]); }
-      caxpy(y[2], -kp + kq, x[2]); caxpy(y[2], -sq2 * kq, x[7]);
-      caxpy(y[3], -kp - kq, x[3]);
-      caxpy(y[4], -kp - kq, x[4]);
-      caxpy(y[5], -kp + kq, x[5]); caxpy(y[5], sq2 * kq, x[6]);
-      caxpy(y[6], -kp, x[6]); caxpy(y[6], sq2 * kq, x[5]);
-      caxpy(y[7], -kp, x[7]); caxpy(y[7], -sq2 * kq, x[2]);
-      if (ax < 2) {
-        caxpy(y[2], kr, x[4]);
-        caxpy(y[3], kr, x[5]); caxpy(y[3], -sq2 * kr, x[6]);
-        caxpy(y[4], kr, x[2]); caxpy(y[4], sq2 * kr, x[7]);
-        caxpy(y[5], kr, x[3]);
-        caxpy(y[6], -sq2 * kr, x[3]);
-        caxpy(y[7], sq2 * kr, x[4]);
-      }
-      if (NB == 8) {
-        // w = signed neighbour value is folded into su/sv; U w = -i su w, V w = -i sv w,
-        // V^H w = -i conj(sv) w.
-        const T su = r[(R_SU + f) * S];
-        const cplx<T> sv = mk<T>(r[(R_SVR + f) * S], r[(R_SVI + f) * S]);
-        // conduction rows from valence inputs
-        cplx<T> m1 = x[2]; caxpy(m1, sq2, x[7]);                   // V^H (x2 + sqrt2 x7)
-        const cplx<T> m2 = cscale(sq3, x[4]);                      // V (sqrt3 x4)
-        cplx<T> m3 = cscale(-sq2, x[5]); m3 = csub(m3, x[6]);      // U (-sqrt2 x5 - x6)
-        cplx<T> acc = czero<T>();
-        cfmac(acc, sv, m1); cfma(acc, sv, m2); caxpy(acc, su, m3);
-        caxpy_i(y[0], T(-1), acc);
-        cplx<T> n1 = cscale(-sq2, x[2]); n1 = cadd(n1, x[7]);      // U (-sqrt2 x2 + x7)
-        const cplx<T> n2 = cscale(-sq3, x[3]);                     // V^H (-sqrt3 x3)
-        cplx<T> n3 = cscale(sq2, x[6]); n3 = csub(n3, x[5]);       // V (-x5 + sqrt2 x6)
-        acc = czero<T>();
-        caxpy(acc, su, n1); cfmac(acc, sv, n2); cfma(acc, sv, n3);
-        caxpy_i(y[1], T(-1), acc);
-        // valence rows from conduction inputs
-        cplx<T> Vw0 = czero<T>(), VHw0 = czero<T>(), Vw1 = czero<T>(), VHw1 = czero<T>();
-        cfma(Vw0, sv, x[0]); cfmac(VHw0, sv, x[0]); cfma(Vw1, sv, x[1]); cfmac(VHw1, sv, x[1]);
-        const cplx<T> Uw0 = cscale(su, x[0]), Uw1 = cscale(su, x[1]);
-        // every term carries the common factor -i
-        cplx<T> t2 = Vw0; caxpy(t2, -sq2, Uw1); caxpy_i(y[2], T(-1), t2);
-        caxpy_i(y[3], sq3, Vw1);
-        caxpy_i(y[4], -sq3, VHw0);
-        cplx<T> t5 = cscale(-sq2, Uw0); t5 = csub(t5, VHw1); caxpy_i(y[5], T(-1), t5);
-        cplx<T> t6 = cscale(sq2, VHw1); t6 = csub(t6, Uw0); caxpy_i(y[6], T(-1), t6);
-        cplx<T> t7 = cscale(sq2, Vw0); t7 = cadd(t7, Uw1); caxpy_i(y[7], T(-1), t7);
-      }
+  for (int f = 0; f < 6; ++f) {
+    const int ax = f >> 1, dir = f & 1;
+    if (!(msk & (1u << f))) continue;
+    ld.face(f, x);
+    const T kp = rc.face(ax, dir, 0), k2 = rc.face(ax, dir, 1);
+    const T kq = wQ[ax] * k2;
+    if (NB == 8) { caxpy(y[0], cb, x[0]); caxpy(y[1], cb, x[1]); }
+    caxpy(y[2], -kp + kq, x[2]); caxpy(y[2], -sq2 * kq, x[7]);
+    caxpy(y[3], -kp - kq, x[3]);
+    caxpy(y[4], -kp - kq, x[4]);
+    caxpy(y[5], -kp + kq, x[5]); caxpy(y[5], sq2 * kq, x[6]);
+    caxpy(y[6], -kp, x[6]); caxpy(y[6], sq2 * kq, x[5]);
+    caxpy(y[7], -kp, x[7]); caxpy(y[7], -sq2 * kq, x[2]);
+    if (ax < 2) {
+      const T kr = wR[ax] * k2;
+      caxpy(y[2], kr, x[4]);
+      caxpy(y[3], kr, x[5]); caxpy(y[3], -sq2 * kr, x[6]);
+      caxpy(y[4], kr, x[2]); caxpy(y[4], sq2 * kr, x[7]);
+      caxpy(y[5], kr, x[3]);
+      caxpy(y[6], -sq2 * kr, x[3]);
+      caxpy(y[7], sq2 * kr, x[4]);
     }
-
-    // ---- twelve edge neighbours: cross(g3, a, b) ---------------------------------------
-    // plane xy -> R (+i cR) / R^H (-i cR); plane zx -> S, S^H (cS); plane zy -> S (-i cS),
-    // S^H (+i cS). Coefficient of x(p + sa e_a + sb e_b): -(sa sb)/(8h^2) (g_{sa a} + g_{sb b}).
-#pragma unroll
-    for (int pl = 0; pl < 3; ++pl) {
-      const int ea = pl == 0 ? 0 : 2;      // xy: a = x; zx, zy: a = z
-      const int eb = pl == 0 ? 1 : (pl == 1 ? 0 : 1);
-#pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        const int sa = (e & 1) ? -1 : 1, sb = (e & 2) ? -1 : 1;
-        if (!(msk & (1u << (6 + 4 * pl + e)))) continue;
-        const T ga = r[(R_G3 + 2 * ea + (sa < 0)) * S];
-        const T gb = r[(R_G3 + 2 * eb + (sb < 0)) * S];
-        const T c = T(2) * sq3 * G * (-(T)(sa * sb) * i8h2) * (ga + gb);
-        load_site<T, NB, true>(xs, bstr, sa * str[ea] + sb * str[eb], x);
-        if (pl == 0) {
-          caxpy_i(y[2], c, x[4]);
-          caxpy_i(y[4], -c, x[2]);
-          caxpy_i(y[3], c, x[5]);
-          caxpy_i(y[5], -c, x[3]);
-          caxpy_i(y[3], -sq2 * c, x[6]);
-          caxpy_i(y[6], sq2 * c, x[3]);
-          caxpy_i(y[4], -sq2 * c, x[7]);
-          caxpy_i(y[7], sq2 * c, x[4]);
-        } else if (pl == 1) {
-          caxpy(y[3], -c, x[2]); caxpy(y[2], sq32 * c, x[6]); caxpy(y[3], isq2 * c, x[7]);
-          caxpy(y[5], c, x[4]); caxpy(y[6], isq2 * c, x[4]); caxpy(y[7], sq32 * c, x[5]);
-          caxpy(y[2], -c, x[3]); caxpy(y[6], sq32 * c, x[2]); caxpy(y[7], isq2 * c, x[3]);
-          caxpy(y[4], c, x[5]); caxpy(y[4], isq2 * c, x[6]); caxpy(y[5], sq32 * c, x[7]);
-        } else {
-          // S entries get -i c, S^H entries +i c
-          caxpy_i(y[3], c, x[2]); caxpy_i(y[2], -sq32 * c, x[6]); caxpy_i(y[3], -isq2 * c, x[7]);
-          caxpy_i(y[5], -c, x[4]); caxpy_i(y[6], -isq2 * c, x[4]); caxpy_i(y[7], -sq32 * c, x[5]);
-          caxpy_i(y[2], -c, x[3]); caxpy_i(y[6], sq32 * c, x[2]); caxpy_i(y[7], isq2 * c, x[3]);
-          caxpy_i(y[4], c, x[5]); caxpy_i(y[4], isq2 * c, x[6]); caxpy_i(y[5], sq32 * c, x[7]);
-        }
-      }
+    if (NB == 8) {
+      // first-order weights of this face; U w = -i su w, V w = -i sv w, V^H w = -i conj(sv) w
+      // for the neighbour value w.
+      const T su = rc.face(ax, dir, 2);
+      const cplx<T> sv = mk<T>(rc.face(ax, dir, 3), rc.face(ax, dir, 4));
+      // conduction rows from valence inputs
+      cplx<T> m1 = x[2]; caxpy(m1, sq2, x[7]);                   // V^H (x2 + sqrt2 x7)
+      const cplx<T> m2 = cscale(sq3, x[4]);                      // V (sqrt3 x4)
+      cplx<T> m3 = cscale(-sq2, x[5]); m3 = csub(m3, x[6]);      // U (-sqrt2 x5 - x6)
+      cplx<T> acc = czero<T>();
+      cfmac(acc, sv, m1); cfma(acc, sv, m2); caxpy(acc, su, m3);
+      caxpy_i(y[0], T(-1), acc);
+      cplx<T> n1 = cscale(-sq2, x[2]); n1 = cadd(n1, x[7]);      // U (-sqrt2 x2 + x7)
+      const cplx<T> n2 = cscale(-sq3, x[3]);                     // V^H (-sqrt3 x3)
+      cplx<T> n3 = cscale(sq2, x[6]); n3 = csub(n3, x[5]);       // V (-x5 + sqrt2 x6)
+      acc = czero<T>();
+      caxpy(acc, su, n1); cfmac(acc, sv, n2); cfma(acc, sv, n3);
+      caxpy_i(y[1], T(-1), acc);
+      // valence rows from conduction inputs
+      cplx<T> Vw0 = czero<T>(), VHw0 = czero<T>(), Vw1 = czero<T>(), VHw1 = czero<T>();
+      cfma(Vw0, sv, x[0]); cfmac(VHw0, sv, x[0]); cfma(Vw1, sv, x[1]); cfmac(VHw1, sv, x[1]);
+      const cplx<T> Uw0 = cscale(su, x[0]), Uw1 = cscale(su, x[1]);
+      // every term carries the common factor -i
+      cplx<T> t2 = Vw0; caxpy(t2, -sq2, Uw1); caxpy_i(y[2], T(-1), t2);
+      caxpy_i(y[3], sq3, Vw1);
+      caxpy_i(y[4], -sq3, VHw0);
+      cplx<T> t5 = cscale(-sq2, Uw0); t5 = csub(t5, VHw1); caxpy_i(y[5], T(-1), t5);
+      cplx<T> t6 = cscale(sq2, VHw1); t6 = csub(t6, Uw0); caxpy_i(y[6], T(-1), t6);
+      cplx<T> t7 = cscale(sq2, Vw0); t7 = cadd(t7, Uw1); caxpy_i(y[7], T(-1), t7);
     }
+  }
 
-    // ---- sign (hole convention / negation), store ---------------------------------------
+  // ---- twelve edge neighbours: cross(g3, a, b) ---------------------------------------
+  // z = sum_e c_e x(p + sa e_a + sb e_b) over the plane's edges, then the plane's constant
+  // band mixing: xy -> R (+i z) / R^H (-i z); zx -> S, S^H (z); zy -> S (-i z), S^H (+i z).
 #pragma unroll
-    for (int b = 0; b < 8; ++b) {
-      if (!has_band<NB>(b)) continue;
-      a.Y[(s * a.ldy + j) + (long long)((b - band_off<NB>()) * ystr)] = cscale(a.sign, y[b]);
+  for (int pl = 0; pl < 3; ++pl) {
+    if (!(msk & (0xFu << (6 + 4 * pl)))) continue;
+    cplx<T> z[8];
+#pragma unroll
+    for (int b = 0; b < 8; ++b) z[b] = czero<T>();
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      if (!(msk & (1u << (6 + 4 * pl + e)))) continue;
+      ld.edge(pl, e, x);
+      const T c = rc.own(K_EDGE + 4 * pl + e);
+#pragma unroll
+      for (int b = 2; b < 8; ++b) caxpy(z[b], c, x[b]);
+    }
+    if (pl == 0) {
+      caxpy_i(y[2], T(1), z[4]);
+      caxpy_i(y[4], T(-1), z[2]);
+      caxpy_i(y[3], T(1), z[5]);
+      caxpy_i(y[5], T(-1), z[3]);
+      caxpy_i(y[3], -sq2, z[6]);
+      caxpy_i(y[6], sq2, z[3]);
+      caxpy_i(y[4], -sq2, z[7]);
+      caxpy_i(y[7], sq2, z[4]);
+    } else if (pl == 1) {
+      caxpy(y[3], T(-1), z[2]); caxpy(y[2], sq32, z[6]); caxpy(y[3], isq2, z[7]);
+      caxpy(y[5], T(1), z[4]); caxpy(y[6], isq2, z[4]); caxpy(y[7], sq32, z[5]);
+      caxpy(y[2], T(-1), z[3]); caxpy(y[6], sq32, z[2]); caxpy(y[7], isq2, z[3]);
+      caxpy(y[4], T(1), z[5]); caxpy(y[4], isq2, z[6]); caxpy(y[5], sq32, z[7]);
+    } else {
+      caxpy_i(y[3], T(1), z[2]); caxpy_i(y[2], -sq32, z[6]); caxpy_i(y[3], -isq2, z[7]);
+      caxpy_i(y[5], T(-1), z[4]); caxpy_i(y[6], -isq2, z[4]); caxpy_i(y[7], -sq32, z[5]);
+      caxpy_i(y[2], T(-1), z[3]); caxpy_i(y[6], sq32, z[2]); caxpy_i(y[7], isq2, z[3]);
+      caxpy_i(y[4], T(1), z[5]); caxpy_i(y[4], isq2, z[6]); caxpy_i(y[5], sq32, z[7]);
     }
   }
 }
 
+// ---------------------------------------------------------------------------------------------
+// complex64 form of the same arithmetic on packed f32x2 registers (sm_100 `fma.rn.f32x2`):
+// a complex value is one 64-bit register pair, and every term is a real scalar (broadcast to
+// both halves) times a neighbour value. Products that carry a factor i go to a second
+// accumulator yi, so the result is Y = y + i yi and complex coefficients c = cr + i ci split
+// into cr -> y and ci -> yi. Half the issue slots of the scalar form for the same arithmetic.
+// ---------------------------------------------------------------------------------------------
+typedef unsigned long long f2;
+__device__ __forceinline__ f2 f2pk(float a, float b) {
+  f2 r; asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b)); return r;
+}
+__device__ __forceinline__ f2 f2bc(float s) { return f2pk(s, s); }
+__device__ __forceinline__ float2 f2up(f2 v) {
+  float2 r; asm("mov.b64 {%0, %1}, %2;" : "=f"(r.x), "=f"(r.y) : "l"(v)); return r;
+}
+__device__ __forceinline__ f2 fma2(f2 a, f2 b, f2 c) {
+  f2 d; asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c)); return d;
+}
+__device__ __forceinline__ f2 mul2(f2 a, f2 b) {
+  f2 d; asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b)); return d;
+}
+__device__ __forceinline__ f2 add2(f2 a, f2 b) {
+  f2 d; asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b)); return d;
+}
+__device__ __forceinline__ f2 sub2(f2 a, f2 b) {
+  f2 d; asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b)); return d;
+}
+
+template <class L, class Rc>
+__device__ __forceinline__ void hx_math_packed(const L& ld, const Rc& rc, unsigned msk,
+                                               float shift, float cb, float2 (&Y)[8]) {
+  const float sq2 = 1.41421356237309504880f, sq3 = 1.73205080756887729353f;
+  const float sq32 = 1.22474487139158904910f, isq2 = 0.70710678118654752440f;
+  const f2 C2 = f2bc(sq2), CN2 = f2bc(-sq2), C3 = f2bc(sq3), C32 = f2bc(sq32);
+  const f2 CN32 = f2bc(-sq32), Ci2 = f2bc(isq2), CNi2 = f2bc(-isq2), CN1 = f2bc(-1.f);
+  const f2 CB = f2bc(cb);
+  f2 y[8], yi[8], x[8];
+
+  // ---- local block, the shift -sigma folded into the diagonal ---------------------------
+  ld.centre2(x);
+  {
+    const float Rr = rc.own(K_RRE), Ri = rc.own(K_RIM), Sr = rc.own(K_SRE), Si = rc.own(K_SIM);
+    const float q2 = rc.own(K_Q2);
+    const f2 PA = f2bc(rc.own(K_A) + shift), P2 = f2bc(rc.own(K_A2) + shift);
+    const f2 P3 = f2bc(rc.own(K_A3) + shift), P6 = f2bc(rc.own(K_A6) + shift);
+    const f2 Q2 = f2bc(q2), NQ2 = f2bc(-q2);
+    const f2 SR = f2bc(Sr), NSR = f2bc(-Sr), SI = f2bc(Si), NSI = f2bc(-Si);
+    const f2 RR = f2bc(Rr), RI = f2bc(Ri), NRI = f2bc(-Ri);
+    const f2 S32R = f2bc(sq32 * Sr), S32I = f2bc(sq32 * Si), NS32I = f2bc(-sq32 * Si);
+    const f2 R2R = f2bc(sq2 * Rr), NR2R = f2bc(-sq2 * Rr), R2I = f2bc(sq2 * Ri);
+    const f2 NR2I = f2bc(-sq2 * Ri);
+    const f2 SI2R = f2bc(isq2 * Sr), SI2I = f2bc(isq2 * Si), NSI2I = f2bc(-isq2 * Si);
+    y[0] = mul2(PA, x[0]); y[1] = mul2(PA, x[1]);
+    yi[0] = 0ull; yi[1] = 0ull;
+    y[2] = fma2(NSR, x[3], mul2(P2, x[2]));   yi[2] = mul2(SI, x[3]);
+    y[2] = fma2(RR, x[4], y[2]);              yi[2] = fma2(RI, x[4], yi[2]);
+    y[2] = fma2(S32R, x[6], y[2]);            yi[2] = fma2(S32I, x[6], yi[2]);
+    y[2] = fma2(NQ2, x[7], y[2]);
+    y[3] = fma2(NSR, x[2], mul2(P3, x[3]));   yi[3] = mul2(NSI, x[2]);
+    y[3] = fma2(RR, x[5], y[3]);              yi[3] = fma2(RI, x[5], yi[3]);
+    y[3] = fma2(NR2R, x[6], y[3]);            yi[3] = fma2(NR2I, x[6], yi[3]);
+    y[3] = fma2(SI2R, x[7], y[3]);            yi[3] = fma2(SI2I, x[7], yi[3]);
+    y[4] = fma2(RR, x[2], mul2(P3, x[4]));    yi[4] = mul2(NRI, x[2]);
+    y[4] = fma2(SR, x[5], y[4]);              yi[4] = fma2(NSI, x[5], yi[4]);
+    y[4] = fma2(SI2R, x[6], y[4]);            yi[4] = fma2(NSI2I, x[6], yi[4]);
+    y[4] = fma2(R2R, x[7], y[4]);             yi[4] = fma2(NR2I, x[7], yi[4]);
+    y[5] = fma2(RR, x[3], mul2(P2, x[5]));    yi[5] = mul2(NRI, x[3]);
+    y[5] = fma2(SR, x[4], y[5]);              yi[5] = fma2(SI, x[4], yi[5]);
+    y[5] = fma2(Q2, x[6], y[5]);
+    y[5] = fma2(S32R, x[7], y[5]);            yi[5] = fma2(NS32I, x[7], yi[5]);
+    y[6] = fma2(S32R, x[2], mul2(P6, x[6]));  yi[6] = mul2(NS32I, x[2]);
+    y[6] = fma2(NR2R, x[3], y[6]);            yi[6] = fma2(R2I, x[3], yi[6]);
+    y[6] = fma2(SI2R, x[4], y[6]);            yi[6] = fma2(SI2I, x[4], yi[6]);
+    y[6] = fma2(Q2, x[5], y[6]);
+    y[7] = fma2(NQ2, x[2], mul2(P6, x[7]));
+    y[7] = fma2(SI2R, x[3], y[7]);            yi[7] = mul2(NSI2I, x[3]);
+    y[7] = fma2(R2R, x[4], y[7]);             yi[7] = fma2(R2I, x[4], yi[7]);
+    y[7] = fma2(S32R, x[5], y[7]);            yi[7] = fma2(S32I, x[5], yi[7]);
+  }
+
+  // ---- six face neighbours ------------------------------------------------------------
+#pragma unroll
+  for (int f = 0; f < 6; ++f) {
+    const int ax = f >> 1, dir = f & 1;
+    if (!(msk & (1u << f))) continue;
+    ld.face2(f, x);
+    const float kp = rc.face(ax, dir, 0), k2 = rc.face(ax, dir, 1);
+    const float kq = (ax == 2 ? -2.f : 1.f) * k2;
+    y[0] = fma2(CB, x[0], y[0]); y[1] = fma2(CB, x[1], y[1]);
+    const f2 KPQ = f2bc(kq - kp), NKPQ = f2bc(-kp - kq), NKP = f2bc(-kp);
+    const f2 K2Q = f2bc(sq2 * kq), NK2Q = f2bc(-sq2 * kq);
+    y[2] = fma2(KPQ, x[2], y[2]); y[2] = fma2(NK2Q, x[7], y[2]);
+    y[3] = fma2(NKPQ, x[3], y[3]);
+    y[4] = fma2(NKPQ, x[4], y[4]);
+    y[5] = fma2(KPQ, x[5], y[5]); y[5] = fma2(K2Q, x[6], y[5]);
+    y[6] = fma2(NKP, x[6], y[6]); y[6] = fma2(K2Q, x[5], y[6]);
+    y[7] = fma2(NKP, x[7], y[7]); y[7] = fma2(NK2Q, x[2], y[7]);
+    if (ax < 2) {
+      const float kr = (ax == 0 ? -sq3 : sq3) * k2;
+      const f2 KR = f2bc(kr), K2R = f2bc(sq2 * kr), NK2R = f2bc(-sq2 * kr);
+      y[2] = fma2(KR, x[4], y[2]);
+      y[3] = fma2(KR, x[5], y[3]); y[3] = fma2(NK2R, x[6], y[3]);
+      y[4] = fma2(KR, x[2], y[4]); y[4] = fma2(K2R, x[7], y[4]);
+      y[5] = fma2(KR, x[3], y[5]);
+      y[6] = fma2(NK2R, x[3], y[6]);
+      y[7] = fma2(K2R, x[4], y[7]);
+    }
+    // first-order (U, V) couplings with the face weights su (real), sv = svr + i svi:
+    //   y0 += -i [conj(sv)(x2 + sqrt2 x7) + sv sqrt3 x4 + su (-sqrt2 x5 - x6)]
+    //   y1 += -i [su (-sqrt2 x2 + x7) - conj(sv) sqrt3 x3 + sv (-x5 + sqrt2 x6)]
+    //   y2..y7 from x0, x1 (the adjoint blocks)
+    const float su = rc.face(ax, dir, 2), svr = rc.face(ax, dir, 3), svi = rc.face(ax, dir, 4);
+    const f2 SVI = f2bc(svi), SVR = f2bc(svr), SU = f2bc(su), NSVR = f2bc(-svr), NSU = f2bc(-su);
+    const f2 S2SU = f2bc(sq2 * su), N3SVI = f2bc(-sq3 * svi), S3SVR = f2bc(sq3 * svr);
+    const f2 N3SVR = f2bc(-sq3 * svr), N2SVI = f2bc(-sq2 * svi), N2SVR = f2bc(-sq2 * svr);
+    const f2 S2SVI = f2bc(sq2 * svi);
+    {
+      const f2 t = fma2(C2, x[7], x[2]);        // x2 + sqrt2 x7
+      const f2 u = mul2(C3, x[4]);              // sqrt3 x4
+      y[0] = fma2(SVI, sub2(u, t), y[0]);
+      yi[0] = fma2(NSVR, add2(u, t), yi[0]);
+      yi[0] = fma2(SU, fma2(C2, x[5], x[6]), yi[0]);
+      const f2 v = mul2(C3, x[3]);              // sqrt3 x3
+      const f2 w = fma2(CN2, x[6], x[5]);       // x5 - sqrt2 x6
+      y[1] = fma2(SVI, sub2(v, w), y[1]);
+      yi[1] = fma2(SVR, add2(v, w), yi[1]);
+      yi[1] = fma2(SU, fma2(C2, x[2], mul2(CN1, x[7])), yi[1]);
+    }
+    y[2] = fma2(SVI, x[0], y[2]);   yi[2] = fma2(NSVR, x[0], yi[2]); yi[2] = fma2(S2SU, x[1], yi[2]);
+    y[3] = fma2(N3SVI, x[1], y[3]); yi[3] = fma2(S3SVR, x[1], yi[3]);
+    y[4] = fma2(N3SVI, x[0], y[4]); yi[4] = fma2(N3SVR, x[0], yi[4]);
+    y[5] = fma2(SVI, x[1], y[5]);   yi[5] = fma2(S2SU, x[0], yi[5]); yi[5] = fma2(SVR, x[1], yi[5]);
+    y[6] = fma2(N2SVI, x[1], y[6]); yi[6] = fma2(N2SVR, x[1], yi[6]); yi[6] = fma2(SU, x[0], yi[6]);
+    y[7] = fma2(S2SVI, x[0], y[7]); yi[7] = fma2(N2SVR, x[0], yi[7]); yi[7] = fma2(NSU, x[1], yi[7]);
+  }
+
+  // ---- twelve edge neighbours: z = sum_e c_e x_e, then the plane's band mixing ---------
+#pragma unroll
+  for (int pl = 0; pl < 3; ++pl) {
+    if (!(msk & (0xFu << (6 + 4 * pl)))) continue;
+    f2 z[8];
+#pragma unroll
+    for (int b = 2; b < 8; ++b) z[b] = 0ull;
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      if (!(msk & (1u << (6 + 4 * pl + e)))) continue;
+      ld.edge2(pl, e, x);
+      const f2 C = f2bc(rc.own(K_EDGE + 4 * pl + e));
+#pragma unroll
+      for (int b = 2; b < 8; ++b) z[b] = fma2(C, x[b], z[b]);
+    }
+    if (pl == 0) {            // R: +i z, R^H: -i z
+      yi[2] = add2(yi[2], z[4]); yi[4] = sub2(yi[4], z[2]);
+      yi[3] = add2(yi[3], z[5]); yi[5] = sub2(yi[5], z[3]);
+      yi[3] = fma2(CN2, z[6], yi[3]); yi[6] = fma2(C2, z[3], yi[6]);
+      yi[4] = fma2(CN2, z[7], yi[4]); yi[7] = fma2(C2, z[4], yi[7]);
+    } else if (pl == 1) {     // S, S^H: z
+      y[3] = sub2(y[3], z[2]); y[2] = fma2(C32, z[6], y[2]); y[3] = fma2(Ci2, z[7], y[3]);
+      y[5] = add2(y[5], z[4]); y[6] = fma2(Ci2, z[4], y[6]); y[7] = fma2(C32, z[5], y[7]);
+      y[2] = sub2(y[2], z[3]); y[6] = fma2(C32, z[2], y[6]); y[7] = fma2(Ci2, z[3], y[7]);
+      y[4] = add2(y[4], z[5]); y[4] = fma2(Ci2, z[6], y[4]); y[5] = fma2(C32, z[7], y[5]);
+    } else {                  // S: -i z, S^H: +i z
+      yi[3] = add2(yi[3], z[2]); yi[2] = fma2(CN32, z[6], yi[2]); yi[3] = fma2(CNi2, z[7], yi[3]);
+      yi[5] = sub2(yi[5], z[4]); yi[6] = fma2(CNi2, z[4], yi[6]); yi[7] = fma2(CN32, z[5], yi[7]);
+      yi[2] = sub2(yi[2], z[3]); yi[6] = fma2(C32, z[2], yi[6]); yi[7] = fma2(Ci2, z[3], yi[7]);
+      yi[4] = add2(yi[4], z[5]); yi[4] = fma2(Ci2, z[6], yi[4]); yi[5] = fma2(C32, z[7], yi[5]);
+    }
+  }
+
+  // ---- Y = y + i yi -------------------------------------------------------------------
+#pragma unroll
+  for (int b = 0; b < 8; ++b) {
+    const float2 a = f2up(y[b]), c = f2up(yi[b]);
+    Y[b] = make_float2(a.x - c.y, a.y + c.x);
+  }
+}
+
+// complex64 eight-band blocks take the packed form, everything else the scalar one
+template <typename T, int NB, class L, class Rc>
+__device__ __forceinline__ void hx_compute(const L& ld, const Rc& rc, unsigned msk, T shift,
+                                           T cb, cplx<T> (&y)[8]) {
+  if constexpr (std::is_same<T, float>::value && NB == 8) hx_math_packed(ld, rc, msk, shift, cb, y);
+  else hx_math<T, NB>(ld, rc, msk, shift, cb, y);
+}
+
+// neighbour mask of site (ix, iy, iz): bit f (0..5) face x+, x-, y+, y-, z+, z-; bit
+// 6 + 4 pl + e the in-plane edge e of plane pl (xy, zx, zy), sa = e & 1 ? -1 : 1,
+// sb = e & 2 ? -1 : 1 (a = x, z, z; b = y, x, y). An edge exists when both of its faces do.
+__device__ __forceinline__ unsigned site_mask(int ix, int iy, int iz, int nx, int ny, int nz) {
+  const unsigned xp = ix + 1 < nx, xm = ix > 0, yp = iy + 1 < ny, ym = iy > 0;
+  const unsigned zp = iz + 1 < nz, zm = iz > 0;
+  unsigned m = xp | (xm << 1) | (yp << 2) | (ym << 3) | (zp << 4) | (zm << 5);
+  m |= (xp & yp) << 6 | (xm & yp) << 7 | (xp & ym) << 8 | (xm & ym) << 9;      // xy
+  m |= (zp & xp) << 10 | (zm & xp) << 11 | (zp & xm) << 12 | (zm & xm) << 13;  // zx
+  m |= (zp & yp) << 14 | (zm & yp) << 15 | (zp & ym) << 16 | (zm & ym) << 17;  // zy
+  return m;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Direct kernel: one thread per (site, column), neighbours read through L1/L2. Serves the six-
+// and four-band slices, blocks the staged kernel cannot take, and the batched engine.
+// ---------------------------------------------------------------------------------------------
+template <typename T>
+struct HXArgs {
+  const T* __restrict__ rec;
+  const unsigned* __restrict__ msk;
+  const cplx<T>* __restrict__ X;
+  cplx<T>* __restrict__ Y;
+  int N, ldx, ldy, m, sx, sy;   // sites, leading dimensions, columns, site strides of x and y
+  int nz, nzp, NP;              // z extent, its padded record extent, record entry stride
+  T shift;                      // -sigma for a shifted apply, else 0
+  T cb;                         // conduction-band face weight sign (-G / h^2)
+};
+
+// x[b] = X[band b, site s + offset, column j] with xs = &X[0, s, j], bs = N ldx (elements);
+// every offset fits 32 bits for the grids this library accepts (n ldx < 2^31).
 template <typename T, int NB>
-__global__ void __launch_bounds__(256, ApplyOcc<T>::kMinBlocks) kp_apply_kernel(const ApplyArgs<T> a) {
-  extern __shared__ unsigned char smem_raw[];
-  apply_tile<T, NB>(a, (long long)blockIdx.x * a.S, reinterpret_cast<T*>(smem_raw));
+struct GlobalLoader {
+  const cplx<T>* __restrict__ xs;
+  int bs, xstr[3];
+  __device__ __forceinline__ void at(int off, bool vb_only, cplx<T> (&x)[8]) const {
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+      if (!has_band<NB>(b) || (vb_only && b < 2)) { x[b] = czero<T>(); continue; }
+      x[b] = __ldg(xs + ((b - band_off<NB>()) * bs + off));
+    }
+  }
+  __device__ __forceinline__ void centre(cplx<T> (&x)[8]) const { at(0, false, x); }
+  __device__ __forceinline__ void face(int f, cplx<T> (&x)[8]) const {
+    at((f & 1) ? -xstr[f >> 1] : xstr[f >> 1], false, x);
+  }
+  __device__ __forceinline__ void edge(int pl, int e, cplx<T> (&x)[8]) const {
+    const int ea = pl == 0 ? 0 : 2, eb = pl == 0 ? 1 : (pl == 1 ? 0 : 1);
+    const int sa = (e & 1) ? -1 : 1, sb = (e & 2) ? -1 : 1;
+    at(sa * xstr[ea] + sb * xstr[eb], true, x);
+  }
+  // packed complex64 loads (eight bands only)
+  __device__ __forceinline__ void at2(int off, int b0, f2 (&x)[8]) const {
+    const unsigned long long* p = reinterpret_cast<const unsigned long long*>(xs);
+#pragma unroll
+    for (int b = b0; b < 8; ++b) x[b] = __ldg(p + (b * bs + off));
+  }
+  __device__ __forceinline__ void centre2(f2 (&x)[8]) const { at2(0, 0, x); }
+  __device__ __forceinline__ void face2(int f, f2 (&x)[8]) const {
+    at2((f & 1) ? -xstr[f >> 1] : xstr[f >> 1], 0, x);
+  }
+  __device__ __forceinline__ void edge2(int pl, int e, f2 (&x)[8]) const {
+    const int ea = pl == 0 ? 0 : 2, eb = pl == 0 ? 1 : (pl == 1 ? 0 : 1);
+    const int sa = (e & 1) ? -1 : 1, sb = (e & 2) ? -1 : 1;
+    at2(sa * xstr[ea] + sb * xstr[eb], 2, x);
+  }
+};
+
+template <typename T>
+struct GlobalRecord {
+  const T* __restrict__ R;   // record base + padded site index
+  int NP;
+  __device__ __forceinline__ T own(int k) const { return __ldg(R + k * NP); }
+  __device__ __forceinline__ T face(int ax, int dir, int k) const {
+    return own(K_FACE + 5 * (2 * ax + dir) + k);
+  }
+};
+
+template <typename T, int NB>
+__device__ __forceinline__ void hx_item(const HXArgs<T>& a, int s, int j) {
+  GlobalLoader<T, NB> ld;
+  ld.xs = a.X + ((long long)s * a.ldx + j);
+  ld.bs = a.N * a.ldx;
+  ld.xstr[0] = a.sx * a.ldx; ld.xstr[1] = a.sy * a.ldx; ld.xstr[2] = a.ldx;
+  GlobalRecord<T> rc;
+  rc.R = a.rec + (s + (s / a.nz) * (a.nzp - a.nz));
+  rc.NP = a.NP;
+  cplx<T> y[8];
+  hx_compute<T, NB>(ld, rc, __ldg(a.msk + s), a.shift, a.cb, y);
+  cplx<T>* __restrict__ ys = a.Y + ((long long)s * a.ldy + j);
+  const int ybs = a.N * a.ldy;
+#pragma unroll
+  for (int b = 0; b < 8; ++b) {
+    if (!has_band<NB>(b)) continue;
+    ys[(b - band_off<NB>()) * ybs] = y[b];
+  }
+}
+
+constexpr int kApplyThreads = 256;
+template <typename T> struct ApplyOcc;
+template <> struct ApplyOcc<double> { static constexpr int kMinBlocks = 2; };
+template <> struct ApplyOcc<float> { static constexpr int kMinBlocks = 3; };
+
+template <typename T, int NB>
+__global__ void __launch_bounds__(kApplyThreads, ApplyOcc<T>::kMinBlocks)
+kp_apply_kernel(const HXArgs<T> a) {
+  const int it = blockIdx.x * kApplyThreads + threadIdx.x;
+  if (it >= a.N * a.m) return;
+  const int s = it / a.m;
+  hx_item<T, NB>(a, s, it - s * a.m);
 }
 
 // Many operators and blocks in one launch (the batched engine): CTA b serves slot k with
 // tile0[k] <= b < tile0[k+1]; the column count is read on the device (the slot's active width).
 template <typename T>
-__global__ void __launch_bounds__(256, ApplyOcc<T>::kMinBlocks)
+__global__ void __launch_bounds__(kApplyThreads, ApplyOcc<T>::kMinBlocks)
 kp_apply_multi_kernel(const HXSlot* __restrict__ slots, int nslots) {
-  extern __shared__ unsigned char smem_raw[];
   int k = 0;
   while (k + 1 < nslots && (int)blockIdx.x >= slots[k + 1].tile0) ++k;
   const HXSlot& d = slots[k];
   if (d.skip && *d.skip) return;
   const int m = d.m_dev ? *d.m_dev : d.m;
-  if (m <= 0) return;
-  ApplyArgs<T> a;
-  a.F = static_cast<const T*>(d.F);
+  const int it = (blockIdx.x - d.tile0) * kApplyThreads + threadIdx.x;
+  if (m <= 0 || it >= d.N * m) return;
+  HXArgs<T> a;
+  a.rec = static_cast<const T*>(d.rec);
+  a.msk = d.msk;
   a.X = static_cast<const cplx<T>*>(d.X);
   a.Y = static_cast<cplx<T>*>(d.Y);
   a.N = d.N; a.ldx = d.ld_same ? m : d.ldx; a.ldy = d.ld_same ? m : d.ldy;
-  a.nx = d.nx; a.ny = d.ny; a.nz = d.nz; a.m = m; a.flags = d.flags; a.S = d.S;
-  a.h = (T)d.h; a.sigma = (T)d.sigma; a.sign = (T)d.sign; a.shifted = d.shifted;
-  apply_tile<T, 8>(a, (long long)(blockIdx.x - d.tile0) * d.S, reinterpret_cast<T*>(smem_raw));
+  a.m = m; a.sx = d.sx; a.sy = d.sy;
+  a.nz = d.sy; a.nzp = d.nzp; a.NP = d.NP;
+  a.shift = d.shifted ? (T)(-d.sigma) : T(0);
+  a.cb = (T)d.cb;
+  const int s = it / m;
+  hx_item<T, 8>(a, s, it - s * m);
 }
 
-int launch_apply_multi(const HXSlot* slots_dev, int nslots, int total_tiles, int S_max,
-                       int precision, cudaStream_t st) {
-  if (total_tiles <= 0) return QDKP_OK;
-  if (precision == QDKP_C128) {
-    kp_apply_multi_kernel<double><<<total_tiles, 256,
-        (size_t)R_COUNT * S_max * sizeof(double) + S_max * sizeof(unsigned), st>>>(slots_dev, nslots);
-  } else {
-    kp_apply_multi_kernel<float><<<total_tiles, 256,
-        (size_t)R_COUNT * S_max * sizeof(float) + S_max * sizeof(unsigned), st>>>(slots_dev, nslots);
+// ---------------------------------------------------------------------------------------------
+// Staged kernel (eight bands): a CTA owns a TY x TZ tile of (y, z) sites and MC consecutive
+// columns and walks a run of x planes. A ring of four shared-memory plane buffers holds planes
+// x-1, x, x+1 of the tile with a one-site halo in y and z while plane x+2 streams in with
+// cp.async, so every X value crosses L2 about once (plus the halo) and the 19-point stencil reads
+// come from shared memory. Smem layout of a plane: [band][y + 1][z + 1][column].
+// ---------------------------------------------------------------------------------------------
+template <typename T, int MC_, int TY_, int TZ_>
+struct Staged {
+  static constexpr int MC = MC_, TY = TY_, TZ = TZ_;
+  static constexpr int PY = TY + 2, PZ = TZ + 2;
+  static constexpr int BAND = PY * PZ * MC;        // complex elements per band of a plane
+  static constexpr int PLANE = 8 * BAND;
+  static constexpr int NSLOT = 4;
+  static constexpr int RPLANE = K_COUNT * TY * TZ;   // record values of one tile plane
+  static constexpr int THREADS = TY * TZ * MC;
+  static constexpr size_t VEC_BYTES = (size_t)NSLOT * PLANE * sizeof(cplx<T>);
+  static constexpr size_t SMEM = VEC_BYTES + (size_t)2 * RPLANE * sizeof(T);
+  static_assert(TZ % 4 == 0, "record rows are copied in 16-byte z runs");
+  static_assert(SMEM <= 231424, "over the opt-in shared memory of one CTA");
+};
+
+template <typename T>
+struct StagedArgs {
+  const T* __restrict__ rec;
+  const cplx<T>* __restrict__ X;
+  cplx<T>* __restrict__ Y;
+  int N, nx, ny, nz, ldx, ldy, m;
+  int nzp, NP;
+  int tiles_z, chunks, xsplit, xlen;
+  T shift, cb;
+};
+
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void* smem_dst, const void* gmem_src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+  if (BYTES == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" :: "r"(d), "l"(gmem_src) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" :: "r"(d), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+template <typename T, class G>
+struct SmemLoader {
+  const cplx<T>* p[3];   // planes x-1, x, x+1 at this thread's (y, z, column)
+  __device__ __forceinline__ void at(const cplx<T>* q, int off, bool vb_only, cplx<T> (&x)[8]) const {
+#pragma unroll
+    for (int b = 0; b < 8; ++b) x[b] = (vb_only && b < 2) ? czero<T>() : q[b * G::BAND + off];
   }
+  __device__ __forceinline__ void centre(cplx<T> (&x)[8]) const { at(p[1], 0, false, x); }
+  __device__ __forceinline__ void face(int f, cplx<T> (&x)[8]) const {
+    const int ax = f >> 1, sg = (f & 1) ? -1 : 1;
+    if (ax == 0) at(p[1 + sg], 0, false, x);
+    else if (ax == 1) at(p[1], sg * G::PZ * G::MC, false, x);
+    else at(p[1], sg * G::MC, false, x);
+  }
+  __device__ __forceinline__ void edge(int pl, int e, cplx<T> (&x)[8]) const {
+    const int sa = (e & 1) ? -1 : 1, sb = (e & 2) ? -1 : 1;
+    if (pl == 0) at(p[1 + sa], sb * G::PZ * G::MC, true, x);                 // a = x, b = y
+    else if (pl == 1) at(p[1 + sb], sa * G::MC, true, x);                    // a = z, b = x
+    else at(p[1], sa * G::MC + sb * G::PZ * G::MC, true, x);                 // a = z, b = y
+  }
+  // packed complex64 loads
+  __device__ __forceinline__ void at2(const cplx<T>* q, int off, int b0, f2 (&x)[8]) const {
+#pragma unroll
+    for (int b = b0; b < 8; ++b) x[b] = *reinterpret_cast<const f2*>(q + b * G::BAND + off);
+  }
+  __device__ __forceinline__ void centre2(f2 (&x)[8]) const { at2(p[1], 0, 0, x); }
+  __device__ __forceinline__ void face2(int f, f2 (&x)[8]) const {
+    const int ax = f >> 1, sg = (f & 1) ? -1 : 1;
+    if (ax == 0) at2(p[1 + sg], 0, 0, x);
+    else if (ax == 1) at2(p[1], sg * G::PZ * G::MC, 0, x);
+    else at2(p[1], sg * G::MC, 0, x);
+  }
+  __device__ __forceinline__ void edge2(int pl, int e, f2 (&x)[8]) const {
+    const int sa = (e & 1) ? -1 : 1, sb = (e & 2) ? -1 : 1;
+    if (pl == 0) at2(p[1 + sa], sb * G::PZ * G::MC, 2, x);
+    else if (pl == 1) at2(p[1 + sb], sa * G::MC, 2, x);
+    else at2(p[1], sa * G::MC + sb * G::PZ * G::MC, 2, x);
+  }
+};
+
+template <typename T, class G, bool V16>
+__device__ __forceinline__ void copy_plane(const StagedArgs<T>& a, cplx<T>* slot, int xp,
+                                           int y0, int z0, int c0) {
+  constexpr int EPU = V16 ? (int)(16 / sizeof(cplx<T>)) : 1;   // complex elements per copy
+  constexpr int UPC = G::MC / EPU;                              // copies per (band, y, z) cell
+  constexpr int UNITS = 8 * G::PY * G::PZ * UPC;
+  for (int u = threadIdx.x; u < UNITS; u += G::THREADS) {
+    const int cu = u % UPC;
+    int r = u / UPC;
+    const int zz = r % G::PZ; r /= G::PZ;
+    const int yy = r % G::PY;
+    const int bb = r / G::PY;
+    const int gy = y0 - 1 + yy, gz = z0 - 1 + zz, gc = c0 + cu * EPU;
+    if (gy < 0 || gy >= a.ny || gz < 0 || gz >= a.nz || gc >= a.m) continue;
+    const int site = (xp * a.ny + gy) * a.nz + gz;
+    const cplx<T>* src = a.X + ((long long)(bb * a.N + site) * a.ldx + gc);
+    cplx<T>* dst = slot + ((bb * G::PY + yy) * G::PZ + zz) * G::MC + cu * EPU;
+    cp_async<V16 ? 16 : (int)sizeof(cplx<T>)>(dst, src);
+  }
+}
+
+// The tile's records of plane xp: rows (entry k, y) of TZ values, in 16-byte runs (z0 and TZ are
+// multiples of 4, nzp too, so a run never straddles the padded row end).
+template <typename T, class G>
+__device__ __forceinline__ void copy_record(const StagedArgs<T>& a, T* slot, int xp, int y0,
+                                            int z0) {
+  constexpr int EPU = (int)(16 / sizeof(T));
+  constexpr int RUNS = G::TZ / EPU;
+  constexpr int UNITS = K_COUNT * G::TY * RUNS;
+  for (int u = threadIdx.x; u < UNITS; u += G::THREADS) {
+    const int ru = u % RUNS;
+    const int r = u / RUNS;
+    const int ty = r % G::TY;
+    const int k = r / G::TY;
+    const int gy = y0 + ty, gz = z0 + ru * EPU;
+    if (gy >= a.ny || gz >= a.nzp) continue;
+    const T* src = a.rec + ((long long)k * a.NP + ((long long)xp * a.ny + gy) * a.nzp + gz);
+    cp_async<16>(slot + (k * G::TY + ty) * G::TZ + ru * EPU, src);
+  }
+}
+
+template <typename T, class G>
+struct SmemRecord {
+  const T* r;     // record slot + ty * TZ + tz
+  __device__ __forceinline__ T own(int k) const { return r[k * G::TY * G::TZ]; }
+  __device__ __forceinline__ T face(int ax, int dir, int k) const {
+    return own(K_FACE + 5 * (2 * ax + dir) + k);
+  }
+};
+
+template <typename T, class G, bool V16>
+__global__ void __launch_bounds__(G::THREADS, 1) kp_apply_staged_kernel(const StagedArgs<T> a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<T>* ring = reinterpret_cast<cplx<T>*>(smem_raw);
+  T* rring = reinterpret_cast<T*>(smem_raw + G::VEC_BYTES);
+  int bid = blockIdx.x;
+  const int xs = bid % a.xsplit; bid /= a.xsplit;
+  const int ch = bid % a.chunks; bid /= a.chunks;
+  const int tzi = bid % a.tiles_z;
+  const int tyi = bid / a.tiles_z;
+  const int c0 = ch * G::MC, y0 = tyi * G::TY, z0 = tzi * G::TZ;
+  const int xa = xs * a.xlen, xb = min(a.nx, xa + a.xlen);
+  if (c0 >= a.m || xa >= xb) return;          // uniform over the CTA
+  const int t = threadIdx.x;
+  const int c = t % G::MC, tz = (t / G::MC) % G::TZ, ty = t / (G::MC * G::TZ);
+  const int iy = y0 + ty, iz = z0 + tz, col = c0 + c;
+  const bool active = iy < a.ny && iz < a.nz && col < a.m;
+  const int cell = ((ty + 1) * G::PZ + (tz + 1)) * G::MC + c;
+
+  if (xa > 0) copy_plane<T, G, V16>(a, ring + ((xa - 1) & 3) * G::PLANE, xa - 1, y0, z0, c0);
+  cp_async_commit();
+  copy_plane<T, G, V16>(a, ring + (xa & 3) * G::PLANE, xa, y0, z0, c0);
+  copy_record<T, G>(a, rring + (xa & 1) * G::RPLANE, xa, y0, z0);
+  cp_async_commit();
+  if (xa + 1 < a.nx) copy_plane<T, G, V16>(a, ring + ((xa + 1) & 3) * G::PLANE, xa + 1, y0, z0, c0);
+  cp_async_commit();
+  for (int x = xa; x < xb; ++x) {
+    cp_async_wait_all();
+    __syncthreads();                          // planes x-1..x+1 landed; slot (x+2) & 3 is free
+    if (x + 2 <= xb && x + 2 < a.nx)
+      copy_plane<T, G, V16>(a, ring + ((x + 2) & 3) * G::PLANE, x + 2, y0, z0, c0);
+    if (x + 1 < xb) copy_record<T, G>(a, rring + ((x + 1) & 1) * G::RPLANE, x + 1, y0, z0);
+    cp_async_commit();
+    if (!active) continue;
+    SmemLoader<T, G> ld;
+    ld.p[0] = ring + ((x + 3) & 3) * G::PLANE + cell;
+    ld.p[1] = ring + (x & 3) * G::PLANE + cell;
+    ld.p[2] = ring + ((x + 1) & 3) * G::PLANE + cell;
+    const int s = (x * a.ny + iy) * a.nz + iz;
+    SmemRecord<T, G> rc;
+    rc.r = rring + (x & 1) * G::RPLANE + ty * G::TZ + tz;
+    cplx<T> y[8];
+    hx_compute<T, 8>(ld, rc, site_mask(x, iy, iz, a.nx, a.ny, a.nz), a.shift, a.cb, y);
+    cplx<T>* __restrict__ ys = a.Y + ((long long)s * a.ldy + col);
+    const int ybs = a.N * a.ldy;
+#pragma unroll
+    for (int b = 0; b < 8; ++b) ys[b * ybs] = y[b];
+  }
+  cp_async_wait_all();
+}
+
+// Tile shapes the staged kernel is built for: {precision, MC, TY, TZ}.
+template <typename T> struct StagedCfgs;
+template <> struct StagedCfgs<float> {
+  using C0 = Staged<float, 4, 8, 12>;
+  using C1 = Staged<float, 4, 6, 16>;
+  using C2 = Staged<float, 4, 4, 20>;
+  using C3 = Staged<float, 2, 8, 24>;
+};
+template <> struct StagedCfgs<double> {
+  using C0 = Staged<double, 2, 8, 12>;
+  using C1 = Staged<double, 2, 6, 16>;
+  using C2 = Staged<double, 2, 4, 20>;
+  using C3 = Staged<double, 1, 8, 16>;
+};
+constexpr int kStagedCfgs = 4;
+constexpr int kDirect = -2;      // staged_cfg value selecting the direct kernel
+
+struct StagedGeom { int tiles_y, tiles_z, chunks, xsplit, xlen, ctas; };
+
+// CTA decomposition for a grid: x is split so that the CTA count fills whole waves of one CTA
+// per SM, trading the two halo planes each extra x run costs.
+static StagedGeom staged_geom(int nx, int ny, int nz, int m, int MC, int TY, int TZ, int sms) {
+  StagedGeom g;
+  g.tiles_y = (ny + TY - 1) / TY;
+  g.tiles_z = (nz + TZ - 1) / TZ;
+  g.chunks = (m + MC - 1) / MC;
+  const long long base = (long long)g.tiles_y * g.tiles_z * g.chunks;
+  double best = 1e30;
+  g.xsplit = 1;
+  for (int xs = 1; xs <= nx; ++xs) {
+    const int xlen = (nx + xs - 1) / xs;
+    if ((long long)(xs - 1) * xlen >= nx) continue;
+    const long long ctas = base * xs;
+    const double cost = (double)((ctas + sms - 1) / sms) * (xlen + 2);
+    if (cost < best - 1e-9) { best = cost; g.xsplit = xs; }
+  }
+  g.xlen = (nx + g.xsplit - 1) / g.xsplit;
+  g.ctas = (int)(base * g.xsplit);
+  return g;
+}
+
+template <typename T, class G, bool V16>
+static int launch_staged_g(const qdkp_operator* op, const T* rec, const void* X, int ldx,
+                           void* Y, int ldy, int m, T shift, T cb, int sms, cudaStream_t st) {
+  static bool attr_done = false;     // per instantiation; the attribute is per device function
+  if (!attr_done) {
+    QDKP_CUDA_TRY(cudaFuncSetAttribute(kp_apply_staged_kernel<T, G, V16>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::SMEM));
+    attr_done = true;
+  }
+  const StagedGeom g = staged_geom(op->nx, op->ny, op->nz, m, G::MC, G::TY, G::TZ, sms);
+  StagedArgs<T> a;
+  a.rec = rec;
+  a.X = static_cast<const cplx<T>*>(X);
+  a.Y = static_cast<cplx<T>*>(Y);
+  a.N = (int)op->n_sites; a.nx = op->nx; a.ny = op->ny; a.nz = op->nz;
+  a.ldx = ldx; a.ldy = ldy; a.m = m;
+  a.nzp = op->nzp; a.NP = op->nx * op->ny * op->nzp;
+  a.tiles_z = g.tiles_z; a.chunks = g.chunks; a.xsplit = g.xsplit; a.xlen = g.xlen;
+  a.shift = shift; a.cb = cb;
+  kp_apply_staged_kernel<T, G, V16><<<g.ctas, G::THREADS, G::SMEM, st>>>(a);
   count_launch();
   QDKP_CUDA_TRY(cudaGetLastError());
   return QDKP_OK;
 }
 
-int apply_tile_sites(int m) {
-  int S = (512 + m - 1) / m;
-  return S < 32 ? 32 : (S > 128 ? 128 : S);
+template <typename T, class G>
+static int launch_staged_v(const qdkp_operator* op, const T* rec, const void* X, int ldx,
+                           void* Y, int ldy, int m, T shift, T cb, int sms, cudaStream_t st) {
+  // 16-byte copies need 16-byte aligned sources: always true for complex128 (with an aligned
+  // base); for complex64 the leading dimension, the column count and the chunk must be even.
+  const bool aligned = ((uintptr_t)X & 15) == 0;
+  const bool v16 = aligned && (sizeof(T) == 8 || (ldx % 2 == 0 && m % 2 == 0 && G::MC % 2 == 0));
+  if (v16) return launch_staged_g<T, G, true>(op, rec, X, ldx, Y, ldy, m, shift, cb, sms, st);
+  return launch_staged_g<T, G, false>(op, rec, X, ldx, Y, ldy, m, shift, cb, sms, st);
 }
 
 template <typename T>
-static int launch_apply_t(const qdkp_operator* op, const T* F, const void* X, int64_t ldx,
-                          void* Y, int64_t ldy, int m, double sigma, int shifted,
+static int launch_staged(int cfg, const qdkp_operator* op, const T* rec, const void* X, int ldx,
+                         void* Y, int ldy, int m, T shift, T cb, int sms, cudaStream_t st) {
+  using C = StagedCfgs<T>;
+  switch (cfg) {
+    case 0: return launch_staged_v<T, typename C::C0>(op, rec, X, ldx, Y, ldy, m, shift, cb, sms, st);
+    case 1: return launch_staged_v<T, typename C::C1>(op, rec, X, ldx, Y, ldy, m, shift, cb, sms, st);
+    case 2: return launch_staged_v<T, typename C::C2>(op, rec, X, ldx, Y, ldy, m, shift, cb, sms, st);
+    default: return launch_staged_v<T, typename C::C3>(op, rec, X, ldx, Y, ldy, m, shift, cb, sms, st);
+  }
+}
+
+int launch_apply_multi(const HXSlot* slots_dev, int nslots, int total_tiles, int precision,
+                       cudaStream_t st) {
+  if (total_tiles <= 0) return QDKP_OK;
+  if (precision == QDKP_C128)
+    kp_apply_multi_kernel<double><<<total_tiles, kApplyThreads, 0, st>>>(slots_dev, nslots);
+  else
+    kp_apply_multi_kernel<float><<<total_tiles, kApplyThreads, 0, st>>>(slots_dev, nslots);
+  count_launch();
+  QDKP_CUDA_TRY(cudaGetLastError());
+  return QDKP_OK;
+}
+
+int apply_tiles(int64_t n_sites, int m) {
+  return (int)((n_sites * m + kApplyThreads - 1) / kApplyThreads);
+}
+
+// sign of the operator as applied: -1 for a hole-convention 6/4-band slice, flipped by NEGATE
+static double op_sign(const qdkp_operator* op) {
+  double sign = ((op->flags & QDKP_HOLE_CONVENTION) && op->n_bands != 8) ? -1.0 : 1.0;
+  if (op->flags & QDKP_NEGATE) sign = -sign;
+  return sign;
+}
+
+double apply_cb_weight(const qdkp_operator* op) { return op_sign(op) * (-kG / (op->h * op->h)); }
+
+int build_records(qdkp_operator* op) {
+  const long long N = op->n_sites;
+  const int blocks = (int)std::min<long long>((N + 127) / 128, 148 * 16);
+  kp_record_kernel<<<blocks, 128>>>(op->fields64, N, op->nx, op->ny, op->nz, op->nzp, op->h,
+                                     op->flags, op->n_bands, op_sign(op), op->rec64, op->rec32,
+                                     op->nbmask);
+  count_launch();
+  QDKP_CUDA_TRY(cudaGetLastError());
+  QDKP_CUDA_TRY(cudaDeviceSynchronize());
+  return QDKP_OK;
+}
+
+size_t record_doubles(int nx, int ny, int nzp) { return (size_t)K_COUNT * nx * ny * nzp; }
+
+static int num_sms(int device) {
+  static int cached[64] = {0};
+  if (device < 0 || device >= 64) return 148;
+  if (!cached[device]) {
+    int v = 0;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || v <= 0)
+      v = 148;
+    cached[device] = v;
+  }
+  return cached[device];
+}
+
+// Staged tile shape for a launch: the fewest padded (y, z) sites per useful site, ties to the
+// lower index (the larger tiles).
+static int pick_staged_cfg(const qdkp_operator* op, int precision) {
+  static const int shape[2][kStagedCfgs][2] = {
+      {{8, 12}, {6, 16}, {4, 20}, {8, 16}},   // complex128: TY, TZ
+      {{8, 12}, {6, 16}, {4, 20}, {8, 24}}};  // complex64
+  int best = 0;
+  double best_w = 1e30;
+  for (int c = 0; c < kStagedCfgs; ++c) {
+    const int TY = shape[precision == QDKP_C64][c][0], TZ = shape[precision == QDKP_C64][c][1];
+    const double w = (double)((op->ny + TY - 1) / TY * TY) * ((op->nz + TZ - 1) / TZ * TZ) *
+                     (1.0 + 2.0 / TY) * (1.0 + 2.0 / TZ);
+    if (w < best_w - 1e-9) { best_w = w; best = c; }
+  }
+  return best;
+}
+
+template <typename T>
+static int launch_apply_t(const qdkp_operator* op, const T* rec, const void* X, int64_t ldx,
+                          void* Y, int64_t ldy, int m, double sigma, int shifted, int precision,
                           cudaStream_t st) {
   if ((int64_t)op->n_bands * op->n_sites * std::max(ldx, ldy) >= (int64_t(1) << 31)) {
     set_error("H.X: n * leading dimension must stay below 2^31 elements");
     return QDKP_ERR_UNSUPPORTED;
   }
-  ApplyArgs<T> a;
-  a.F = F;
+  const T shift = shifted ? (T)(-sigma) : T(0);
+  const T cb = (T)apply_cb_weight(op);
+  const int forced = op->staged_cfg[precision == QDKP_C64];
+  if (op->n_bands == 8 && forced != kDirect && ((uintptr_t)X % sizeof(cplx<T>)) == 0) {
+    const int cfg = forced >= 0 ? forced : pick_staged_cfg(op, precision);
+    return launch_staged<T>(cfg, op, rec, X, (int)ldx, Y, (int)ldy, m, shift, cb,
+                            num_sms(op->device), st);
+  }
+  HXArgs<T> a;
+  a.rec = rec;
+  a.msk = op->nbmask;
   a.X = static_cast<const cplx<T>*>(X);
   a.Y = static_cast<cplx<T>*>(Y);
-  a.N = op->n_sites; a.ldx = ldx; a.ldy = ldy;
-  a.nx = op->nx; a.ny = op->ny; a.nz = op->nz; a.m = m; a.flags = op->flags;
-  a.h = (T)op->h; a.sigma = (T)sigma; a.shifted = shifted;
-  a.sign = ((op->flags & QDKP_HOLE_CONVENTION) && op->n_bands != 8) ? T(-1) : T(1);
-  if (op->flags & QDKP_NEGATE) a.sign = -a.sign;
-  const int S = apply_tile_sites(m);
-  a.S = S;
-  const size_t smem = (size_t)R_COUNT * S * sizeof(T) + (size_t)S * sizeof(unsigned);
-  const unsigned grid = (unsigned)((op->n_sites + S - 1) / S);
+  a.N = (int)op->n_sites; a.ldx = (int)ldx; a.ldy = (int)ldy; a.m = m;
+  a.sx = op->ny * op->nz; a.sy = op->nz;
+  a.nz = op->nz; a.nzp = op->nzp; a.NP = op->nx * op->ny * op->nzp;
+  a.shift = shift;
+  a.cb = cb;
+  const unsigned grid = (unsigned)apply_tiles(op->n_sites, m);
   switch (op->n_bands) {
-    case 8: kp_apply_kernel<T, 8><<<grid, 256, smem, st>>>(a); break;
-    case 6: kp_apply_kernel<T, 6><<<grid, 256, smem, st>>>(a); break;
-    case 4: kp_apply_kernel<T, 4><<<grid, 256, smem, st>>>(a); break;
+    case 8: kp_apply_kernel<T, 8><<<grid, kApplyThreads, 0, st>>>(a); break;
+    case 6: kp_apply_kernel<T, 6><<<grid, kApplyThreads, 0, st>>>(a); break;
+    case 4: kp_apply_kernel<T, 4><<<grid, kApplyThreads, 0, st>>>(a); break;
     default: set_error("n_bands must be 8, 6 or 4"); return QDKP_ERR_ARG;
   }
   count_launch();
@@ -434,11 +1034,70 @@ static int launch_apply_t(const qdkp_operator* op, const T* F, const void* X, in
 int launch_apply(const qdkp_operator* op, const void* X, int64_t ldx, void* Y, int64_t ldy,
                  int m, double sigma, int shifted, int precision, cudaStream_t st) {
   if (precision == QDKP_C128)
-    return launch_apply_t<double>(op, op->fields64, X, ldx, Y, ldy, m, sigma, shifted, st);
+    return launch_apply_t<double>(op, op->rec64, X, ldx, Y, ldy, m, sigma, shifted, precision, st);
   if (precision == QDKP_C64)
-    return launch_apply_t<float>(op, op->fields32, X, ldx, Y, ldy, m, sigma, shifted, st);
+    return launch_apply_t<float>(op, op->rec32, X, ldx, Y, ldy, m, sigma, shifted, precision, st);
   set_error("precision must be QDKP_C128 or QDKP_C64");
   return QDKP_ERR_ARG;
 }
 
 }  // namespace qdkp
+
+using namespace qdkp;
+
+extern "C" {
+
+int qdkp_operator_set_tile(qdkp_operator* op, int precision, int tile) {
+  QDKP_CHECK_ARG(op != nullptr, "operator must not be NULL");
+  QDKP_CHECK_ARG(precision == QDKP_C128 || precision == QDKP_C64, "bad precision");
+  QDKP_CHECK_ARG(tile >= QDKP_TILE_DIRECT && tile < kStagedCfgs, "tile out of range");
+  op->staged_cfg[precision == QDKP_C64] = tile;
+  return QDKP_OK;
+}
+
+int qdkp_operator_get_tile(const qdkp_operator* op, int precision, int* tile) {
+  QDKP_CHECK_ARG(op != nullptr && tile != nullptr, "NULL argument");
+  QDKP_CHECK_ARG(precision == QDKP_C128 || precision == QDKP_C64, "bad precision");
+  *tile = op->staged_cfg[precision == QDKP_C64];
+  return QDKP_OK;
+}
+
+int qdkp_operator_tune(qdkp_operator* op, const void* X, int64_t ldx, void* Y, int64_t ldy,
+                       int m, int precision, int reps, double* seconds, void* stream) {
+  QDKP_CHECK_ARG(op != nullptr && X != nullptr && Y != nullptr, "NULL argument");
+  QDKP_CHECK_ARG(precision == QDKP_C128 || precision == QDKP_C64, "bad precision");
+  QDKP_CHECK_ARG(m > 0 && ldx >= m && ldy >= m && reps > 0, "bad block or repetitions");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  QDKP_CUDA_TRY(cudaSetDevice(op->device));
+  const int pi = precision == QDKP_C64;
+  const int saved = op->staged_cfg[pi];
+  cudaEvent_t e0, e1;
+  QDKP_CUDA_TRY(cudaEventCreate(&e0));
+  QDKP_CUDA_TRY(cudaEventCreate(&e1));
+  int best = saved;
+  float best_ms = 3.4e38f;
+  int rc = QDKP_OK;
+  const int first = op->n_bands == 8 ? 0 : kStagedCfgs;   // 6/4-band slices: direct only
+  for (int c = first; c <= kStagedCfgs && rc == QDKP_OK; ++c) {
+    const int tile = c < kStagedCfgs ? c : kDirect;
+    op->staged_cfg[pi] = tile;
+    rc = launch_apply(op, X, ldx, Y, ldy, m, 0.0, 0, precision, st);      // warm-up
+    if (rc != QDKP_OK) break;
+    if (cudaEventRecord(e0, st) != cudaSuccess) { rc = QDKP_ERR_CUDA; break; }
+    for (int r = 0; r < reps && rc == QDKP_OK; ++r)
+      rc = launch_apply(op, X, ldx, Y, ldy, m, 0.0, 0, precision, st);
+    if (rc != QDKP_OK) break;
+    float ms = 0.f;
+    if (cudaEventRecord(e1, st) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+        cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) { rc = QDKP_ERR_CUDA; break; }
+    if (seconds) seconds[c - first] = ms * 1e-3 / reps;
+    if (ms < best_ms) { best_ms = ms; best = tile; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  op->staged_cfg[pi] = rc == QDKP_OK ? best : saved;
+  if (rc == QDKP_ERR_CUDA) set_error("qdkp_operator_tune: CUDA event failure");
+  return rc;
+}
+
+}  // extern "C"

@@ -6,6 +6,8 @@
 
 #include "../../include/qdkp.h"
 
+struct qdkp_operator;
+
 namespace qdkp {
 
 // ---------------------------------------------------------------------------------------------
@@ -55,6 +57,7 @@ QDKP_CPLX_OPS(float2, float)
 void set_error(const std::string& msg);
 // Counts kernel launches made by this library (qdkp_kernel_launches).
 void count_launch(int n = 1);
+long long launches_so_far();
 
 #define QDKP_CUDA_TRY(expr)                                                              \
   do {                                                                                   \
@@ -80,24 +83,31 @@ constexpr double kG = 0.0380998;   // hbar^2 / 2 m0 in eV nm^2 (qdsolver_core.py
 
 // One operator/block pair of a multi-slot H.X launch (eight bands).
 struct HXSlot {
-  const void* F;          // fields in the launch precision
+  const void* rec;        // operator record in the launch precision
+  const unsigned* msk;    // neighbour masks of the operator's sites
   const void* X;
   void* Y;
-  long long N, ldx, ldy;
-  int nx, ny, nz, flags;
-  int S;                  // sites per tile
+  int N, ldx, ldy;        // sites; leading dimensions (unused when ld_same)
+  int sx, sy;             // site strides of x and y (ny nz, nz)
   int tile0;              // first CTA of this slot in the launch
   int m;                  // column count if m_dev is NULL
   const int* m_dev;       // device column count (active width), or NULL
   const int* skip;        // nonzero: slot idle this tick
   int ld_same;            // leading dimensions equal the column count
+  int nzp, NP;            // padded z extent of the record and its entry stride
   int shifted;
-  double h, sigma, sign;
+  double sigma;
+  double cb;              // conduction-band face weight (apply_cb_weight)
 };
 
-int launch_apply_multi(const HXSlot* slots_dev, int nslots, int total_tiles, int S_max,
-                       int precision, cudaStream_t st);
-int apply_tile_sites(int m);
+int launch_apply_multi(const HXSlot* slots_dev, int nslots, int total_tiles, int precision,
+                       cudaStream_t st);
+// CTAs one H.X launch uses for n_sites x m items
+int apply_tiles(int64_t n_sites, int m);
+double apply_cb_weight(const qdkp_operator* op);
+// (re)build the per-site stencil record and neighbour masks from fields64
+int build_records(qdkp_operator* op);
+size_t record_doubles(int nx, int ny, int nzp);
 
 }  // namespace qdkp
 
@@ -110,6 +120,10 @@ struct qdkp_operator {
   int flags;              // QDKP_* flags
   int device;
   double* fields64;       // device, F_COUNT * n_sites doubles (library-owned)
-  float* fields32;        // device, F_COUNT * n_sites floats (library-owned)
+  int nzp;                // nz rounded up to a multiple of 4 (record rows)
+  double* rec64;          // device, per-site stencil record (FP64), record_doubles(nx, ny, nzp)
+  float* rec32;           // the same record in FP32
+  unsigned* nbmask;       // device, per-site neighbour mask
+  int staged_cfg[2];      // staged H.X tile shape per precision (c128, c64); -1 = by heuristic
   int64_t nnz_equiv;      // CSR nonzero count of the equivalent assembled matrix
 };

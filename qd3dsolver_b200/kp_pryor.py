@@ -203,6 +203,37 @@ class KPOperator(spla.LinearOperator):
               'qdkp_apply')
         return Y
 
+    def set_tile(self, tile, precision=_lib.C128):
+        """Force the H.X kernel for this operator and precision: a staged tile shape
+        0..TILE_COUNT-1, TILE_DIRECT, or TILE_AUTO (padding heuristic)."""
+        check(lib().qdkp_operator_set_tile(self.handle, precision, int(tile)),
+              'qdkp_operator_set_tile')
+
+    def get_tile(self, precision=_lib.C128):
+        t = ctypes.c_int()
+        check(lib().qdkp_operator_get_tile(self.handle, precision, ctypes.byref(t)),
+              'qdkp_operator_get_tile')
+        return t.value
+
+    def tune(self, m, dtype=None, reps=5):
+        """Autotune the H.X kernel for (n, m) blocks of `dtype` (complex128 by default): time
+        every staged tile shape and the direct kernel on a random block, keep the fastest for
+        this operator. Returns {tile: seconds per launch}."""
+        torch = _torch()
+        dtype = dtype or torch.complex128
+        prec = {torch.complex128: _lib.C128, torch.complex64: _lib.C64}[dtype]
+        dev = f'cuda:{self.device}'
+        X = torch.randn(self.shape[0], m, dtype=dtype, device=dev)
+        Y = torch.empty_like(X)
+        secs = (ctypes.c_double * (_lib.TILE_COUNT + 1))()
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        check(lib().qdkp_operator_tune(self.handle, X.data_ptr(), m, Y.data_ptr(), m, m, prec,
+                                       int(reps), secs, stream), 'qdkp_operator_tune')
+        tiles = list(range(_lib.TILE_COUNT)) + [_lib.TILE_DIRECT]
+        if self.n_bands != 8:
+            return {_lib.TILE_DIRECT: secs[0]}
+        return {t: secs[i] for i, t in enumerate(tiles)}
+
     def negated(self):
         """-H as a second device operator (same fields, sign flipped in the stencil)."""
         f = {k: (v.reshape(self.grid_shape) if v is not None else None)

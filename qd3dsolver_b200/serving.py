@@ -11,6 +11,12 @@ that arrive later. Admission checks free HBM before a slot's workspace is alloca
   Request(H, k, sigma, ...)          -- one solve (folded around sigma, or extremal)
   solve_batch(requests)              -- continuous batching over a list, all present at t = 0
   serve(requests, arrivals)          -- requests that arrive over time; p50 / p99 latency
+
+Mixed precision (Request(precision='mixed')): a request first iterates in complex64 (H.X on
+the packed FP32 stencil, tall blocks in complex64, every Gram, Cholesky and Rayleigh-Ritz matrix
+in FP64) down to `mixed_tol`, above the complex64 rounding floor of the folded residual; its
+Ritz block is then promoted to a complex128 slot (re-orthonormalised, Rayleigh-Ritz in FP64)
+that iterates to `tol`. Results, selection and residuals are the complex128 ones.
 """
 import ctypes
 import time
@@ -40,12 +46,16 @@ class Request:
     seed: int = 0
     folded: bool = True
     tag: object = None
+    precision: str = 'c128'        # 'c128', or 'mixed' (complex64 search, complex128 finish)
+    mixed_tol: float = 1e-4        # residual at which a mixed request leaves complex64
     # filled in by the engine
     slot: int = -1
     t_arrive: float = 0.0
     t_admit: float = 0.0
     t_done: float = 0.0
     result: dict = field(default=None)
+    phase: str = 'c128'            # precision of the slot the request occupies
+    iters_done: int = 0            # iterations of finished phases
 
     @property
     def block(self):
@@ -56,7 +66,7 @@ class Request:
 class Engine:
     """The batched engine on one device: admit, step, poll, retire."""
 
-    def __init__(self, max_slots=64, device=None):
+    def __init__(self, max_slots=64, device=None, graphs=True):
         torch = _torch()
         self.device = torch.cuda.current_device() if device is None else int(device)
         self.max_slots = int(max_slots)
@@ -64,6 +74,8 @@ class Engine:
         check(lib().qdkp_engine_create(self.max_slots, self.device, ctypes.byref(h)),
               'qdkp_engine_create')
         self._h = h
+        if not graphs:
+            check(lib().qdkp_engine_set_graphs(self._h, 0), 'qdkp_engine_set_graphs')
         self._slots = {}       # slot -> (request, workspace, X0)
         self.ticks = 0
 
@@ -83,10 +95,16 @@ class Engine:
     def stream(self):
         return _torch().cuda.current_stream(self.device).cuda_stream
 
-    def _params(self, r):
+    def _params(self, r, phase=None):
+        phase = phase or ('c64' if r.precision == 'mixed' else 'c128')
+        if phase == 'c64':
+            tol, prec = max(float(r.mixed_tol), float(r.tol or 0.0)), _lib.C64
+        else:
+            tol, prec = (float(r.tol) if r.tol else 0.0), _lib.C128
+        maxiter = max(1, int(r.maxiter) - int(r.iters_done))
         return _lib.LobpcgParams(block=r.block, folded=int(r.folded), sigma=float(r.sigma),
-                                 tol=float(r.tol) if r.tol else 0.0, maxiter=int(r.maxiter),
-                                 restart_control=20, precision=_lib.C128, verbosity=0, time_hx=0)
+                                 tol=tol, maxiter=maxiter, restart_control=20, precision=prec,
+                                 verbosity=0, time_hx=0)
 
     def workspace_bytes(self, r):
         prm = self._params(r)
@@ -102,14 +120,19 @@ class Engine:
         free_b, _ = _torch().cuda.mem_get_info(self.device)
         return free_b >= self.workspace_bytes(r) + reserve_bytes
 
-    def admit(self, r):
+    def admit(self, r, X0=None, phase=None):
+        """Give request r a slot. X0 (device, n x block complex128) defaults to the seeded start
+        block of solve_interior; `phase` ('c64' / 'c128') defaults to the request's first."""
         torch = _torch()
-        prm = self._params(r)
-        need = self.workspace_bytes(r)
+        phase = phase or ('c64' if r.precision == 'mixed' else 'c128')
+        prm = self._params(r, phase)
+        need = int(lib().qdkp_engine_slot_workspace_size(r.H.handle, ctypes.byref(prm)))
         if need == 0:
             raise ValueError(f"block {r.block} outside [1, 24]")
         ws = torch.empty(need, dtype=torch.uint8, device=f'cuda:{self.device}')
-        X0 = torch.from_numpy(start_block(r.H.shape[0], r.block, r.seed, True)).to(ws.device)
+        if X0 is None:
+            X0 = torch.from_numpy(start_block(r.H.shape[0], r.block, r.seed, True)).to(ws.device)
+        r.phase = phase
         slot = ctypes.c_int()
         check(lib().qdkp_engine_admit(self._h, r.H.handle, ctypes.byref(prm), X0.data_ptr(),
                                       ws.data_ptr(), need, self.stream, ctypes.byref(slot)),
@@ -130,6 +153,29 @@ class Engine:
         check(lib().qdkp_engine_poll(self._h, state, status, iters, self.stream),
               'qdkp_engine_poll')
         return list(state), list(status), list(iters)
+
+    def promote(self, slot):
+        """A stopped complex64 slot: its final Ritz block becomes the start block of a
+        complex128 slot for the same request. Returns the new slot."""
+        torch = _torch()
+        r, ws, X0 = self._slots.pop(slot)
+        V = torch.empty((r.H.shape[0], r.block), dtype=torch.complex128, device=ws.device)
+        lam = np.empty(r.block)
+        info = _lib.LobpcgInfo()
+        check(lib().qdkp_engine_retire(self._h, slot, lam.ctypes.data, V.data_ptr(), None,
+                                       ctypes.byref(info), self.stream), 'qdkp_engine_retire')
+        r.iters_done += int(info.iterations)
+        del ws, X0
+        return self.admit(r, X0=V, phase='c128')
+
+    def finish(self, slot):
+        """Retire a stopped slot, or promote it if it ended a complex64 phase; returns the new
+        slot id for a promotion, else None."""
+        r = self._slots[slot][0]
+        if r.phase == 'c64':
+            return self.promote(slot)
+        self.retire(slot)
+        return None
 
     def retire(self, slot, certify_tol=1e-6):
         """Final Rayleigh-Ritz, then solve_interior's selection (k nearest sigma, ascending)
@@ -154,7 +200,7 @@ class Engine:
         Vk = V[:, list(sel)].contiguous()
         _, res = _device_residuals(r.H, Vk, E)
         r.t_done = time.perf_counter()
-        r.result = dict(E=E, V=Vk, residuals=res, iterations=info.iterations, mu=lam,
+        r.result = dict(E=E, V=Vk, residuals=res, iterations=r.iters_done + info.iterations, mu=lam,
                         status=_lib.LOBPCG_STATUS.get(info.status, 'unknown'),
                         converged=bool(res.max() < certify_tol))
         del ws, X0
@@ -181,8 +227,10 @@ def solve_batch(requests, max_slots=64, ticks_per_poll=8, engine=None):
             eng.step(ticks_per_poll)
             state, status, iters = eng.poll()
             for s in [s for s in running if state[s] == 0]:
-                eng.retire(s)
-                running.pop(s)
+                r = running.pop(s)
+                s2 = eng.finish(s)
+                if s2 is not None:
+                    running[s2] = r
     finally:
         if own:
             eng.close()
@@ -211,8 +259,10 @@ def serve(requests, arrivals, max_slots=64, ticks_per_poll=8):
             eng.step(ticks_per_poll)
             state, status, iters = eng.poll()
             for s in [s for s in running if state[s] == 0]:
-                eng.retire(s)
-                running.pop(s)
+                r = running.pop(s)
+                s2 = eng.finish(s)
+                if s2 is not None:
+                    running[s2] = r
     finally:
         eng.close()
     wall = time.perf_counter() - t0

@@ -38,6 +38,24 @@ def test_apply_c64_within_single_precision(operator_cases):
         assert err < 2e-6, (c['name'], err)
 
 
+def test_c64_column_layouts(operator_cases):
+    """complex64 blocks with even, odd and strided column layouts (the staged kernel copies
+    16-byte pairs of columns only when the leading dimension and width are even)."""
+    import torch
+    rng = np.random.default_rng(5)
+    for c in [c for c in operator_cases if c['n_bands'] == 8][:6]:
+        H = _build(c)
+        n = H.shape[0]
+        for m, ld in ((4, 4), (3, 3), (4, 6), (5, 7)):
+            X = rng.standard_normal((n, m)) + 1j * rng.standard_normal((n, m))
+            ref = H @ X
+            big = torch.zeros((n, ld), dtype=torch.complex64, device='cuda')
+            big[:, :m] = torch.from_numpy(X.astype(np.complex64)).cuda()
+            Y = H.apply(big[:, :m]).cpu().numpy()
+            err = np.abs(Y - ref).max() / np.abs(ref).max()
+            assert err < 2e-6, (c['name'], m, ld, err)
+
+
 def test_shifted_and_folded_modes(operator_cases):
     import torch
     from qd3dsolver_b200 import _lib
@@ -89,3 +107,37 @@ def test_config1_operator_against_oracle():
     Yo = Ho @ X
     assert np.abs(Y - Yo).max() / np.abs(Yo).max() < 1e-13
     assert Ho.nnz <= H.nnz <= Ho.nnz * (1 + 1e-4)   # structural count bounds scipy's
+
+
+def test_every_tile_shape_matches_reference(operator_cases):
+    """Each staged tile shape and the direct kernel reproduce the reference H @ X (the
+    autotuner may pick any of them)."""
+    import torch
+    from qd3dsolver_b200 import _lib
+    cases = [c for c in operator_cases if c['n_bands'] == 8]
+    for c in cases[:10]:
+        H = _build(c)
+        for tile in list(range(_lib.TILE_COUNT)) + [_lib.TILE_DIRECT]:
+            H.set_tile(tile, _lib.C128)
+            H.set_tile(tile, _lib.C64)
+            Y = H @ c['X']
+            err = np.abs(Y - c['Y']).max() / np.abs(c['Y']).max()
+            assert err < 1e-13, (c['name'], tile, err)
+            X32 = torch.from_numpy(c['X'].astype(np.complex64)).cuda()
+            e32 = np.abs(H.apply(X32).cpu().numpy() - c['Y']).max() / np.abs(c['Y']).max()
+            assert e32 < 2e-6, (c['name'], tile, e32)
+
+
+def test_autotuner_keeps_a_valid_choice():
+    from qd3dsolver_b200 import _lib, workloads as wl
+    import torch
+    w = wl.fig4_environment(6.0)
+    from qd3dsolver_b200 import kp_pryor as kpg
+    f = w.fields
+    H = kpg.confined_hamiltonian(kpg.GridOperators(w.shape, w.h), f, 8,
+                                 strain={k: f[k] for k in wl.STRAIN_KEYS})
+    secs = H.tune(12, torch.complex128, reps=2)
+    assert len(secs) == _lib.TILE_COUNT + 1 and all(v > 0 for v in secs.values())
+    best = min(secs, key=secs.get)
+    assert H.get_tile(_lib.C128) == best
+    H.close()

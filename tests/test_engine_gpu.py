@@ -67,3 +67,45 @@ def test_engine_alone_equals_mix(ops):
         if r.tag in ('cb', 'vb'):
             assert np.abs(np.sort(r.result['E']) - np.array(ref[r.tag]['E'])).max() < 1e-6
             assert r.result['converged']
+
+
+def test_graph_replay_equals_direct_launches(ops):
+    """Ticks replayed from a captured CUDA graph give exactly the directly launched result."""
+    from qd3dsolver_b200 import serving
+    H, ref = ops['small'], ops['meta']['interior_vb']
+    out = []
+    for graphs in (True, False):
+        eng = serving.Engine(2, graphs=graphs)
+        r = serving.Request(H, k=4, sigma=ref['sigma'], tol=1e-9, maxiter=4000)
+        serving.solve_batch([r], engine=eng, ticks_per_poll=6)
+        eng.close()
+        out.append(r.result)
+    assert out[0]['iterations'] == out[1]['iterations']
+    assert np.abs(out[0]['E'] - out[1]['E']).max() <= 1e-13
+    assert np.abs(out[0]['residuals'] - out[1]['residuals']).max() <= 1e-13
+
+
+def test_mixed_precision_reaches_the_reference_levels(ops):
+    """complex64 search + complex128 finish: the reference's Fig-4 b = 10 nm levels within
+    1e-6 eV, Kramers pairs degenerate, residuals certified, and the same levels as the
+    complex128 engine; each result is the same alone and in the mix."""
+    from qd3dsolver_b200 import serving
+    w, H4 = ops['w'], ops['fig4']
+    with open(os.path.join(GOLDEN, 'fig4_b10.json')) as fh:
+        ref = json.load(fh)
+
+    def reqs(prec):
+        return [serving.Request(H4, k=8, sigma=w.sigma[b], tol=1e-7, maxiter=8000, tag=b,
+                                precision=prec) for b in ('cb', 'vb')]
+    mixed = serving.solve_batch(reqs('mixed'), max_slots=2, ticks_per_poll=8)
+    plain = serving.solve_batch(reqs('c128'), max_slots=2, ticks_per_poll=8)
+    for r, p in zip(mixed, plain):
+        E = np.sort(r.result['E'])
+        assert r.result['converged'] and r.result['residuals'].max() < 1e-6, r.tag
+        assert np.abs(E - np.array(ref[r.tag]['E'])).max() < 1e-6, r.tag
+        assert np.abs(E - np.sort(p.result['E'])).max() < 1e-6, r.tag
+        assert np.abs(E[0::2] - E[1::2]).max() < 1e-7, r.tag       # Kramers pairs
+    alone = [serving.solve_batch([r], max_slots=1, ticks_per_poll=5)[0] for r in reqs('mixed')]
+    for a, b in zip(alone, mixed):
+        assert a.result['iterations'] == b.result['iterations'], a.tag
+        assert np.abs(a.result['E'] - b.result['E']).max() <= 1e-12, a.tag
