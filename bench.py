@@ -178,13 +178,15 @@ def run_ours(args):
 
     def served_step():
         reqs = [serving.Request(H, k=K, sigma=w.sigma[band], tol=TOL, maxiter=MAXITER,
-                                tag=(w.meta['base'], band), precision=args.precision)
+                                tag=(w.meta['base'], band), precision=args.precision,
+                                mixed_tol=args.mixed_tol)
                 for w, H in zip(wls, ops) for band in BANDS]
         t0 = time.perf_counter()
         serving.solve_batch(reqs, max_slots=len(reqs), ticks_per_poll=args.ticks_per_poll)
         lat = [r.t_done - t0 for r in reqs]
         pairs = sum(int((r.result['residuals'] <= RES_TOL).sum()) for r in reqs)
         return dict(pairs=pairs, lat=lat, iters={r.tag: r.result['iterations'] for r in reqs},
+                    ticks={r.tag: r.result['ticks'] for r in reqs},
                     maxres=max(float(r.result['residuals'].max()) for r in reqs),
                     hx_s=0.0, hx_b=0.0, hx_n=0)
 
@@ -350,6 +352,8 @@ def run_ours(args):
             'latency_s': {'p50': lat[len(lat) // 2], 'p99': lat[min(len(lat) - 1, int(0.99 * len(lat)))],
                           'per': 'solve'},
             'iterations': {f"b{int(b)}_{band}": it for (b, band), it in steps[-1]['iters'].items()},
+            'ticks_per_phase': ({f"b{int(b)}_{band}": t for (b, band), t in steps[-1]['ticks'].items()}
+                                if 'ticks' in steps[-1] else None),
             'roofline': {'kernel': 'kp_apply_kernel<double,8> (H.X, timed in the plain form)',
                          'bound': 'hbm',
                          'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
@@ -527,6 +531,8 @@ def main():
                     help='only run the served engine for --probe-ticks ticks (profiling)')
     ap.add_argument('--probe-ticks', type=int, default=20)
     ap.add_argument('--ticks-per-poll', type=int, default=16)
+    ap.add_argument('--mixed-tol', type=float, default=1e-4,
+                    help='residual at which a mixed-precision solve leaves complex64')
     ap.add_argument('--precision', choices=('mixed', 'c128'), default='mixed',
                     help='served form: complex64 search + complex128 finish, or complex128 only')
     args = ap.parse_args()

@@ -188,6 +188,9 @@ typedef struct {
   int precision;         /* QDKP_C128 (plain) or QDKP_C64 (search directions in complex64) */
   int verbosity;         /* 0 = silent */
   int time_hx;           /* 1: time every H X launch with CUDA events (info->hx_seconds) */
+  int stall_iterations;  /* batched engine only: > 0 stops a slot (status QDKP_LOBPCG_MAXITER)
+                            once its best mean residual is this many iterations old; used to end
+                            a complex64 search phase that has reached its rounding floor */
 } qdkp_lobpcg_params;
 
 typedef struct {
@@ -255,6 +258,24 @@ int qdkp_engine_poll(qdkp_engine* e, int* state, int* status, int* iterations, v
  * V (device, n x block complex128), residuals[block] (host, may be NULL); frees the slot. */
 int qdkp_engine_retire(qdkp_engine* e, int slot, double* lambda, void* V, double* residuals,
                        qdkp_lobpcg_info* info, void* stream);
+
+/*
+ * The tall-skinny block products of scipy's LOBPCG (the Gram assembly X^H A X, X^H A R, ... at
+ * lobpcg.py:833-880 and the Ritz updates X Cx + R Cr + P Cp at lobpcg.py:921-973), on device
+ * blocks of complex128 (FP64 tensor-core MMA) or complex64 (split-precision TF32 tensor-core MMA
+ * accumulated in FP32, partial sums in FP64).
+ *   qdkp_block_gram:   out (host, P x Q complex128, row-major) = A^H B, A (n x P, lda), B (n x Q)
+ *   qdkp_block_update: Y (n x q) = A (n x P) C, C (host, P x q complex128, row-major)
+ * Synchronous on `stream`; workspaces from the *_workspace_size functions.
+ */
+size_t qdkp_block_gram_workspace_size(int P, int Q);
+int qdkp_block_gram(const void* A, int64_t lda, int P, const void* B, int64_t ldb, int Q,
+                    int64_t n, int precision, double* out, void* ws, size_t ws_bytes,
+                    void* stream);
+size_t qdkp_block_update_workspace_size(int P, int q);
+int qdkp_block_update(const void* A, int64_t lda, int P, const double* C, int q, int64_t n,
+                      void* Y, int64_t ldy, int precision, void* ws, size_t ws_bytes,
+                      void* stream);
 
 /*
  * Rayleigh quotients and residual norms of H for the columns of V (device, n x k complex128,

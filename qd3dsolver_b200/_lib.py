@@ -26,7 +26,8 @@ class LobpcgParams(ctypes.Structure):
     _fields_ = [('block', ctypes.c_int), ('folded', ctypes.c_int), ('sigma', ctypes.c_double),
                 ('tol', ctypes.c_double), ('maxiter', ctypes.c_int),
                 ('restart_control', ctypes.c_int), ('precision', ctypes.c_int),
-                ('verbosity', ctypes.c_int), ('time_hx', ctypes.c_int)]
+                ('verbosity', ctypes.c_int), ('time_hx', ctypes.c_int),
+                ('stall_iterations', ctypes.c_int)]
 
 
 class LobpcgInfo(ctypes.Structure):
@@ -95,6 +96,16 @@ _SIGNATURES = {
     'qdkp_engine_retire': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
                                           ctypes.c_void_p, ctypes.c_void_p,
                                           ctypes.POINTER(LobpcgInfo), ctypes.c_void_p]),
+    'qdkp_block_gram_workspace_size': (ctypes.c_size_t, [ctypes.c_int, ctypes.c_int]),
+    'qdkp_block_gram': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int,
+                                       ctypes.c_void_p, ctypes.c_int64, ctypes.c_int,
+                                       ctypes.c_int64, ctypes.c_int, ctypes.c_void_p,
+                                       ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]),
+    'qdkp_block_update_workspace_size': (ctypes.c_size_t, [ctypes.c_int, ctypes.c_int]),
+    'qdkp_block_update': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int,
+                                         ctypes.c_void_p, ctypes.c_int, ctypes.c_int64,
+                                         ctypes.c_void_p, ctypes.c_int64, ctypes.c_int,
+                                         ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]),
     'qdkp_residuals_workspace_size': (ctypes.c_size_t, [ctypes.c_void_p, ctypes.c_int]),
     'qdkp_residuals': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
                                       ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,

@@ -158,8 +158,14 @@ gram_partial_kernel(const BlockList<T> A, const BlockList<T> B, long long n,
   extern __shared__ __align__(16) unsigned char gsm_d[];
   const int RP = (2 * A.total() + 7) / 8 * 8, RQ = (2 * B.total() + 7) / 8 * 8;
   const long long r0 = blockIdx.x * rows_per_part;
-  gram_core<MR, MC>(A, B, r0, min(n, r0 + rows_per_part),
-                    partial + (long long)blockIdx.x * RP * RQ, gsm_d);
+  double* out = partial + (long long)blockIdx.x * RP * RQ;
+  if constexpr (std::is_same<T, float>::value) {
+    if (gram_tf32_rects(A.total(), B.total()) <= (int)(blockDim.x >> 5)) {
+      gram_core_tf32(A, B, r0, min(n, r0 + rows_per_part), out, gsm_d);
+      return;
+    }
+  }
+  gram_core<MR, MC>(A, B, r0, min(n, r0 + rows_per_part), out, gsm_d);
 }
 
 // Stage 1: column-block sums of the partial C' slices (coalesced over the RP x RQ elements);
@@ -228,6 +234,10 @@ int launch_gram(const BlockList<T>& A, const BlockList<T>& B, long long n,
   }
   int MR, MC, threads;
   gram_shape(P, Q, MR, MC, threads);
+  if (std::is_same<T, float>::value) {   // the TF32 core wants one warp per tile rectangle
+    const int G = gram_tf32_rects(P, Q);
+    if (G > threads / 32 && G <= 16) threads = 512;
+  }
   double* pd = reinterpret_cast<double*>(partial);
   const unsigned grid = (unsigned)parts;
   if (MR == 3 && MC == 3) gram_partial_kernel<3, 3, T><<<grid, threads, smem, st>>>(A, B, n, rpp, pd);
@@ -257,10 +267,14 @@ update_kernel(const BlockList<T> A, const CoefList C, int q, long long n, cplx<T
               long long ldy, int accumulate) {
   extern __shared__ __align__(16) unsigned char usm[];
   const double2* Cf[3] = {C.c[0], C.c[1], C.c[2]};
-  const long long per = ((n + gridDim.x - 1) / gridDim.x + kUpdChunk - 1) / kUpdChunk * kUpdChunk;
+  constexpr int chunk = std::is_same<T, float>::value ? kTfUpdChunk : kUpdChunk;
+  const long long per = ((n + gridDim.x - 1) / gridDim.x + chunk - 1) / chunk * chunk;
   const long long r0 = (long long)blockIdx.x * per;
   if (r0 >= n) return;
-  update_rows(A, Cf, q, r0, min(n, r0 + per), Y, ldy, accumulate, 0, usm);
+  if constexpr (std::is_same<T, float>::value)
+    update_rows_tf32(A, Cf, q, r0, min(n, r0 + per), Y, ldy, accumulate, 0, usm);
+  else
+    update_rows(A, Cf, q, r0, min(n, r0 + per), Y, ldy, accumulate, 0, usm);
 }
 
 template <typename T>
@@ -270,7 +284,8 @@ int launch_update(const BlockList<T>& A, const double2* const* C, int q, long lo
   CoefList cl;
   for (int b = 0; b < 3; ++b) cl.c[b] = b < A.nblk ? C[b] : nullptr;
   const int P = A.total();
-  const size_t smem = update_smem_bytes(P, q, (int)sizeof(cplx<T>));
+  const size_t smem = std::is_same<T, float>::value ? update_tf32_smem_bytes(P, q)
+                                                    : update_smem_bytes(P, q, (int)sizeof(cplx<T>));
   static bool attr = false;
   if (!attr) {
     QDKP_CUDA_TRY(cudaFuncSetAttribute(update_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -362,3 +377,82 @@ template int launch_copy<float, double>(const float2*, long long, int, long long
                                         long long, cudaStream_t);
 
 }  // namespace qdkp
+
+using namespace qdkp;
+
+extern "C" {
+
+size_t qdkp_block_gram_workspace_size(int P, int Q) {
+  if (P < 1 || Q < 1 || P > kMaxSmall || Q > kMaxSmall) return 0;
+  return gram_partial_elems(P, Q) * sizeof(double2) + (size_t)P * Q * sizeof(double2) + 256;
+}
+
+int qdkp_block_gram(const void* A, int64_t lda, int P, const void* B, int64_t ldb, int Q,
+                    int64_t n, int precision, double* out, void* ws, size_t ws_bytes,
+                    void* stream) {
+  QDKP_CHECK_ARG(A && B && out && ws, "NULL argument");
+  QDKP_CHECK_ARG(P >= 1 && Q >= 1 && P <= kMaxSmall && Q <= kMaxSmall && n >= 1 && lda >= P &&
+                 ldb >= Q, "bad block shapes");
+  QDKP_CHECK_ARG(precision == QDKP_C128 || precision == QDKP_C64, "bad precision");
+  if (ws_bytes < qdkp_block_gram_workspace_size(P, Q)) {
+    set_error("qdkp_block_gram: workspace too small");
+    return QDKP_ERR_WORKSPACE;
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const size_t pe = gram_partial_elems(P, Q);
+  double2* part = static_cast<double2*>(ws);
+  double2* dout = part + pe;
+  int rc;
+  if (precision == QDKP_C64) {
+    BlockList<float> La, Lb;
+    La.nblk = 1; La.p[0] = static_cast<const float2*>(A); La.ld[0] = lda; La.cols[0] = P;
+    Lb.nblk = 1; Lb.p[0] = static_cast<const float2*>(B); Lb.ld[0] = ldb; Lb.cols[0] = Q;
+    rc = launch_gram(La, Lb, n, part, pe, dout, st);
+  } else {
+    BlockList<double> La, Lb;
+    La.nblk = 1; La.p[0] = static_cast<const double2*>(A); La.ld[0] = lda; La.cols[0] = P;
+    Lb.nblk = 1; Lb.p[0] = static_cast<const double2*>(B); Lb.ld[0] = ldb; Lb.cols[0] = Q;
+    rc = launch_gram(La, Lb, n, part, pe, dout, st);
+  }
+  if (rc != QDKP_OK) return rc;
+  QDKP_CUDA_TRY(cudaMemcpyAsync(out, dout, (size_t)P * Q * sizeof(double2), cudaMemcpyDeviceToHost, st));
+  QDKP_CUDA_TRY(cudaStreamSynchronize(st));
+  return QDKP_OK;
+}
+
+size_t qdkp_block_update_workspace_size(int P, int q) {
+  if (P < 1 || q < 1 || P > kMaxSmall || q > kMaxBlock) return 0;
+  return (size_t)P * q * sizeof(double2) + 256;
+}
+
+int qdkp_block_update(const void* A, int64_t lda, int P, const double* C, int q, int64_t n,
+                      void* Y, int64_t ldy, int precision, void* ws, size_t ws_bytes,
+                      void* stream) {
+  QDKP_CHECK_ARG(A && C && Y && ws, "NULL argument");
+  QDKP_CHECK_ARG(P >= 1 && q >= 1 && P <= kMaxSmall && q <= kMaxBlock && n >= 1 && lda >= P &&
+                 ldy >= q, "bad block shapes");
+  QDKP_CHECK_ARG(precision == QDKP_C128 || precision == QDKP_C64, "bad precision");
+  if (ws_bytes < qdkp_block_update_workspace_size(P, q)) {
+    set_error("qdkp_block_update: workspace too small");
+    return QDKP_ERR_WORKSPACE;
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  double2* dC = static_cast<double2*>(ws);
+  QDKP_CUDA_TRY(cudaMemcpyAsync(dC, C, (size_t)P * q * sizeof(double2), cudaMemcpyHostToDevice, st));
+  const double2* Cs[1] = {dC};
+  int rc;
+  if (precision == QDKP_C64) {
+    BlockList<float> La;
+    La.nblk = 1; La.p[0] = static_cast<const float2*>(A); La.ld[0] = lda; La.cols[0] = P;
+    rc = launch_update(La, Cs, q, n, static_cast<float2*>(Y), ldy, 0, st);
+  } else {
+    BlockList<double> La;
+    La.nblk = 1; La.p[0] = static_cast<const double2*>(A); La.ld[0] = lda; La.cols[0] = P;
+    rc = launch_update(La, Cs, q, n, static_cast<double2*>(Y), ldy, 0, st);
+  }
+  if (rc != QDKP_OK) return rc;
+  QDKP_CUDA_TRY(cudaStreamSynchronize(st));
+  return QDKP_OK;
+}
+
+}  // extern "C"

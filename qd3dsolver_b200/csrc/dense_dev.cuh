@@ -11,6 +11,39 @@ static __device__ __forceinline__ void dmma(double& d0, double& d1, double a, do
 }
 
 
+constexpr int kStageBudget = 64 * 1024;    // shared memory for the row stages of one CTA
+
+// Stages in flight: as many (2..4) as fit the budget, so that a CTA keeps several chunk loads
+// outstanding while it works on one (the kernels are latency- or bandwidth-bound otherwise).
+__host__ __device__ __forceinline__ int stage_count(size_t stage_bytes) {
+  const int ns = (int)(kStageBudget / stage_bytes);
+  return ns < 2 ? 2 : (ns > 4 ? 4 : ns);
+}
+
+// Dynamic shared memory this launch was given (the %dynamic_smem_size special register). The
+// staged kernels fit their stage count and chunk size into it, so a product narrower than the
+// one the launch was sized for can never over-run its allocation.
+__device__ __forceinline__ unsigned dyn_smem_bytes() {
+  unsigned r;
+  asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(r));
+  return r;
+}
+
+// Stages (2..4) of `stage_bytes` that fit both the budget and `avail` bytes.
+__device__ __forceinline__ int stage_count_fit(size_t stage_bytes, size_t avail) {
+  int ns = stage_count(stage_bytes);
+  while (ns > 2 && (size_t)ns * stage_bytes > avail) --ns;
+  return ns;
+}
+
+// cp.async.wait_group takes an immediate: wait until at most n (0..3) groups are pending
+__device__ __forceinline__ void cp_async_wait_pending(int n) {
+  if (n >= 3) asm volatile("cp.async.wait_group 3;\n" ::: "memory");
+  else if (n == 2) asm volatile("cp.async.wait_group 2;\n" ::: "memory");
+  else if (n == 1) asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+  else asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
 template <typename T>
 static __device__ __forceinline__ double2 list_elem(const BlockList<T>& L, long long r, int c) {
   int b = 0;
@@ -273,10 +306,6 @@ constexpr int kUpdThreads = 256;
 constexpr int kUpdWarps = kUpdThreads / 32;
 constexpr int kUpdChunk = kUpdRows * kUpdWarps;     // 64 rows per stage
 
-__host__ __device__ __forceinline__ size_t update_smem_bytes(int P, int q, int elem_bytes) {
-  const size_t KPp = (2 * P + 3) / 4 * 4 + 4, NQ = (2 * q + 7) / 8 * 8;
-  return KPp * NQ * sizeof(double) + 2 * (size_t)kUpdChunk * P * elem_bytes;
-}
 
 template <typename T>
 static __device__ void update_rows(const BlockList<T>& A, const double2* const* C, int q,
@@ -288,7 +317,9 @@ static __device__ void update_rows(const BlockList<T>& A, const double2* const* 
   const int NQ = (2 * q + 7) / 8 * 8;
   double* sC = reinterpret_cast<double*>(smem);
   cplx<T>* stage0 = reinterpret_cast<cplx<T>*>(smem + (size_t)(KPp + 4) * NQ * sizeof(double));
-  cplx<T>* stage[2] = {stage0, stage0 + (size_t)kUpdChunk * P};
+  const size_t stage_elems = (size_t)kUpdChunk * P;
+  const int NS = stage_count_fit(stage_elems * sizeof(cplx<T>),
+                                 dyn_smem_bytes() - (size_t)(KPp + 4) * NQ * sizeof(double));
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const double sg = neg ? -1.0 : 1.0;
   int off[3], kst[3];
@@ -330,21 +361,23 @@ static __device__ void update_rows(const BlockList<T>& A, const double2* const* 
       }
     }
   };
-  if (nchunks > 0) stage_rows(r0, (int)min((long long)kUpdChunk, nrows), stage[0]);
-  asm volatile("cp.async.commit_group;\n" ::: "memory");
+  auto issue = [&](int c) {
+    if (c < nchunks) {
+      const long long rn = r0 + (long long)c * kUpdChunk;
+      stage_rows(rn, (int)min((long long)kUpdChunk, r1 - rn), stage0 + (size_t)(c % NS) * stage_elems);
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  };
+  for (int c = 0; c < NS - 1; ++c) issue(c);
   for (int ch = 0; ch < nchunks; ++ch) {
     const long long rc = r0 + (long long)ch * kUpdChunk;
     const int rows = (int)min((long long)kUpdChunk, r1 - rc);
-    if (ch + 1 < nchunks) {
-      const long long rn = rc + kUpdChunk;
-      stage_rows(rn, (int)min((long long)kUpdChunk, r1 - rn), stage[(ch + 1) & 1]);
-    }
-    asm volatile("cp.async.commit_group;\n" ::: "memory");
-    asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+    issue(ch + NS - 1);
+    cp_async_wait_pending(NS - 1);
     __syncthreads();
     const int tr = warp * kUpdRows;             // this warp's 8-row tile in the chunk
     if (tr < rows) {
-      const T* sr = reinterpret_cast<const T*>(stage[ch & 1]);
+      const T* sr = reinterpret_cast<const T*>(stage0 + (size_t)(ch % NS) * stage_elems);
       const int row = tr + g;
       const bool rok = row < rows;
       const long long rowg = rc + row;
@@ -394,25 +427,39 @@ static __device__ void update_rows(const BlockList<T>& A, const double2* const* 
 // are staged as they are and widened to FP64 in the fragment loads.
 // ---------------------------------------------------------------------------------------------
 constexpr int kGramCtaThreads = 256;
-constexpr int kGramRows = 32;       // rows per shared-memory chunk (a multiple of 4)
+constexpr int kGramRows = 32;       // fewest rows per shared-memory chunk (a multiple of 8)
+constexpr int kGramStageTarget = 24 * 1024;   // bytes a chunk brings in per barrier
+
+// Rows per chunk: about kGramStageTarget bytes of the two lists, a multiple of 8 in
+// [kGramRows, 512], so that narrow products still move many rows per CTA barrier.
+__host__ __device__ __forceinline__ int gram_chunk_rows(int P, int Q, int elem_bytes) {
+  int r = kGramStageTarget / ((P + Q) * elem_bytes);
+  r = r / 8 * 8;
+  return r < kGramRows ? kGramRows : (r > 512 ? 512 : r);
+}
+__host__ __device__ __forceinline__ size_t update_smem_bytes(int P, int q, int elem_bytes) {
+  const size_t KPp = (2 * P + 3) / 4 * 4 + 4, NQ = (2 * q + 7) / 8 * 8;
+  const size_t stage = (size_t)kUpdChunk * P * elem_bytes;
+  return KPp * NQ * sizeof(double) + stage_count(stage) * stage;
+}
 
 __host__ __device__ __forceinline__ size_t gram_smem_bytes(int P, int Q, int elem_bytes) {
   const size_t RP = (2 * P + 7) / 8 * 8, RQ = (2 * Q + 7) / 8 * 8;
-  const size_t stage = (size_t)kGramRows * (P + Q) * 2 * elem_bytes;
+  const size_t stage = (size_t)gram_chunk_rows(P, Q, elem_bytes) * (P + Q) * elem_bytes;
   const size_t red = RP * RQ * sizeof(double);
-  const size_t st2 = 2 * stage;
-  return st2 > red ? st2 : red;
+  const size_t st = stage_count(stage) * stage;
+  return st > red ? st : red;
 }
 
 template <typename T>
 __device__ __forceinline__ void gram_copy_rows(const BlockList<T>& L, long long r, int nrows,
-                                               cplx<T>* dst) {
+                                               cplx<T>* dst, int crow) {
   int off = 0;
   for (int b = 0; b < L.nblk; ++b) {
     const int cols = L.cols[b];
     const int units = nrows * cols;
     const cplx<T>* src = L.p[b] + r * L.ld[b];
-    cplx<T>* d = dst + (long long)off * kGramRows;
+    cplx<T>* d = dst + (long long)off * crow;
     if (L.ld[b] == cols) {
       for (int u = threadIdx.x; u < units; u += blockDim.x) {
         const unsigned sa = (unsigned)__cvta_generic_to_shared(d + u);
@@ -453,12 +500,18 @@ static __device__ void gram_core(const BlockList<T>& A, const BlockList<T>& B,
   const int rect = warp % G, slice = warp / G;
   const bool active_warp = slice < slices;
   const int tr0 = (rect / GC) * MR, tc0 = (rect % GC) * MC;
-  // stage layout: per list, per block, kGramRows x cols complex values; A's blocks first
-  cplx<T>* stage[2];
-  stage[0] = reinterpret_cast<cplx<T>*>(smem);
-  stage[1] = stage[0] + (size_t)kGramRows * (P + Q);
+  // stage layout: per list, per block, crow x cols complex values; A's blocks first
+  const unsigned avail = dyn_smem_bytes();
+  int crow = gram_chunk_rows(P, Q, (int)sizeof(cplx<T>));
+  {   // two stages must fit the launch's shared memory
+    const int fit = (int)(avail / (2 * (size_t)(P + Q) * sizeof(cplx<T>))) / 8 * 8;
+    if (crow > fit) crow = fit;
+  }
+  const size_t stage_elems = (size_t)crow * (P + Q);
+  const int NS = stage_count_fit(stage_elems * sizeof(cplx<T>), avail);
+  cplx<T>* stage0 = reinterpret_cast<cplx<T>*>(smem);
   // per tile: the real offset of its column inside a staged row block (-1: outside P / Q)
-  // as (block start in complex columns * kGramRows, block width, real column in the row)
+  // as (block start in complex columns * crow, block width, real column in the row)
   int sa_off[MR], sa_w[MR], sa_c[MR], sb_off[MC], sb_w[MC], sb_c[MC];
 #pragma unroll
   for (int i = 0; i < MR; ++i) {
@@ -466,7 +519,7 @@ static __device__ void gram_core(const BlockList<T>& A, const BlockList<T>& B,
     int c = col >> 1, blk = 0, start = 0;
     while (blk < A.nblk - 1 && c >= A.cols[blk]) { c -= A.cols[blk]; start += A.cols[blk]; ++blk; }
     const bool ok = active_warp && tr0 + i < TR && col < 2 * P;
-    sa_off[i] = ok ? start * kGramRows : -1;
+    sa_off[i] = ok ? start * crow : -1;
     sa_w[i] = A.cols[blk];
     sa_c[i] = 2 * c + (col & 1);
   }
@@ -476,7 +529,7 @@ static __device__ void gram_core(const BlockList<T>& A, const BlockList<T>& B,
     int c = col >> 1, blk = 0, start = 0;
     while (blk < B.nblk - 1 && c >= B.cols[blk]) { c -= B.cols[blk]; start += B.cols[blk]; ++blk; }
     const bool ok = active_warp && tc0 + j < TC && col < 2 * Q;
-    sb_off[j] = ok ? (P + start) * kGramRows : -1;
+    sb_off[j] = ok ? (P + start) * crow : -1;
     sb_w[j] = B.cols[blk];
     sb_c[j] = 2 * c + (col & 1);
   }
@@ -487,27 +540,26 @@ static __device__ void gram_core(const BlockList<T>& A, const BlockList<T>& B,
     for (int j = 0; j < MC; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
 
   const long long nrows = r1 - r0;
-  const int nchunks = (int)((nrows + kGramRows - 1) / kGramRows);
-  if (nchunks > 0) {
-    const int n0 = (int)min((long long)kGramRows, nrows);
-    gram_copy_rows(A, r0, n0, stage[0]);
-    gram_copy_rows(B, r0, n0, stage[0] + (size_t)P * kGramRows);
-  }
-  asm volatile("cp.async.commit_group;\n" ::: "memory");
-  for (int ch = 0; ch < nchunks; ++ch) {
-    const long long rc = r0 + (long long)ch * kGramRows;
-    const int rows = (int)min((long long)kGramRows, r1 - rc);
-    if (ch + 1 < nchunks) {
-      const long long rn = rc + kGramRows;
-      const int nn = (int)min((long long)kGramRows, r1 - rn);
-      cplx<T>* st = stage[(ch + 1) & 1];
-      gram_copy_rows(A, rn, nn, st);
-      gram_copy_rows(B, rn, nn, st + (size_t)P * kGramRows);
+  const int nchunks = (int)((nrows + crow - 1) / crow);
+  // chunk c lives in stage c % NS; NS - 1 chunks are in flight while one is consumed
+  auto issue = [&](int c) {
+    if (c < nchunks) {
+      const long long rn = r0 + (long long)c * crow;
+      const int nn = (int)min((long long)crow, r1 - rn);
+      cplx<T>* st = stage0 + (size_t)(c % NS) * stage_elems;
+      gram_copy_rows(A, rn, nn, st, crow);
+      gram_copy_rows(B, rn, nn, st + (size_t)P * crow, crow);
     }
     asm volatile("cp.async.commit_group;\n" ::: "memory");
-    asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+  };
+  for (int c = 0; c < NS - 1; ++c) issue(c);
+  for (int ch = 0; ch < nchunks; ++ch) {
+    const long long rc = r0 + (long long)ch * crow;
+    const int rows = (int)min((long long)crow, r1 - rc);
+    issue(ch + NS - 1);
+    cp_async_wait_pending(NS - 1);
     __syncthreads();
-    const T* sr = reinterpret_cast<const T*>(stage[ch & 1]);
+    const T* sr = reinterpret_cast<const T*>(stage0 + (size_t)(ch % NS) * stage_elems);
     if (active_warp) {
       for (int k0 = 4 * slice; k0 < rows; k0 += 4 * slices) {
         const int row = k0 + t4;
@@ -552,6 +604,320 @@ static __device__ void gram_core(const BlockList<T>& A, const BlockList<T>& B,
     __syncthreads();
   }
   for (int e = threadIdx.x; e < RP * RQ; e += blockDim.x) out[e] = gsm[e];
+}
+
+// ---------------------------------------------------------------------------------------------
+// complex64 blocks: split-precision TF32 tensor-core products (mma.sync.m16n8k8 .tf32, FP32
+// accumulation). Every FP32 value x is split into x = hi + lo with hi, lo TF32 (10-bit
+// mantissas; cvt.rna), and a product is formed as lo*hi + hi*lo + hi*hi (the lo*lo term is below
+// FP32 rounding), which keeps the FP32 accuracy of the inputs. A CTA accumulates its rows in
+// FP32 registers and writes an FP64 partial; partials are summed in FP64.
+// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ unsigned tf32_round(float x) {
+  unsigned r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ void tf32_split(float x, unsigned& hi, unsigned& lo) {
+  hi = tf32_round(x);
+  lo = tf32_round(x - __uint_as_float(hi));
+}
+__device__ __forceinline__ void mma_tf32(float (&d)[4], unsigned a0, unsigned a1, unsigned a2,
+                                         unsigned a3, unsigned b0, unsigned b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+      "{%8,%9}, {%0,%1,%2,%3};"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+// d += (ahi + alo)(bhi + blo) without the lo * lo term
+__device__ __forceinline__ void mma_tf32x3(float (&d)[4], const unsigned (&ah)[4],
+                                           const unsigned (&al)[4], const unsigned (&bh)[2],
+                                           const unsigned (&bl)[2]) {
+  mma_tf32(d, al[0], al[1], al[2], al[3], bh[0], bh[1]);
+  mma_tf32(d, ah[0], ah[1], ah[2], ah[3], bl[0], bl[1]);
+  mma_tf32(d, ah[0], ah[1], ah[2], ah[3], bh[0], bh[1]);
+}
+
+// Gram partial C' = A'^T B' over rows [r0, r1) of complex64 lists (same staging and output as
+// gram_core). MMA tiles: 16 columns of A' (M) x 8 columns of B' (N) x 8 rows (K); a warp owns a
+// rectangle of kTfMR x kTfMC tiles and a slice of the chunk's 8-row k steps.
+// Fragments (m16n8k8 tf32; g = lane / 4, t = lane % 4): A_mma[m][k] = A'[k][m]:
+// a0 = (k t, m g), a1 = (k t, m g + 8), a2 = (k t + 4, m g), a3 = (k t + 4, m g + 8);
+// B_mma[k][n] = B'[k][n]: b0 = (k t, n g), b1 = (k t + 4, n g); D: (m g, n 2t), (m g, n 2t + 1),
+// (m g + 8, n 2t), (m g + 8, n 2t + 1).
+constexpr int kTfMR = 3, kTfMC = 3;
+
+__host__ __device__ __forceinline__ int gram_tf32_rects(int P, int Q) {
+  const int TR = (2 * P + 15) / 16, TC = (2 * Q + 7) / 8;
+  return ((TR + kTfMR - 1) / kTfMR) * ((TC + kTfMC - 1) / kTfMC);
+}
+
+static __device__ void gram_core_tf32(const BlockList<float>& A, const BlockList<float>& B,
+                                      long long r0, long long r1, double* __restrict__ out,
+                                      unsigned char* smem) {
+  const int P = A.total(), Q = B.total();
+  const int RP = (2 * P + 7) / 8 * 8, RQ = (2 * Q + 7) / 8 * 8;   // partial layout (as FP64 core)
+  const int TR = (2 * P + 15) / 16, TC = (2 * Q + 7) / 8;
+  const int GC = (TC + kTfMC - 1) / kTfMC;
+  const int G = gram_tf32_rects(P, Q);
+  const int nwarps = blockDim.x >> 5;
+  const int slices = nwarps / G;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = lane >> 2, t = lane & 3;
+  const int rect = warp % G, slice = warp / G;
+  const bool active_warp = slice < slices;
+  const int tr0 = (rect / GC) * kTfMR, tc0 = (rect % GC) * kTfMC;
+  const unsigned avail = dyn_smem_bytes();
+  int crow = gram_chunk_rows(P, Q, (int)sizeof(float2));
+  {
+    const int fit = (int)(avail / (2 * (size_t)(P + Q) * sizeof(float2))) / 8 * 8;
+    if (crow > fit) crow = fit;
+  }
+  const size_t stage_elems = (size_t)crow * (P + Q);
+  const int NS = stage_count_fit(stage_elems * sizeof(float2), avail);
+  float2* stage0 = reinterpret_cast<float2*>(smem);
+  // staged real offset of a real column of A' (two per M tile: m g, m g + 8) and of B' (n g)
+  int ao[kTfMR][2], aw[kTfMR][2], bo[kTfMC], bw[kTfMC];
+#pragma unroll
+  for (int i = 0; i < kTfMR; ++i)
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int col = (tr0 + i) * 16 + g + 8 * h;
+      int c = col >> 1, blk = 0, start = 0;
+      while (blk < A.nblk - 1 && c >= A.cols[blk]) { c -= A.cols[blk]; start += A.cols[blk]; ++blk; }
+      const bool ok = active_warp && tr0 + i < TR && col < 2 * P;
+      ao[i][h] = ok ? 2 * start * crow + 2 * c + (col & 1) : -1;
+      aw[i][h] = 2 * A.cols[blk];
+    }
+#pragma unroll
+  for (int j = 0; j < kTfMC; ++j) {
+    const int col = (tc0 + j) * 8 + g;
+    int c = col >> 1, blk = 0, start = 0;
+    while (blk < B.nblk - 1 && c >= B.cols[blk]) { c -= B.cols[blk]; start += B.cols[blk]; ++blk; }
+    const bool ok = active_warp && tc0 + j < TC && col < 2 * Q;
+    bo[j] = ok ? 2 * (P + start) * crow + 2 * c + (col & 1) : -1;
+    bw[j] = 2 * B.cols[blk];
+  }
+  float acc[kTfMR][kTfMC][4];
+#pragma unroll
+  for (int i = 0; i < kTfMR; ++i)
+#pragma unroll
+    for (int j = 0; j < kTfMC; ++j)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.f;
+
+  const long long nrows = r1 - r0;
+  const int nchunks = (int)((nrows + crow - 1) / crow);
+  auto issue = [&](int c) {
+    if (c < nchunks) {
+      const long long rn = r0 + (long long)c * crow;
+      const int nn = (int)min((long long)crow, r1 - rn);
+      float2* st = stage0 + (size_t)(c % NS) * stage_elems;
+      gram_copy_rows(A, rn, nn, st, crow);
+      gram_copy_rows(B, rn, nn, st + (size_t)P * crow, crow);
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  };
+  for (int c = 0; c < NS - 1; ++c) issue(c);
+  for (int ch = 0; ch < nchunks; ++ch) {
+    const long long rc = r0 + (long long)ch * crow;
+    const int rows = (int)min((long long)crow, r1 - rc);
+    issue(ch + NS - 1);
+    cp_async_wait_pending(NS - 1);
+    __syncthreads();
+    const float* sr = reinterpret_cast<const float*>(stage0 + (size_t)(ch % NS) * stage_elems);
+    if (active_warp) {
+      for (int k0 = 8 * slice; k0 < rows; k0 += 8 * slices) {
+        const int ra = k0 + t, rb = k0 + t + 4;      // the two rows of this lane's fragments
+        const bool oka = ra < rows, okb = rb < rows;
+        unsigned bh[kTfMC][2], bl[kTfMC][2];
+#pragma unroll
+        for (int j = 0; j < kTfMC; ++j) {
+          const float x0 = (oka && bo[j] >= 0) ? sr[bo[j] + ra * bw[j]] : 0.f;
+          const float x1 = (okb && bo[j] >= 0) ? sr[bo[j] + rb * bw[j]] : 0.f;
+          tf32_split(x0, bh[j][0], bl[j][0]);
+          tf32_split(x1, bh[j][1], bl[j][1]);
+        }
+#pragma unroll
+        for (int i = 0; i < kTfMR; ++i) {
+          const float v0 = (oka && ao[i][0] >= 0) ? sr[ao[i][0] + ra * aw[i][0]] : 0.f;
+          const float v1 = (oka && ao[i][1] >= 0) ? sr[ao[i][1] + ra * aw[i][1]] : 0.f;
+          const float v2 = (okb && ao[i][0] >= 0) ? sr[ao[i][0] + rb * aw[i][0]] : 0.f;
+          const float v3 = (okb && ao[i][1] >= 0) ? sr[ao[i][1] + rb * aw[i][1]] : 0.f;
+          unsigned ah[4], al[4];
+          tf32_split(v0, ah[0], al[0]);
+          tf32_split(v1, ah[1], al[1]);
+          tf32_split(v2, ah[2], al[2]);
+          tf32_split(v3, ah[3], al[3]);
+#pragma unroll
+          for (int j = 0; j < kTfMC; ++j) mma_tf32x3(acc[i][j], ah, al, bh[j], bl[j]);
+        }
+      }
+    }
+    __syncthreads();
+  }
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+  __syncthreads();
+  double* gsm = reinterpret_cast<double*>(smem);
+  for (int e = threadIdx.x; e < RP * RQ; e += blockDim.x) gsm[e] = 0.0;
+  __syncthreads();
+  for (int sl = 0; sl < slices; ++sl) {
+    if (active_warp && slice == sl) {
+#pragma unroll
+      for (int i = 0; i < kTfMR; ++i)
+#pragma unroll
+        for (int j = 0; j < kTfMC; ++j) {
+          const int ti = tr0 + i, tj = tc0 + j;
+          if (ti < TR && tj < TC) {
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+              const int rr = ti * 16 + g + 8 * h, cc = tj * 8 + 2 * t;
+              if (rr < RP && cc < RQ) {
+                gsm[rr * RQ + cc] += (double)acc[i][j][2 * h];
+                gsm[rr * RQ + cc + 1] += (double)acc[i][j][2 * h + 1];
+              }
+            }
+          }
+        }
+    }
+    __syncthreads();
+  }
+  for (int e = threadIdx.x; e < RP * RQ; e += blockDim.x) out[e] = gsm[e];
+}
+
+// Y' = A' C'' for rows [r0, r1) of complex64 blocks on TF32 tensor cores (split as above; same
+// staging as update_rows with kTfUpdChunk rows per stage, one 16-row M tile per warp). Fragments:
+// A_mma[m][k] = A'[row m][k]: a0 = (m g, k t), a1 = (m g + 8, k t), a2 = (m g, k t + 4),
+// a3 = (m g + 8, k t + 4); B_mma[k][n] = C''[k][n]: b0 = (k t, n g), b1 = (k t + 4, n g);
+// D (m g, n 2t .. 2t + 1) is one complex output, (m g + 8, ...) another.
+constexpr int kTfUpdChunk = 16 * kUpdWarps;     // 128 rows per stage
+
+__host__ __device__ __forceinline__ size_t update_tf32_smem_bytes(int P, int q) {
+  const size_t KP8 = (2 * P + 7) / 8 * 8 + 8, NQ = (2 * q + 7) / 8 * 8;
+  const size_t stage = (size_t)kTfUpdChunk * P * sizeof(float2);
+  return 2 * KP8 * NQ * sizeof(unsigned) + stage_count(stage) * stage;
+}
+
+static __device__ void update_rows_tf32(const BlockList<float>& A, const double2* const* C, int q,
+                                        long long r0, long long r1, float2* Y, long long ldy,
+                                        int accumulate, int neg, unsigned char* smem) {
+  const int P = A.total();
+  const int KP = 2 * P;
+  const int KP8 = (KP + 7) / 8 * 8 + 8;
+  const int NQ = (2 * q + 7) / 8 * 8;
+  unsigned* sCh = reinterpret_cast<unsigned*>(smem);        // C'' hi, KP8 x NQ
+  unsigned* sCl = sCh + (size_t)KP8 * NQ;                   // C'' lo
+  float2* stage0 = reinterpret_cast<float2*>(sCl + (size_t)KP8 * NQ);
+  const size_t stage_elems = (size_t)kTfUpdChunk * P;
+  const int NS = stage_count_fit(stage_elems * sizeof(float2),
+                                 dyn_smem_bytes() - 2 * (size_t)KP8 * NQ * sizeof(unsigned));
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const double sg = neg ? -1.0 : 1.0;
+  int off[3], kst[3];
+  int tot = 0;
+  for (int b = 0; b < A.nblk; ++b) { off[b] = tot; tot += A.cols[b]; }
+  for (int e = threadIdx.x; e < KP8 * NQ; e += blockDim.x) { sCh[e] = 0u; sCl[e] = 0u; }
+  __syncthreads();
+  for (int e = threadIdx.x; e < P * q; e += blockDim.x) {
+    const int i = e / q, j = e - i * q;
+    int b = 0;
+    while (b < A.nblk - 1 && i >= off[b] + A.cols[b]) ++b;
+    const double2 c = C[b][(i - off[b]) * q + j];
+    const float v[4] = {(float)(sg * c.x), (float)(sg * c.y), (float)(-sg * c.y), (float)(sg * c.x)};
+    const int idx[4] = {(2 * i) * NQ + 2 * j, (2 * i) * NQ + 2 * j + 1, (2 * i + 1) * NQ + 2 * j,
+                        (2 * i + 1) * NQ + 2 * j + 1};
+#pragma unroll
+    for (int u = 0; u < 4; ++u) tf32_split(v[u], sCh[idx[u]], sCl[idx[u]]);
+  }
+  for (int b = 0; b < A.nblk; ++b) kst[b] = off[b] * kTfUpdChunk;
+  const int g = lane >> 2, t = lane & 3;
+  const int NT = NQ / 8;
+  const long long nrows = r1 - r0;
+  const int nchunks = (int)((nrows + kTfUpdChunk - 1) / kTfUpdChunk);
+  auto stage_rows = [&](long long r, int nr, float2* dst) {
+    for (int b = 0; b < A.nblk; ++b) {
+      const int cols = A.cols[b];
+      const int units = nr * cols;
+      const float2* src = A.p[b] + r * A.ld[b];
+      float2* d = dst + kst[b];
+      for (int u = threadIdx.x; u < units; u += blockDim.x) {
+        const int rr = A.ld[b] == cols ? 0 : u / cols;
+        const float2* gp = A.ld[b] == cols ? src + u : src + (long long)rr * A.ld[b] + (u - rr * cols);
+        const unsigned sa = (unsigned)__cvta_generic_to_shared(d + u);
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" :: "r"(sa), "l"(gp) : "memory");
+      }
+    }
+  };
+  auto issue = [&](int c) {
+    if (c < nchunks) {
+      const long long rn = r0 + (long long)c * kTfUpdChunk;
+      stage_rows(rn, (int)min((long long)kTfUpdChunk, r1 - rn), stage0 + (size_t)(c % NS) * stage_elems);
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  };
+  for (int c = 0; c < NS - 1; ++c) issue(c);
+  for (int ch = 0; ch < nchunks; ++ch) {
+    const long long rc = r0 + (long long)ch * kTfUpdChunk;
+    const int rows = (int)min((long long)kTfUpdChunk, r1 - rc);
+    issue(ch + NS - 1);
+    cp_async_wait_pending(NS - 1);
+    __syncthreads();
+    const int tr = warp * 16;                    // this warp's 16-row M tile in the chunk
+    if (tr < rows) {
+      const float* sr = reinterpret_cast<const float*>(stage0 + (size_t)(ch % NS) * stage_elems);
+      const int ra = tr + g, rb = tr + g + 8;
+      const bool oka = ra < rows, okb = rb < rows;
+      float acc[6][4];
+#pragma unroll
+      for (int j = 0; j < 6; ++j) {
+        const int col = j * 4 + t;
+        float2 ya = make_float2(0.f, 0.f), yb = make_float2(0.f, 0.f);
+        if (accumulate && j < NT && col < q) {
+          if (oka) ya = Y[(rc + ra) * ldy + col];
+          if (okb) yb = Y[(rc + rb) * ldy + col];
+        }
+        acc[j][0] = ya.x; acc[j][1] = ya.y; acc[j][2] = yb.x; acc[j][3] = yb.y;
+      }
+      int kbase = 0;
+      for (int b = 0; b < A.nblk; ++b) {
+        const int kb = 2 * A.cols[b];
+        const float* rsa = sr + 2 * kst[b] + (oka ? ra : 0) * kb;
+        const float* rsb = sr + 2 * kst[b] + (okb ? rb : 0) * kb;
+        for (int k = 0; k < kb; k += 8) {
+          const float v0 = (oka && k + t < kb) ? rsa[k + t] : 0.f;
+          const float v1 = (okb && k + t < kb) ? rsb[k + t] : 0.f;
+          const float v2 = (oka && k + t + 4 < kb) ? rsa[k + t + 4] : 0.f;
+          const float v3 = (okb && k + t + 4 < kb) ? rsb[k + t + 4] : 0.f;
+          unsigned ah[4], al[4];
+          tf32_split(v0, ah[0], al[0]);
+          tf32_split(v1, ah[1], al[1]);
+          tf32_split(v2, ah[2], al[2]);
+          tf32_split(v3, ah[3], al[3]);
+          const int kr = kbase + k;
+#pragma unroll
+          for (int j = 0; j < 6; ++j) {
+            if (j < NT) {
+              const int i0 = (kr + t) * NQ + j * 8 + g, i1 = (kr + t + 4) * NQ + j * 8 + g;
+              const unsigned bh[2] = {sCh[i0], sCh[i1]}, bl[2] = {sCl[i0], sCl[i1]};
+              mma_tf32x3(acc[j], ah, al, bh, bl);
+            }
+          }
+        }
+        kbase += kb;
+      }
+#pragma unroll
+      for (int j = 0; j < 6; ++j) {
+        const int col = j * 4 + t;
+        if (j < NT && col < q) {
+          if (oka) Y[(rc + ra) * ldy + col] = make_float2(acc[j][0], acc[j][1]);
+          if (okb) Y[(rc + rb) * ldy + col] = make_float2(acc[j][2], acc[j][3]);
+        }
+      }
+    }
+    __syncthreads();
+  }
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
 
 // (MR, MC, threads) for a product: the smallest tile rectangles that fit 8 warps, else 16.

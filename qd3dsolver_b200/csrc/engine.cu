@@ -98,6 +98,10 @@ __global__ void e_decide_kernel(const ESlot* __restrict__ S) {
   st->idle = 1; st->copy_best = 0; st->skip_recompute = 1; st->skip_p = 1; st->skip_pnorm = 1;
   if (!st->running) return;
   if (st->iter >= d.maxiter) { st->running = 0; st->status = QDKP_LOBPCG_MAXITER; return; }
+  if (d.stall_iterations > 0 && st->iter - st->best_iter > d.stall_iterations &&
+      st->best_iter <= st->iter) {
+    st->running = 0; st->status = QDKP_LOBPCG_MAXITER; return;
+  }
   st->iter += 1;
   double mean = 0.0, mx = 0.0;
   bool finite = true;
@@ -258,8 +262,10 @@ e_gram_kernel(const ESlot* __restrict__ S, int ns, int which, int m_only) {
     BlockList<float> A, B;
     if (!gram_lists<float>(d, which, A, B, out)) return;
     const int RP = (2 * A.total() + 7) / 8 * 8, RQ = (2 * B.total() + 7) / 8 * 8;
-    gram_core<MR, MC>(A, B, r0, min(d.n, r0 + d.rows_per_gpart),
-                      d.gpart + (long long)part * RP * RQ, gsm_e);
+    // complex64 blocks, FP64 products: the Gram matrices of the search stay exact to FP64
+    // (the split TF32 form loses convergence in the explicit-Gram regime of scipy's method)
+    double* po = d.gpart + (long long)part * RP * RQ;
+    gram_core<MR, MC>(A, B, r0, min(d.n, r0 + d.rows_per_gpart), po, gsm_e);
   } else {
     BlockList<double> A, B;
     if (!gram_lists<double>(d, which, A, B, out)) return;
@@ -355,7 +361,7 @@ e_update_kernel(const ESlot* __restrict__ S, int ns, int which) {
     BlockList<float> A;
     float2* Y;
     if (!upd_lists<float>(d, which, A, Cf, q, Y, accumulate, neg)) return;
-    update_rows(A, Cf, q, r0, r1, Y, (long long)q, accumulate, neg, usm_e);
+    update_rows_tf32(A, Cf, q, r0, r1, Y, (long long)q, accumulate, neg, usm_e);
   } else {
     BlockList<double> A;
     double2* Y;
@@ -698,7 +704,8 @@ int launch_gram_multi(qdkp_engine* e, int which, cudaStream_t st) {
     if (which == GR_BA) { P = 3 * m; Q = 2 * m; }
     else if (which == GR_BB) { P = 2 * m; Q = m; }
     else if (which == GR_WW || which == GR_WAW) { P = 3 * m; Q = 3 * m; }
-    const size_t smem = gram_smem_bytes(P, Q, (int)sizeof(double2));
+    const size_t smem = std::max(gram_smem_bytes(P, Q, (int)sizeof(double2)),
+                                 gram_smem_bytes(P, Q, (int)sizeof(float2)));
     int MR, MC, threads;
     gram_shape(P, Q, MR, MC, threads);
     if (MR == 3 && MC == 3) e_gram_kernel<3, 3><<<e->gram_ctas, threads, smem, st>>>(e->d_slots, e->ns, which, m);
@@ -717,7 +724,8 @@ int launch_gram_multi(qdkp_engine* e, int which, cudaStream_t st) {
 }
 
 int launch_update_multi(qdkp_engine* e, int which, cudaStream_t st) {
-  const size_t smem = update_smem_bytes(2 * e->m_max, e->m_max, (int)sizeof(double2));
+  const size_t smem = std::max(update_smem_bytes(2 * e->m_max, e->m_max, (int)sizeof(double2)),
+                               update_tf32_smem_bytes(2 * e->m_max, e->m_max));
   e_update_kernel<<<e->row_ctas, kUpdThreads, smem, st>>>(e->d_slots, e->ns, which);
   count_launch();
   QDKP_CUDA_TRY(cudaGetLastError());
@@ -928,6 +936,7 @@ int qdkp_engine_admit(qdkp_engine* e, const qdkp_operator* op, const qdkp_lobpcg
                                   : std::sqrt(std::numeric_limits<double>::epsilon());
   d.tol = prm->tol > 0 ? prm->tol : std::sqrt(std::numeric_limits<double>::epsilon()) * (double)n;
   d.maxiter = prm->maxiter;
+  d.stall_iterations = prm->stall_iterations;
   d.restart_control = prm->restart_control > 0 ? prm->restart_control : 20;
   d.nparts = L.nparts; d.gparts = L.gparts; d.rows_per_gpart = L.rows_per_gpart;
   d.rows_per_cta = kERowsPerCta;

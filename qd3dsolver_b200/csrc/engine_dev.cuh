@@ -40,6 +40,7 @@ struct ESlot {
   int folded;
   double tol;
   int maxiter;
+  int stall_iterations;  // > 0: stop once the best mean residual is this many iterations old
   int restart_control;
   double2 *X, *AX, *P, *AP, *best, *Ra, *ARa, *Pa, *APa, *T;
   double2 *W, *G, *U, *gS, *gT, *gA, *gB, *E, *scr, *Cx, *Cr, *Cp, *Im;

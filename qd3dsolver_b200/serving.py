@@ -48,6 +48,7 @@ class Request:
     tag: object = None
     precision: str = 'c128'        # 'c128', or 'mixed' (complex64 search, complex128 finish)
     mixed_tol: float = 1e-4        # residual at which a mixed request leaves complex64
+    mixed_stall: int = 30          # ... or after this many iterations without a new best
     # filled in by the engine
     slot: int = -1
     t_arrive: float = 0.0
@@ -55,7 +56,8 @@ class Request:
     t_done: float = 0.0
     result: dict = field(default=None)
     phase: str = 'c128'            # precision of the slot the request occupies
-    iters_done: int = 0            # iterations of finished phases
+    iters_done: int = 0            # iterations of finished phases (scipy's count)
+    ticks: dict = field(default_factory=dict)   # iterations run per phase
 
     @property
     def block(self):
@@ -97,14 +99,16 @@ class Engine:
 
     def _params(self, r, phase=None):
         phase = phase or ('c64' if r.precision == 'mixed' else 'c128')
+        stall = 0
         if phase == 'c64':
             tol, prec = max(float(r.mixed_tol), float(r.tol or 0.0)), _lib.C64
+            stall = int(r.mixed_stall)
         else:
             tol, prec = (float(r.tol) if r.tol else 0.0), _lib.C128
-        maxiter = max(1, int(r.maxiter) - int(r.iters_done))
+        maxiter = max(1, int(r.maxiter) - int(sum(r.ticks.values())))
         return _lib.LobpcgParams(block=r.block, folded=int(r.folded), sigma=float(r.sigma),
                                  tol=tol, maxiter=maxiter, restart_control=20, precision=prec,
-                                 verbosity=0, time_hx=0)
+                                 verbosity=0, time_hx=0, stall_iterations=stall)
 
     def workspace_bytes(self, r):
         prm = self._params(r)
@@ -152,6 +156,7 @@ class Engine:
         iters = (ctypes.c_int * self.max_slots)()
         check(lib().qdkp_engine_poll(self._h, state, status, iters, self.stream),
               'qdkp_engine_poll')
+        self._iters = list(iters)
         return list(state), list(status), list(iters)
 
     def promote(self, slot):
@@ -172,6 +177,7 @@ class Engine:
         """Retire a stopped slot, or promote it if it ended a complex64 phase; returns the new
         slot id for a promotion, else None."""
         r = self._slots[slot][0]
+        r.ticks[r.phase] = r.ticks.get(r.phase, 0) + int(getattr(self, '_iters', [0] * (slot + 1))[slot])
         if r.phase == 'c64':
             return self.promote(slot)
         self.retire(slot)
@@ -200,7 +206,8 @@ class Engine:
         Vk = V[:, list(sel)].contiguous()
         _, res = _device_residuals(r.H, Vk, E)
         r.t_done = time.perf_counter()
-        r.result = dict(E=E, V=Vk, residuals=res, iterations=r.iters_done + info.iterations, mu=lam,
+        r.result = dict(E=E, V=Vk, residuals=res, iterations=r.iters_done + info.iterations,
+                        ticks=dict(r.ticks), mu=lam,
                         status=_lib.LOBPCG_STATUS.get(info.status, 'unknown'),
                         converged=bool(res.max() < certify_tol))
         del ws, X0
