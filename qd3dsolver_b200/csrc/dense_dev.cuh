@@ -110,7 +110,10 @@ static __device__ void block_upper_inverse(const double2* S, int n, double2* out
 // Round-robin ordering gives n/2 disjoint (p, q) pairs per round. A pair is rotated while
 // |C_pq| > eps sqrt(|C_pp C_qq|) (the relative-accuracy threshold, so eigenvalues far below
 // ||C|| -- the wanted end of a folded spectrum -- are resolved to working precision); the
-// iteration stops after a sweep without rotations.
+// iteration stops after a sweep without rotations. A round is two barriers: the pairs' rotation
+// parameters, then one update phase in which each thread owns a 2x2 block
+// C[{p_k, q_k}, {p_l, q_l}] <- J_k^H C J_l (the blocks of a round are disjoint) or a row pair of
+// V <- V J_k.
 static __device__ void block_jacobi(double2* C, double2* V, int n) {
   __shared__ double rcs[kMaxSmall / 2 + 1], rsn[kMaxSmall / 2 + 1];
   __shared__ double2 re[kMaxSmall / 2 + 1];
@@ -135,6 +138,7 @@ static __device__ void block_jacobi(double2* C, double2* V, int n) {
     }
     __syncthreads();
   }
+  const int nblk = npair * npair;             // 2x2 blocks of C
   for (int sweep = 0; sweep < 30; ++sweep) {
     if (threadIdx.x == 0) rotated = 0;
     __syncthreads();
@@ -163,38 +167,60 @@ static __device__ void block_jacobi(double2* C, double2* V, int n) {
         rp[k] = p; rq[k] = q; rcs[k] = cs; rsn[k] = sn; re[k] = e;
       }
       __syncthreads();
-      // columns: C <- C J, V <- V J with J = [[cs, sn e], [-sn conj(e), cs]] on (p, q)
-      for (int t = threadIdx.x; t < n * npair; t += blockDim.x) {
-        const int k = t / n, i = t - k * n;
-        const int p = rp[k], q = rq[k];
-        if (q >= n || rsn[k] == 0.0) continue;
-        const double cs = rcs[k], sn = rsn[k];
-        const double2 e = re[k];
-        const double2 m10 = make_double2(-sn * e.x, sn * e.y);   // -sn conj(e)
-        const double2 m01 = make_double2(sn * e.x, sn * e.y);    //  sn e
-        double2 x = C[i * n + p], y = C[i * n + q];
-        double2 np = cscale(cs, x); cfma(np, m10, y);
-        double2 nq = cscale(cs, y); cfma(nq, m01, x);
-        C[i * n + p] = np; C[i * n + q] = nq;
-        x = V[i * n + p]; y = V[i * n + q];
-        np = cscale(cs, x); cfma(np, m10, y);
-        nq = cscale(cs, y); cfma(nq, m01, x);
-        V[i * n + p] = np; V[i * n + q] = nq;
-      }
-      __syncthreads();
-      // rows: C <- J^H C, J^H = [[cs, -sn e], [sn conj(e), cs]]
-      for (int t = threadIdx.x; t < n * npair; t += blockDim.x) {
-        const int k = t / n, j = t - k * n;
-        const int p = rp[k], q = rq[k];
-        if (q >= n || rsn[k] == 0.0) continue;
-        const double cs = rcs[k], sn = rsn[k];
-        const double2 e = re[k];
-        const double2 a01 = make_double2(-sn * e.x, -sn * e.y);
-        const double2 a10 = make_double2(sn * e.x, -sn * e.y);
-        const double2 x = C[p * n + j], y = C[q * n + j];
-        double2 np = cscale(cs, x); cfma(np, a01, y);
-        double2 nq = cscale(cs, y); cfma(nq, a10, x);
-        C[p * n + j] = np; C[q * n + j] = nq;
+      // J = [[cs, sn e], [-sn conj(e), cs]] on columns (p, q); J^H = [[cs, -sn e],
+      // [sn conj(e), cs]] on rows (p, q)
+      for (int t = threadIdx.x; t < nblk + n * npair; t += blockDim.x) {
+        if (t < nblk) {
+          const int k = t / npair, l = t - k * npair;
+          const int pk = rp[k], qk = rq[k], pl = rp[l], ql = rq[l];
+          const bool rk = qk < n && rsn[k] != 0.0, rl = ql < n && rsn[l] != 0.0;
+          if (!rk && !rl) continue;
+          // entries that exist: rows pk (always < n) and qk (if < n), same for columns
+          const bool hk = qk < n, hl = ql < n;
+          double2 a = C[pk * n + pl];
+          double2 b = hl ? C[pk * n + ql] : make_double2(0.0, 0.0);
+          double2 c = hk ? C[qk * n + pl] : make_double2(0.0, 0.0);
+          double2 d = (hk && hl) ? C[qk * n + ql] : make_double2(0.0, 0.0);
+          if (rl) {                          // [a b; c d] <- [a b; c d] J_l
+            const double cs = rcs[l], sn = rsn[l];
+            const double2 e = re[l];
+            const double2 m10 = make_double2(-sn * e.x, sn * e.y);   // -sn conj(e)
+            const double2 m01 = make_double2(sn * e.x, sn * e.y);    //  sn e
+            double2 na = cscale(cs, a); cfma(na, m10, b);
+            double2 nb = cscale(cs, b); cfma(nb, m01, a);
+            double2 nc = cscale(cs, c); cfma(nc, m10, d);
+            double2 nd = cscale(cs, d); cfma(nd, m01, c);
+            a = na; b = nb; c = nc; d = nd;
+          }
+          if (rk) {                          // [a b; c d] <- J_k^H [a b; c d]
+            const double cs = rcs[k], sn = rsn[k];
+            const double2 e = re[k];
+            const double2 a01 = make_double2(-sn * e.x, -sn * e.y);  // -sn e
+            const double2 a10 = make_double2(sn * e.x, -sn * e.y);   //  sn conj(e)
+            double2 na = cscale(cs, a); cfma(na, a01, c);
+            double2 nb = cscale(cs, b); cfma(nb, a01, d);
+            double2 nc = cscale(cs, c); cfma(nc, a10, a);
+            double2 nd = cscale(cs, d); cfma(nd, a10, b);
+            a = na; b = nb; c = nc; d = nd;
+          }
+          C[pk * n + pl] = a;
+          if (hl) C[pk * n + ql] = b;
+          if (hk) C[qk * n + pl] = c;
+          if (hk && hl) C[qk * n + ql] = d;
+        } else {
+          const int u = t - nblk;
+          const int k = u / n, i = u - k * n;
+          const int p = rp[k], q = rq[k];
+          if (q >= n || rsn[k] == 0.0) continue;
+          const double cs = rcs[k], sn = rsn[k];
+          const double2 e = re[k];
+          const double2 m10 = make_double2(-sn * e.x, sn * e.y);
+          const double2 m01 = make_double2(sn * e.x, sn * e.y);
+          const double2 x = V[i * n + p], y = V[i * n + q];
+          double2 np = cscale(cs, x); cfma(np, m10, y);
+          double2 nq = cscale(cs, y); cfma(nq, m01, x);
+          V[i * n + p] = np; V[i * n + q] = nq;
+        }
       }
       __syncthreads();
     }
@@ -350,6 +376,14 @@ static __device__ void update_rows(const BlockList<T>& A, const double2* const* 
       const int units = nr * cols;
       const cplx<T>* src = A.p[b] + r * A.ld[b];
       cplx<T>* d = dst + kst[b];
+      if (sizeof(cplx<T>) == 8 && A.ld[b] == cols && (units & 1) == 0 &&
+          ((uintptr_t)src & 15) == 0 && ((uintptr_t)d & 15) == 0) {
+        for (int u = 2 * threadIdx.x; u < units; u += 2 * blockDim.x) {
+          const unsigned sa = (unsigned)__cvta_generic_to_shared(d + u);
+          asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" :: "r"(sa), "l"(src + u) : "memory");
+        }
+        continue;
+      }
       for (int u = threadIdx.x; u < units; u += blockDim.x) {
         const int rr = A.ld[b] == cols ? 0 : u / cols;
         const cplx<T>* gp = A.ld[b] == cols ? src + u : src + (long long)rr * A.ld[b] + (u - rr * cols);
@@ -372,9 +406,11 @@ static __device__ void update_rows(const BlockList<T>& A, const double2* const* 
   for (int ch = 0; ch < nchunks; ++ch) {
     const long long rc = r0 + (long long)ch * kUpdChunk;
     const int rows = (int)min((long long)kUpdChunk, r1 - rc);
-    issue(ch + NS - 1);
-    cp_async_wait_pending(NS - 1);
+    // chunk ch has landed once at most NS - 2 groups are pending; the barrier also means every
+    // warp is done with chunk ch - 1, whose stage the next copy reuses
+    cp_async_wait_pending(NS - 2);
     __syncthreads();
+    issue(ch + NS - 1);
     const int tr = warp * kUpdRows;             // this warp's 8-row tile in the chunk
     if (tr < rows) {
       const T* sr = reinterpret_cast<const T*>(stage0 + (size_t)(ch % NS) * stage_elems);
@@ -409,7 +445,6 @@ static __device__ void update_rows(const BlockList<T>& A, const double2* const* 
         if (j < NT && col < q && rok) Y[rowg * ldy + col] = mk<T>((T)acc[j][0], (T)acc[j][1]);
       }
     }
-    __syncthreads();                 // the stage is overwritten by the copy two chunks on
   }
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
@@ -461,12 +496,21 @@ __device__ __forceinline__ void gram_copy_rows(const BlockList<T>& L, long long 
     const cplx<T>* src = L.p[b] + r * L.ld[b];
     cplx<T>* d = dst + (long long)off * crow;
     if (L.ld[b] == cols) {
-      for (int u = threadIdx.x; u < units; u += blockDim.x) {
-        const unsigned sa = (unsigned)__cvta_generic_to_shared(d + u);
-        if (sizeof(cplx<T>) == 16)
+      if (sizeof(cplx<T>) == 8 && (units & 1) == 0 && ((uintptr_t)src & 15) == 0 &&
+          ((uintptr_t)d & 15) == 0) {
+        // complex64 run that starts and ends on 16 bytes: two values per copy
+        for (int u = 2 * threadIdx.x; u < units; u += 2 * blockDim.x) {
+          const unsigned sa = (unsigned)__cvta_generic_to_shared(d + u);
           asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" :: "r"(sa), "l"(src + u) : "memory");
-        else
-          asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" :: "r"(sa), "l"(src + u) : "memory");
+        }
+      } else {
+        for (int u = threadIdx.x; u < units; u += blockDim.x) {
+          const unsigned sa = (unsigned)__cvta_generic_to_shared(d + u);
+          if (sizeof(cplx<T>) == 16)
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" :: "r"(sa), "l"(src + u) : "memory");
+          else
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" :: "r"(sa), "l"(src + u) : "memory");
+        }
       }
     } else {
       for (int u = threadIdx.x; u < units; u += blockDim.x) {
@@ -556,9 +600,11 @@ static __device__ void gram_core(const BlockList<T>& A, const BlockList<T>& B,
   for (int ch = 0; ch < nchunks; ++ch) {
     const long long rc = r0 + (long long)ch * crow;
     const int rows = (int)min((long long)crow, r1 - rc);
-    issue(ch + NS - 1);
-    cp_async_wait_pending(NS - 1);
+    // chunk ch has landed once at most NS - 2 groups are pending; the barrier also means every
+    // warp is done with chunk ch - 1, whose stage the next copy reuses
+    cp_async_wait_pending(NS - 2);
     __syncthreads();
+    issue(ch + NS - 1);
     const T* sr = reinterpret_cast<const T*>(stage0 + (size_t)(ch % NS) * stage_elems);
     if (active_warp) {
       for (int k0 = 4 * slice; k0 < rows; k0 += 4 * slices) {
@@ -579,7 +625,6 @@ static __device__ void gram_core(const BlockList<T>& A, const BlockList<T>& B,
           for (int j = 0; j < MC; ++j) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
       }
     }
-    __syncthreads();                 // the stage is overwritten by the copy two chunks on
   }
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
   __syncthreads();
@@ -723,9 +768,11 @@ static __device__ void gram_core_tf32(const BlockList<float>& A, const BlockList
   for (int ch = 0; ch < nchunks; ++ch) {
     const long long rc = r0 + (long long)ch * crow;
     const int rows = (int)min((long long)crow, r1 - rc);
-    issue(ch + NS - 1);
-    cp_async_wait_pending(NS - 1);
+    // chunk ch has landed once at most NS - 2 groups are pending; the barrier also means every
+    // warp is done with chunk ch - 1, whose stage the next copy reuses
+    cp_async_wait_pending(NS - 2);
     __syncthreads();
+    issue(ch + NS - 1);
     const float* sr = reinterpret_cast<const float*>(stage0 + (size_t)(ch % NS) * stage_elems);
     if (active_warp) {
       for (int k0 = 8 * slice; k0 < rows; k0 += 8 * slices) {
@@ -755,7 +802,6 @@ static __device__ void gram_core_tf32(const BlockList<float>& A, const BlockList
         }
       }
     }
-    __syncthreads();
   }
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
   __syncthreads();
@@ -841,6 +887,14 @@ static __device__ void update_rows_tf32(const BlockList<float>& A, const double2
       const int units = nr * cols;
       const float2* src = A.p[b] + r * A.ld[b];
       float2* d = dst + kst[b];
+      if (A.ld[b] == cols && (units & 1) == 0 && ((uintptr_t)src & 15) == 0 &&
+          ((uintptr_t)d & 15) == 0) {
+        for (int u = 2 * threadIdx.x; u < units; u += 2 * blockDim.x) {
+          const unsigned sa = (unsigned)__cvta_generic_to_shared(d + u);
+          asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" :: "r"(sa), "l"(src + u) : "memory");
+        }
+        continue;
+      }
       for (int u = threadIdx.x; u < units; u += blockDim.x) {
         const int rr = A.ld[b] == cols ? 0 : u / cols;
         const float2* gp = A.ld[b] == cols ? src + u : src + (long long)rr * A.ld[b] + (u - rr * cols);
@@ -860,9 +914,11 @@ static __device__ void update_rows_tf32(const BlockList<float>& A, const double2
   for (int ch = 0; ch < nchunks; ++ch) {
     const long long rc = r0 + (long long)ch * kTfUpdChunk;
     const int rows = (int)min((long long)kTfUpdChunk, r1 - rc);
-    issue(ch + NS - 1);
-    cp_async_wait_pending(NS - 1);
+    // chunk ch has landed once at most NS - 2 groups are pending; the barrier also means every
+    // warp is done with chunk ch - 1, whose stage the next copy reuses
+    cp_async_wait_pending(NS - 2);
     __syncthreads();
+    issue(ch + NS - 1);
     const int tr = warp * 16;                    // this warp's 16-row M tile in the chunk
     if (tr < rows) {
       const float* sr = reinterpret_cast<const float*>(stage0 + (size_t)(ch % NS) * stage_elems);
@@ -915,7 +971,6 @@ static __device__ void update_rows_tf32(const BlockList<float>& A, const double2
         }
       }
     }
-    __syncthreads();
   }
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }

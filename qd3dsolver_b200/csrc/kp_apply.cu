@@ -975,16 +975,19 @@ static int num_sms(int device) {
   return cached[device];
 }
 
-// Staged tile shape for a launch: the fewest padded (y, z) sites per useful site, ties to the
-// lower index (the larger tiles).
+// Default kernel for a launch without a tuned choice, from measurements of both kernels over
+// grids of 23x23x20 to 128x128x96 and blocks of 12 and 24 columns on B200: complex128 is FP64-
+// issue bound and the direct kernel (more resident warps) is as fast or faster everywhere;
+// complex64 takes the staged kernel on grids of 200k sites and more, where its shared-memory
+// reuse pays, with the tile shape that pads the (y, z) plane least. qdkp_operator_tune refines
+// this per operator.
 static int pick_staged_cfg(const qdkp_operator* op, int precision) {
-  static const int shape[2][kStagedCfgs][2] = {
-      {{8, 12}, {6, 16}, {4, 20}, {8, 16}},   // complex128: TY, TZ
-      {{8, 12}, {6, 16}, {4, 20}, {8, 24}}};  // complex64
+  if (precision == QDKP_C128 || op->n_sites < 200000) return kDirect;
+  static const int shape[kStagedCfgs][2] = {{8, 12}, {6, 16}, {4, 20}, {8, 24}};   // TY, TZ
   int best = 0;
   double best_w = 1e30;
   for (int c = 0; c < kStagedCfgs; ++c) {
-    const int TY = shape[precision == QDKP_C64][c][0], TZ = shape[precision == QDKP_C64][c][1];
+    const int TY = shape[c][0], TZ = shape[c][1];
     const double w = (double)((op->ny + TY - 1) / TY * TY) * ((op->nz + TZ - 1) / TZ * TZ) *
                      (1.0 + 2.0 / TY) * (1.0 + 2.0 / TZ);
     if (w < best_w - 1e-9) { best_w = w; best = c; }
@@ -1003,11 +1006,10 @@ static int launch_apply_t(const qdkp_operator* op, const T* rec, const void* X, 
   const T shift = shifted ? (T)(-sigma) : T(0);
   const T cb = (T)apply_cb_weight(op);
   const int forced = op->staged_cfg[precision == QDKP_C64];
-  if (op->n_bands == 8 && forced != kDirect && ((uintptr_t)X % sizeof(cplx<T>)) == 0) {
-    const int cfg = forced >= 0 ? forced : pick_staged_cfg(op, precision);
+  const int cfg = forced == QDKP_TILE_AUTO ? pick_staged_cfg(op, precision) : forced;
+  if (op->n_bands == 8 && cfg >= 0 && ((uintptr_t)X % sizeof(cplx<T>)) == 0)
     return launch_staged<T>(cfg, op, rec, X, (int)ldx, Y, (int)ldy, m, shift, cb,
                             num_sms(op->device), st);
-  }
   HXArgs<T> a;
   a.rec = rec;
   a.msk = op->nbmask;
