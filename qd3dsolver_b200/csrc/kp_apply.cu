@@ -978,15 +978,16 @@ static int num_sms(int device) {
 // Default kernel for a launch without a tuned choice, from measurements of both kernels over
 // grids of 23x23x20 to 128x128x96 and blocks of 12 and 24 columns on B200: complex128 is FP64-
 // issue bound and the direct kernel (more resident warps) is as fast or faster everywhere;
-// complex64 takes the staged kernel on grids of 200k sites and more, where its shared-memory
+// complex64 takes the staged kernel on grids of 50k sites and more, where its shared-memory
 // reuse pays, with the tile shape that pads the (y, z) plane least. qdkp_operator_tune refines
 // this per operator.
 static int pick_staged_cfg(const qdkp_operator* op, int precision) {
-  if (precision == QDKP_C128 || op->n_sites < 200000) return kDirect;
-  static const int shape[kStagedCfgs][2] = {{8, 12}, {6, 16}, {4, 20}, {8, 24}};   // TY, TZ
+  if (precision == QDKP_C128 || op->n_sites < 50000) return kDirect;
+  // the four-column shapes (0, 1) measured fastest on every grid; pick the one that pads less
+  static const int shape[2][2] = {{8, 12}, {6, 16}};   // TY, TZ
   int best = 0;
   double best_w = 1e30;
-  for (int c = 0; c < kStagedCfgs; ++c) {
+  for (int c = 0; c < 2; ++c) {
     const int TY = shape[c][0], TZ = shape[c][1];
     const double w = (double)((op->ny + TY - 1) / TY * TY) * ((op->nz + TZ - 1) / TZ * TZ) *
                      (1.0 + 2.0 / TY) * (1.0 + 2.0 / TZ);
