@@ -336,33 +336,43 @@ constexpr int kUpdChunk = kUpdRows * kUpdWarps;     // 64 rows per stage
 template <typename T>
 static __device__ void update_rows(const BlockList<T>& A, const double2* const* C, int q,
                                    long long r0, long long r1, cplx<T>* Y, long long ldy,
-                                   int accumulate, int neg, unsigned char* smem) {
+                                   int accumulate, int neg, unsigned char* smem,
+                                   const double2* const* C2 = nullptr, cplx<T>* Y2 = nullptr) {
+  // optional second output Y2 = A C2 (same rows, same q; a NULL block of C2 is zero): the
+  // fused X / P Ritz update reads [X | R | P] once for both
   const int P = A.total();
   const int KP = 2 * P;
   const int KPp = (KP + 3) / 4 * 4;
   const int NQ = (2 * q + 7) / 8 * 8;
+  const int nout = Y2 ? 2 : 1;
   double* sC = reinterpret_cast<double*>(smem);
-  cplx<T>* stage0 = reinterpret_cast<cplx<T>*>(smem + (size_t)(KPp + 4) * NQ * sizeof(double));
+  double* sC2 = sC + (size_t)(KPp + 4) * NQ;
+  const size_t coef_bytes = (size_t)nout * (KPp + 4) * NQ * sizeof(double);
+  cplx<T>* stage0 = reinterpret_cast<cplx<T>*>(smem + coef_bytes);
   const size_t stage_elems = (size_t)kUpdChunk * P;
-  const int NS = stage_count_fit(stage_elems * sizeof(cplx<T>),
-                                 dyn_smem_bytes() - (size_t)(KPp + 4) * NQ * sizeof(double));
+  const int NS = stage_count_fit(stage_elems * sizeof(cplx<T>), dyn_smem_bytes() - coef_bytes);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const double sg = neg ? -1.0 : 1.0;
   int off[3], kst[3];
   int tot = 0;
   for (int b = 0; b < A.nblk; ++b) { off[b] = tot; tot += A.cols[b]; }
   // KPp + 4 rows: a k step may run up to 3 rows past the last block (multiplied by zeros)
-  for (int e = threadIdx.x; e < (KPp + 4) * NQ; e += blockDim.x) sC[e] = 0.0;
+  for (int e = threadIdx.x; e < nout * (KPp + 4) * NQ; e += blockDim.x) sC[e] = 0.0;
   __syncthreads();
-  for (int e = threadIdx.x; e < P * q; e += blockDim.x) {
-    const int i = e / q, j = e - i * q;
-    int b = 0;
-    while (b < A.nblk - 1 && i >= off[b] + A.cols[b]) ++b;
-    const double2 c = C[b][(i - off[b]) * q + j];
-    sC[(2 * i) * NQ + 2 * j] = sg * c.x;
-    sC[(2 * i) * NQ + 2 * j + 1] = sg * c.y;
-    sC[(2 * i + 1) * NQ + 2 * j] = -sg * c.y;
-    sC[(2 * i + 1) * NQ + 2 * j + 1] = sg * c.x;
+  for (int o = 0; o < nout; ++o) {
+    const double2* const* Co = o ? C2 : C;
+    double* so = o ? sC2 : sC;
+    for (int e = threadIdx.x; e < P * q; e += blockDim.x) {
+      const int i = e / q, j = e - i * q;
+      int b = 0;
+      while (b < A.nblk - 1 && i >= off[b] + A.cols[b]) ++b;
+      if (!Co[b]) continue;
+      const double2 c = Co[b][(i - off[b]) * q + j];
+      so[(2 * i) * NQ + 2 * j] = sg * c.x;
+      so[(2 * i) * NQ + 2 * j + 1] = sg * c.y;
+      so[(2 * i + 1) * NQ + 2 * j] = -sg * c.y;
+      so[(2 * i + 1) * NQ + 2 * j + 1] = sg * c.x;
+    }
   }
   for (int b = 0; b < A.nblk; ++b) kst[b] = off[b] * kUpdChunk;   // block start in a stage
   const int g = lane >> 2, t4 = lane & 3;
@@ -417,13 +427,14 @@ static __device__ void update_rows(const BlockList<T>& A, const double2* const* 
       const int row = tr + g;
       const bool rok = row < rows;
       const long long rowg = rc + row;
-      double acc[6][2];
+      double acc[6][2], acc2[6][2];
 #pragma unroll
       for (int j = 0; j < 6; ++j) {
         const int col = j * 4 + t4;
         cplx<T> y0 = czero<T>();
         if (accumulate && j < NT && col < q && rok) y0 = Y[rowg * ldy + col];
         acc[j][0] = (double)y0.x; acc[j][1] = (double)y0.y;
+        acc2[j][0] = 0.0; acc2[j][1] = 0.0;
       }
       // A fragment of an m8n8k4 MMA: lane (g, t4) holds A'[row g][k0 + t4]
       int kbase = 0;
@@ -436,13 +447,22 @@ static __device__ void update_rows(const BlockList<T>& A, const double2* const* 
 #pragma unroll
           for (int j = 0; j < 6; ++j)
             if (j < NT) dmma(acc[j][0], acc[j][1], a, cr[j * 8]);
+          if (Y2) {
+            const double* cr2 = sC2 + (kbase + k + t4) * NQ + g;
+#pragma unroll
+            for (int j = 0; j < 6; ++j)
+              if (j < NT) dmma(acc2[j][0], acc2[j][1], a, cr2[j * 8]);
+          }
         }
         kbase += kb;
       }
 #pragma unroll
       for (int j = 0; j < 6; ++j) {
         const int col = j * 4 + t4;
-        if (j < NT && col < q && rok) Y[rowg * ldy + col] = mk<T>((T)acc[j][0], (T)acc[j][1]);
+        if (j < NT && col < q && rok) {
+          Y[rowg * ldy + col] = mk<T>((T)acc[j][0], (T)acc[j][1]);
+          if (Y2) Y2[rowg * ldy + col] = mk<T>((T)acc2[j][0], (T)acc2[j][1]);
+        }
       }
     }
   }
@@ -472,10 +492,11 @@ __host__ __device__ __forceinline__ int gram_chunk_rows(int P, int Q, int elem_b
   r = r / 8 * 8;
   return r < kGramRows ? kGramRows : (r > 512 ? 512 : r);
 }
-__host__ __device__ __forceinline__ size_t update_smem_bytes(int P, int q, int elem_bytes) {
+__host__ __device__ __forceinline__ size_t update_smem_bytes(int P, int q, int elem_bytes,
+                                                          int nout = 1) {
   const size_t KPp = (2 * P + 3) / 4 * 4 + 4, NQ = (2 * q + 7) / 8 * 8;
   const size_t stage = (size_t)kUpdChunk * P * elem_bytes;
-  return KPp * NQ * sizeof(double) + stage_count(stage) * stage;
+  return nout * KPp * NQ * sizeof(double) + stage_count(stage) * stage;
 }
 
 __host__ __device__ __forceinline__ size_t gram_smem_bytes(int P, int Q, int elem_bytes) {
@@ -839,42 +860,53 @@ static __device__ void gram_core_tf32(const BlockList<float>& A, const BlockList
 // D (m g, n 2t .. 2t + 1) is one complex output, (m g + 8, ...) another.
 constexpr int kTfUpdChunk = 16 * kUpdWarps;     // 128 rows per stage
 
-__host__ __device__ __forceinline__ size_t update_tf32_smem_bytes(int P, int q) {
+__host__ __device__ __forceinline__ size_t update_tf32_smem_bytes(int P, int q, int nout = 1) {
   const size_t KP8 = (2 * P + 7) / 8 * 8 + 8, NQ = (2 * q + 7) / 8 * 8;
   const size_t stage = (size_t)kTfUpdChunk * P * sizeof(float2);
-  return 2 * KP8 * NQ * sizeof(unsigned) + stage_count(stage) * stage;
+  return nout * 2 * KP8 * NQ * sizeof(unsigned) + stage_count(stage) * stage;
 }
 
 static __device__ void update_rows_tf32(const BlockList<float>& A, const double2* const* C, int q,
                                         long long r0, long long r1, float2* Y, long long ldy,
-                                        int accumulate, int neg, unsigned char* smem) {
+                                        int accumulate, int neg, unsigned char* smem,
+                                        const double2* const* C2 = nullptr,
+                                        float2* Y2 = nullptr) {
   const int P = A.total();
   const int KP = 2 * P;
   const int KP8 = (KP + 7) / 8 * 8 + 8;
   const int NQ = (2 * q + 7) / 8 * 8;
+  const int nout = Y2 ? 2 : 1;
   unsigned* sCh = reinterpret_cast<unsigned*>(smem);        // C'' hi, KP8 x NQ
   unsigned* sCl = sCh + (size_t)KP8 * NQ;                   // C'' lo
-  float2* stage0 = reinterpret_cast<float2*>(sCl + (size_t)KP8 * NQ);
+  unsigned* sCh2 = sCl + (size_t)KP8 * NQ;                  // second output's C'' (if any)
+  unsigned* sCl2 = sCh2 + (size_t)KP8 * NQ;
+  float2* stage0 = reinterpret_cast<float2*>(sCh + (size_t)nout * 2 * KP8 * NQ);
   const size_t stage_elems = (size_t)kTfUpdChunk * P;
   const int NS = stage_count_fit(stage_elems * sizeof(float2),
-                                 dyn_smem_bytes() - 2 * (size_t)KP8 * NQ * sizeof(unsigned));
+                                 dyn_smem_bytes() - (size_t)nout * 2 * KP8 * NQ * sizeof(unsigned));
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const double sg = neg ? -1.0 : 1.0;
   int off[3], kst[3];
   int tot = 0;
   for (int b = 0; b < A.nblk; ++b) { off[b] = tot; tot += A.cols[b]; }
-  for (int e = threadIdx.x; e < KP8 * NQ; e += blockDim.x) { sCh[e] = 0u; sCl[e] = 0u; }
+  for (int e = threadIdx.x; e < nout * 2 * KP8 * NQ; e += blockDim.x) sCh[e] = 0u;
   __syncthreads();
-  for (int e = threadIdx.x; e < P * q; e += blockDim.x) {
-    const int i = e / q, j = e - i * q;
-    int b = 0;
-    while (b < A.nblk - 1 && i >= off[b] + A.cols[b]) ++b;
-    const double2 c = C[b][(i - off[b]) * q + j];
-    const float v[4] = {(float)(sg * c.x), (float)(sg * c.y), (float)(-sg * c.y), (float)(sg * c.x)};
-    const int idx[4] = {(2 * i) * NQ + 2 * j, (2 * i) * NQ + 2 * j + 1, (2 * i + 1) * NQ + 2 * j,
-                        (2 * i + 1) * NQ + 2 * j + 1};
+  for (int o = 0; o < nout; ++o) {
+    const double2* const* Co = o ? C2 : C;
+    unsigned* sh = o ? sCh2 : sCh;
+    unsigned* sl = o ? sCl2 : sCl;
+    for (int e = threadIdx.x; e < P * q; e += blockDim.x) {
+      const int i = e / q, j = e - i * q;
+      int b = 0;
+      while (b < A.nblk - 1 && i >= off[b] + A.cols[b]) ++b;
+      if (!Co[b]) continue;
+      const double2 c = Co[b][(i - off[b]) * q + j];
+      const float v[4] = {(float)(sg * c.x), (float)(sg * c.y), (float)(-sg * c.y), (float)(sg * c.x)};
+      const int idx[4] = {(2 * i) * NQ + 2 * j, (2 * i) * NQ + 2 * j + 1, (2 * i + 1) * NQ + 2 * j,
+                          (2 * i + 1) * NQ + 2 * j + 1};
 #pragma unroll
-    for (int u = 0; u < 4; ++u) tf32_split(v[u], sCh[idx[u]], sCl[idx[u]]);
+      for (int u = 0; u < 4; ++u) tf32_split(v[u], sh[idx[u]], sl[idx[u]]);
+    }
   }
   for (int b = 0; b < A.nblk; ++b) kst[b] = off[b] * kTfUpdChunk;
   const int g = lane >> 2, t = lane & 3;
@@ -924,7 +956,7 @@ static __device__ void update_rows_tf32(const BlockList<float>& A, const double2
       const float* sr = reinterpret_cast<const float*>(stage0 + (size_t)(ch % NS) * stage_elems);
       const int ra = tr + g, rb = tr + g + 8;
       const bool oka = ra < rows, okb = rb < rows;
-      float acc[6][4];
+      float acc[6][4], acc2[6][4];
 #pragma unroll
       for (int j = 0; j < 6; ++j) {
         const int col = j * 4 + t;
@@ -934,6 +966,8 @@ static __device__ void update_rows_tf32(const BlockList<float>& A, const double2
           if (okb) yb = Y[(rc + rb) * ldy + col];
         }
         acc[j][0] = ya.x; acc[j][1] = ya.y; acc[j][2] = yb.x; acc[j][3] = yb.y;
+#pragma unroll
+        for (int e2 = 0; e2 < 4; ++e2) acc2[j][e2] = 0.f;
       }
       int kbase = 0;
       for (int b = 0; b < A.nblk; ++b) {
@@ -957,6 +991,10 @@ static __device__ void update_rows_tf32(const BlockList<float>& A, const double2
               const int i0 = (kr + t) * NQ + j * 8 + g, i1 = (kr + t + 4) * NQ + j * 8 + g;
               const unsigned bh[2] = {sCh[i0], sCh[i1]}, bl[2] = {sCl[i0], sCl[i1]};
               mma_tf32x3(acc[j], ah, al, bh, bl);
+              if (Y2) {
+                const unsigned bh2[2] = {sCh2[i0], sCh2[i1]}, bl2[2] = {sCl2[i0], sCl2[i1]};
+                mma_tf32x3(acc2[j], ah, al, bh2, bl2);
+              }
             }
           }
         }
@@ -968,6 +1006,10 @@ static __device__ void update_rows_tf32(const BlockList<float>& A, const double2
         if (j < NT && col < q) {
           if (oka) Y[(rc + ra) * ldy + col] = make_float2(acc[j][0], acc[j][1]);
           if (okb) Y[(rc + rb) * ldy + col] = make_float2(acc[j][2], acc[j][3]);
+          if (Y2) {
+            if (oka) Y2[(rc + ra) * ldy + col] = make_float2(acc2[j][0], acc2[j][1]);
+            if (okb) Y2[(rc + rb) * ldy + col] = make_float2(acc2[j][2], acc2[j][3]);
+          }
         }
       }
     }

@@ -25,7 +25,9 @@ constexpr int kEGramSplit = 16;
 constexpr int kEGramMaxParts = 296;
 
 enum GramWhich { GR_XR = 0, GR_RR, GR_PP, GR_WW, GR_WAW, GR_BA, GR_BB };
-enum UpdWhich { UP_RPROJ = 0, UP_RNORM, UP_PNORM, UP_APNORM, UP_PNEW, UP_APNEW, UP_XNEW, UP_AXNEW };
+// UP_XPNEW: P = R Cr + P Cp and X = X Cx + R Cr + P Cp from one pass over [X | R | P]
+// (lobpcg.py:921-973); UP_AXPNEW: the same for AP and AX.
+enum UpdWhich { UP_RPROJ = 0, UP_RNORM, UP_PNORM, UP_APNORM, UP_XPNEW, UP_AXPNEW };
 enum RowWhich { RW_COPYBEST = 0, RW_RESID, RW_GATHERP };
 
 // ---------------------------------------------------------------------------------------------
@@ -318,11 +320,13 @@ __global__ void e_gram_reduce2(const ESlot* __restrict__ S, int which) {
 // ---------------------------------------------------------------------------------------------
 template <typename T>
 __device__ bool upd_lists(const ESlot& d, int which, BlockList<T>& A, const double2* C[3],
-                          int& q, cplx<T>*& Y, int& accumulate, int& neg) {
+                          int& q, cplx<T>*& Y, int& accumulate, int& neg,
+                          const double2* C2[3], cplx<T>*& Y2) {
   const EState* st = d.st;
   if (st->idle) return false;
   const int m = d.m, ma = st->ma, mp = st->mp;
   accumulate = 0; neg = 0;
+  Y2 = nullptr;
   auto set = [&](int i, double2* p, int ld, int c, const double2* cf) {
     A.p[i] = blk<T>(p); A.ld[i] = ld; A.cols[i] = c; C[i] = cf;
   };
@@ -335,16 +339,18 @@ __device__ bool upd_lists(const ESlot& d, int which, BlockList<T>& A, const doub
     case UP_APNORM:
       if (st->skip_pnorm) return false;
       A.nblk = 1; set(0, d.APa, ma, ma, d.U); q = ma; Y = blk<T>(d.APa); return true;
-    case UP_PNEW:
-      A.nblk = mp ? 2 : 1; set(0, d.Ra, ma, ma, d.Cr); set(1, d.Pa, ma, mp, d.Cp);
-      q = m; Y = blk<T>(d.P); return true;
-    case UP_APNEW:
-      A.nblk = mp ? 2 : 1; set(0, d.ARa, ma, ma, d.Cr); set(1, d.APa, ma, mp, d.Cp);
-      q = m; Y = blk<T>(d.AP); return true;
-    case UP_XNEW:
-      A.nblk = 2; set(0, d.X, m, m, d.Cx); set(1, d.P, m, m, d.Im); q = m; Y = blk<T>(d.X); return true;
-    default:
-      A.nblk = 2; set(0, d.AX, m, m, d.Cx); set(1, d.AP, m, m, d.Im); q = m; Y = blk<T>(d.AX); return true;
+    default: {        // UP_XPNEW / UP_AXPNEW
+      const bool ax = which == UP_AXPNEW;
+      A.nblk = mp ? 3 : 2;
+      set(0, ax ? d.AX : d.X, m, m, nullptr);            // X rows do not enter P
+      set(1, ax ? d.ARa : d.Ra, ma, ma, d.Cr);
+      set(2, ax ? d.APa : d.Pa, ma, mp, d.Cp);
+      C2[0] = d.Cx; C2[1] = d.Cr; C2[2] = d.Cp;
+      q = m;
+      Y = blk<T>(ax ? d.AP : d.P);
+      Y2 = blk<T>(ax ? d.AX : d.X);
+      return true;
+    }
   }
 }
 
@@ -354,19 +360,20 @@ e_update_kernel(const ESlot* __restrict__ S, int ns, int which) {
   const int k = slot_of(S, ns, blockIdx.x, &ESlot::row0);
   const ESlot& d = S[k];
   const double2* Cf[3];
+  const double2* C2[3] = {nullptr, nullptr, nullptr};
   int q, accumulate, neg;
   const long long r0 = (long long)(blockIdx.x - d.row0) * d.rows_per_cta;
   const long long r1 = min(d.n, r0 + d.rows_per_cta);
   if (d.prec == QDKP_C64) {
     BlockList<float> A;
-    float2* Y;
-    if (!upd_lists<float>(d, which, A, Cf, q, Y, accumulate, neg)) return;
-    update_rows_tf32(A, Cf, q, r0, r1, Y, (long long)q, accumulate, neg, usm_e);
+    float2 *Y, *Y2;
+    if (!upd_lists<float>(d, which, A, Cf, q, Y, accumulate, neg, C2, Y2)) return;
+    update_rows_tf32(A, Cf, q, r0, r1, Y, (long long)q, accumulate, neg, usm_e, C2, Y2);
   } else {
     BlockList<double> A;
-    double2* Y;
-    if (!upd_lists<double>(d, which, A, Cf, q, Y, accumulate, neg)) return;
-    update_rows(A, Cf, q, r0, r1, Y, (long long)q, accumulate, neg, usm_e);
+    double2 *Y, *Y2;
+    if (!upd_lists<double>(d, which, A, Cf, q, Y, accumulate, neg, C2, Y2)) return;
+    update_rows(A, Cf, q, r0, r1, Y, (long long)q, accumulate, neg, usm_e, C2, Y2);
   }
 }
 
@@ -724,8 +731,10 @@ int launch_gram_multi(qdkp_engine* e, int which, cudaStream_t st) {
 }
 
 int launch_update_multi(qdkp_engine* e, int which, cudaStream_t st) {
-  const size_t smem = std::max(update_smem_bytes(2 * e->m_max, e->m_max, (int)sizeof(double2)),
-                               update_tf32_smem_bytes(2 * e->m_max, e->m_max));
+  const bool fused = which == UP_XPNEW || which == UP_AXPNEW;
+  const int P = (fused ? 3 : 1) * e->m_max, nout = fused ? 2 : 1;
+  const size_t smem = std::max(update_smem_bytes(P, e->m_max, (int)sizeof(double2), nout),
+                               update_tf32_smem_bytes(P, e->m_max, nout));
   e_update_kernel<<<e->row_ctas, kUpdThreads, smem, st>>>(e->d_slots, e->ns, which);
   count_launch();
   QDKP_CUDA_TRY(cudaGetLastError());
@@ -780,10 +789,8 @@ int tick(qdkp_engine* e, cudaStream_t st) {
   e_rr_kernel<<<ns, kSmallThreads, rr_smem, st>>>(e->d_slots);
   count_launch();
   QDKP_CUDA_TRY(cudaGetLastError());
-  ETRY(launch_update_multi(e, UP_PNEW, st));
-  ETRY(launch_update_multi(e, UP_APNEW, st));
-  ETRY(launch_update_multi(e, UP_XNEW, st));
-  ETRY(launch_update_multi(e, UP_AXNEW, st));
+  ETRY(launch_update_multi(e, UP_XPNEW, st));
+  ETRY(launch_update_multi(e, UP_AXPNEW, st));
 #undef ETRY
   return QDKP_OK;
 }
