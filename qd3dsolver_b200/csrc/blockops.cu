@@ -262,7 +262,7 @@ struct CoefList {
 };
 
 template <typename T>
-__global__ void __launch_bounds__(kUpdThreads)
+__global__ void __launch_bounds__(kUpdThreads, 2)
 update_kernel(const BlockList<T> A, const CoefList C, int q, long long n, cplx<T>* Y,
               long long ldy, int accumulate) {
   extern __shared__ __align__(16) unsigned char usm[];

@@ -152,15 +152,21 @@ static __device__ void block_jacobi(double2* C, double2* V, int n) {
         double cs = 1.0, sn = 0.0;
         double2 e = make_double2(1.0, 0.0);
         if (q < n) {
+          // squared-magnitude tests and reciprocal square roots keep the serial chain of a
+          // round short; Gram-built entries are far from the FP64 range limits (|c|^2 neither
+          // under- nor overflows where the tests pass)
           const double2 c = C[p * n + q];
-          const double ac = hypot(c.x, c.y);
+          const double ac2 = c.x * c.x + c.y * c.y;
           const double a = C[p * n + p].x, b = C[q * n + q].x;
-          if (ac > floor_abs && ac > 2.2e-16 * sqrt(fabs(a) * fabs(b))) {
-            const double tau = (b - a) / (2.0 * ac);
-            const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
-            cs = 1.0 / sqrt(1.0 + t * t);
+          if (ac2 > floor_abs * floor_abs && ac2 > 4.84e-32 * fabs(a * b)) {
+            const double rac = rsqrt(ac2);
+            const double tau = 0.5 * (b - a) * rac;
+            const double at = fabs(tau);
+            const double t = at > 1e150 ? 0.5 / tau
+                                        : (tau >= 0.0 ? 1.0 : -1.0) / (at + sqrt(1.0 + tau * tau));
+            cs = rsqrt(1.0 + t * t);
             sn = t * cs;
-            e = make_double2(c.x / ac, c.y / ac);
+            e = make_double2(c.x * rac, c.y * rac);
             if (sn != 0.0) rotated = 1;
           }
         }
@@ -853,168 +859,198 @@ static __device__ void gram_core_tf32(const BlockList<float>& A, const BlockList
   for (int e = threadIdx.x; e < RP * RQ; e += blockDim.x) out[e] = gsm[e];
 }
 
-// Y' = A' C'' for rows [r0, r1) of complex64 blocks on TF32 tensor cores (split as above; same
-// staging as update_rows with kTfUpdChunk rows per stage, one 16-row M tile per warp). Fragments:
-// A_mma[m][k] = A'[row m][k]: a0 = (m g, k t), a1 = (m g + 8, k t), a2 = (m g, k t + 4),
-// a3 = (m g + 8, k t + 4); B_mma[k][n] = C''[k][n]: b0 = (k t, n g), b1 = (k t + 4, n g);
-// D (m g, n 2t .. 2t + 1) is one complex output, (m g + 8, ...) another.
-constexpr int kTfUpdChunk = 16 * kUpdWarps;     // 128 rows per stage
+// Y' = A' C'' for rows [r0, r1) of complex64 blocks on TF32 tensor cores (split as above).
+// Nothing is staged: a warp owns 16-row M tiles (tiles warp, warp + warps, ... of the CTA's
+// rows) and loads its A fragments from global memory into registers, a ring of k steps ahead of
+// the MMAs, so a CTA needs no barrier after its coefficient setup. The MMA's k order is
+// permuted so that a lane's two k values of a fragment row are the real and imaginary part of
+// one complex element: k step s covers complex columns c0 .. c0 + 3 of one block, and
+// MMA k = t <-> Re A[.][c0 + t], k = t + 4 <-> Im A[.][c0 + t] (g = lane / 4, t = lane % 4), so
+// a0 a2 = A[row g][c0 + t] and a1 a3 = A[row g + 8][c0 + t] are one 8-byte load each. C'' (the
+// real representation of the stacked complex coefficients, as in update_rows) is stored in that
+// k order as one 16-byte word per (k step, 8-column N tile, lane): {hi b0, hi b1, lo b0, lo b1}
+// with b0 = C''[k t][n g], b1 = C''[k t + 4][n g]. A row is read (by the four lanes of its quad)
+// before any of its outputs is written and no other warp touches it, so Y may alias an input.
+constexpr int kTfUpdChunk = 128;   // row granularity of a CTA's span (a multiple of the M tile)
+constexpr int kTfRing = 8;         // k steps of A fragments in flight per warp (narrow outputs)
+constexpr int kTfMaxKs = kMaxSmall / 4 + 3;
+
+// k steps of a list of at most three blocks with P columns in all (ceil(cols / 4) per block)
+__host__ __device__ __forceinline__ int tf32_ksteps_bound(int P) { return (P + 3) / 4 + 2; }
 
 __host__ __device__ __forceinline__ size_t update_tf32_smem_bytes(int P, int q, int nout = 1) {
-  const size_t KP8 = (2 * P + 7) / 8 * 8 + 8, NQ = (2 * q + 7) / 8 * 8;
-  const size_t stage = (size_t)kTfUpdChunk * P * sizeof(float2);
-  return nout * 2 * KP8 * NQ * sizeof(unsigned) + stage_count(stage) * stage;
+  return (size_t)nout * tf32_ksteps_bound(P) * ((q + 3) / 4) * 32 * sizeof(uint4);
 }
 
+// one k step of an update's A list: columns c0 .. c0 + 3 of a block (p points at column c0)
+struct TfKStep {
+  const float2* p;
+  int ld;
+  int rem;          // columns of the block from c0 on
+};
+
+template <int NT, int NOUT, bool ACC>
+static __device__ __forceinline__ void update_tf32_core(const TfKStep* __restrict__ sK,
+                                                        const uint4* __restrict__ sB, int KS,
+                                                        int q, long long r0, long long r1,
+                                                        float2* Y, float2* Y2, long long ldy) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = lane >> 2, t = lane & 3;
+  const int nw = blockDim.x >> 5;
+  const int ntiles = (int)((r1 - r0 + 15) / 16);
+  const int mine = ntiles > warp ? (ntiles - warp + nw - 1) / nw : 0;
+  const int nitems = mine * KS;
+  if (nitems == 0) return;
+  // wide outputs hold more accumulators: a shorter ring keeps the warp within 128 registers
+  constexpr int RING = NT * NOUT <= 6 ? kTfRing : kTfRing / 2;
+  float2 fa[RING], fb[RING];
+  int l_tile = warp, l_s = 0;
+  auto fetch = [&](float2& xa, float2& xb) {
+    const TfKStep k = sK[l_s];
+    const long long ra = r0 + (long long)l_tile * 16 + g, rb = ra + 8;
+    xa = (t < k.rem && ra < r1) ? __ldcs(k.p + ra * k.ld + t) : make_float2(0.f, 0.f);
+    xb = (t < k.rem && rb < r1) ? __ldcs(k.p + rb * k.ld + t) : make_float2(0.f, 0.f);
+    if (++l_s == KS) { l_s = 0; l_tile += nw; }
+  };
+#pragma unroll
+  for (int d = 0; d < RING; ++d)
+    if (d < nitems) fetch(fa[d], fb[d]);
+  float acc[NOUT][NT][4];
+  float2 yo[ACC ? NT : 1][2];
+#pragma unroll
+  for (int o = 0; o < NOUT; ++o)
+#pragma unroll
+    for (int j = 0; j < NT; ++j)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) acc[o][j][e] = 0.f;
+  int c_s = 0, c_tile = warp;
+  for (int base = 0; base < nitems; base += RING) {
+#pragma unroll
+    for (int d = 0; d < RING; ++d) {
+      const int it = base + d;
+      if (it >= nitems) break;
+      unsigned ah[4], al[4];
+      tf32_split(fa[d].x, ah[0], al[0]);
+      tf32_split(fb[d].x, ah[1], al[1]);
+      tf32_split(fa[d].y, ah[2], al[2]);
+      tf32_split(fb[d].y, ah[3], al[3]);
+      if (it + RING < nitems) fetch(fa[d], fb[d]);
+      const long long ra = r0 + (long long)c_tile * 16 + g, rb = ra + 8;
+      if (ACC && c_s == 0) {
+#pragma unroll
+        for (int j = 0; j < NT; ++j) {
+          const int col = j * 4 + t;
+          yo[j][0] = (col < q && ra < r1) ? Y[ra * ldy + col] : make_float2(0.f, 0.f);
+          yo[j][1] = (col < q && rb < r1) ? Y[rb * ldy + col] : make_float2(0.f, 0.f);
+        }
+      }
+      const uint4* bp = sB + (size_t)c_s * NT * 32 + lane;
+#pragma unroll
+      for (int j = 0; j < NT; ++j) {
+        const uint4 b = bp[j * 32];
+        const unsigned bh[2] = {b.x, b.y}, bl[2] = {b.z, b.w};
+        mma_tf32x3(acc[0][j], ah, al, bh, bl);
+        if (NOUT == 2) {
+          const uint4 b2 = bp[(size_t)KS * NT * 32 + j * 32];
+          const unsigned bh2[2] = {b2.x, b2.y}, bl2[2] = {b2.z, b2.w};
+          mma_tf32x3(acc[NOUT - 1][j], ah, al, bh2, bl2);
+        }
+      }
+      if (++c_s == KS) {
+#pragma unroll
+        for (int j = 0; j < NT; ++j) {
+          const int col = j * 4 + t;
+          if (col < q) {
+            float2 va = make_float2(acc[0][j][0], acc[0][j][1]);
+            float2 vb = make_float2(acc[0][j][2], acc[0][j][3]);
+            if (ACC) {
+              va.x += yo[j][0].x; va.y += yo[j][0].y;
+              vb.x += yo[j][1].x; vb.y += yo[j][1].y;
+            }
+            if (ra < r1) Y[ra * ldy + col] = va;
+            if (rb < r1) Y[rb * ldy + col] = vb;
+            if (NOUT == 2) {
+              if (ra < r1) Y2[ra * ldy + col] = make_float2(acc[NOUT - 1][j][0], acc[NOUT - 1][j][1]);
+              if (rb < r1) Y2[rb * ldy + col] = make_float2(acc[NOUT - 1][j][2], acc[NOUT - 1][j][3]);
+            }
+          }
+#pragma unroll
+          for (int o = 0; o < NOUT; ++o)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) acc[o][j][e] = 0.f;
+        }
+        c_s = 0;
+        c_tile += nw;
+      }
+    }
+  }
+}
+
+// Y (+)= sg A C over rows [r0, r1) and, with C2/Y2, Y2 = sg A C2 (one pass over A). C[b] is the
+// cols_b x q row-major coefficient block of A's block b (NULL: the block does not enter);
+// q <= kMaxBlock. Called by every thread of the CTA; smem holds update_tf32_smem_bytes. The
+// two-output form that also accumulates into Y takes two passes over A, so there Y must not
+// alias an input.
 static __device__ void update_rows_tf32(const BlockList<float>& A, const double2* const* C, int q,
                                         long long r0, long long r1, float2* Y, long long ldy,
                                         int accumulate, int neg, unsigned char* smem,
                                         const double2* const* C2 = nullptr,
                                         float2* Y2 = nullptr) {
-  const int P = A.total();
-  const int KP = 2 * P;
-  const int KP8 = (KP + 7) / 8 * 8 + 8;
-  const int NQ = (2 * q + 7) / 8 * 8;
+  __shared__ int2 sK[kTfMaxKs];
+  __shared__ TfKStep sKp[kTfMaxKs];
+  __shared__ int sKS;
   const int nout = Y2 ? 2 : 1;
-  unsigned* sCh = reinterpret_cast<unsigned*>(smem);        // C'' hi, KP8 x NQ
-  unsigned* sCl = sCh + (size_t)KP8 * NQ;                   // C'' lo
-  unsigned* sCh2 = sCl + (size_t)KP8 * NQ;                  // second output's C'' (if any)
-  unsigned* sCl2 = sCh2 + (size_t)KP8 * NQ;
-  float2* stage0 = reinterpret_cast<float2*>(sCh + (size_t)nout * 2 * KP8 * NQ);
-  const size_t stage_elems = (size_t)kTfUpdChunk * P;
-  const int NS = stage_count_fit(stage_elems * sizeof(float2),
-                                 dyn_smem_bytes() - (size_t)nout * 2 * KP8 * NQ * sizeof(unsigned));
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const double sg = neg ? -1.0 : 1.0;
-  int off[3], kst[3];
-  int tot = 0;
-  for (int b = 0; b < A.nblk; ++b) { off[b] = tot; tot += A.cols[b]; }
-  for (int e = threadIdx.x; e < nout * 2 * KP8 * NQ; e += blockDim.x) sCh[e] = 0u;
+  const int NT = (q + 3) / 4;
+  if (threadIdx.x == 0) {
+    int s = 0;
+    for (int b = 0; b < A.nblk; ++b)
+      for (int c0 = 0; c0 < A.cols[b]; c0 += 4) {
+        sKp[s].p = A.p[b] + c0; sKp[s].ld = (int)A.ld[b]; sKp[s].rem = A.cols[b] - c0;
+        sK[s++] = make_int2(b, c0);
+      }
+    sKS = s;
+  }
   __syncthreads();
-  for (int o = 0; o < nout; ++o) {
-    const double2* const* Co = o ? C2 : C;
-    unsigned* sh = o ? sCh2 : sCh;
-    unsigned* sl = o ? sCl2 : sCl;
-    for (int e = threadIdx.x; e < P * q; e += blockDim.x) {
-      const int i = e / q, j = e - i * q;
-      int b = 0;
-      while (b < A.nblk - 1 && i >= off[b] + A.cols[b]) ++b;
-      if (!Co[b]) continue;
-      const double2 c = Co[b][(i - off[b]) * q + j];
-      const float v[4] = {(float)(sg * c.x), (float)(sg * c.y), (float)(-sg * c.y), (float)(sg * c.x)};
-      const int idx[4] = {(2 * i) * NQ + 2 * j, (2 * i) * NQ + 2 * j + 1, (2 * i + 1) * NQ + 2 * j,
-                          (2 * i + 1) * NQ + 2 * j + 1};
-#pragma unroll
-      for (int u = 0; u < 4; ++u) tf32_split(v[u], sh[idx[u]], sl[idx[u]]);
+  const int KS = sKS;
+  uint4* sB = reinterpret_cast<uint4*>(smem);
+  const float sg = neg ? -1.f : 1.f;
+  const int per_out = KS * NT * 32;
+  for (int e = threadIdx.x; e < nout * per_out; e += blockDim.x) {
+    const int o = e / per_out, r = e - o * per_out;
+    const int s = r / (NT * 32), r2 = r - s * NT * 32;
+    const int j = r2 >> 5, ln = r2 & 31;
+    const int gg = ln >> 2, tt = ln & 3;
+    const int2 k = sK[s];
+    const int cols = k.x == 0 ? A.cols[0] : k.x == 1 ? A.cols[1] : A.cols[2];
+    const double2* Cb = (o ? C2 : C)[k.x];
+    const int i = k.y + tt, jj = j * 4 + (gg >> 1);
+    float v0 = 0.f, v1 = 0.f;
+    if (Cb && i < cols && jj < q) {
+      const double2 c = Cb[(size_t)i * q + jj];
+      const float re = sg * (float)c.x, im = sg * (float)c.y;
+      if (gg & 1) { v0 = im; v1 = re; }          // C''[2i][2jj+1], C''[2i+1][2jj+1]
+      else { v0 = re; v1 = -im; }                // C''[2i][2jj],   C''[2i+1][2jj]
     }
+    uint4 w;
+    tf32_split(v0, w.x, w.z);
+    tf32_split(v1, w.y, w.w);
+    sB[e] = w;
   }
-  for (int b = 0; b < A.nblk; ++b) kst[b] = off[b] * kTfUpdChunk;
-  const int g = lane >> 2, t = lane & 3;
-  const int NT = NQ / 8;
-  const long long nrows = r1 - r0;
-  const int nchunks = (int)((nrows + kTfUpdChunk - 1) / kTfUpdChunk);
-  auto stage_rows = [&](long long r, int nr, float2* dst) {
-    for (int b = 0; b < A.nblk; ++b) {
-      const int cols = A.cols[b];
-      const int units = nr * cols;
-      const float2* src = A.p[b] + r * A.ld[b];
-      float2* d = dst + kst[b];
-      if (A.ld[b] == cols && (units & 1) == 0 && ((uintptr_t)src & 15) == 0 &&
-          ((uintptr_t)d & 15) == 0) {
-        for (int u = 2 * threadIdx.x; u < units; u += 2 * blockDim.x) {
-          const unsigned sa = (unsigned)__cvta_generic_to_shared(d + u);
-          asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" :: "r"(sa), "l"(src + u) : "memory");
-        }
-        continue;
-      }
-      for (int u = threadIdx.x; u < units; u += blockDim.x) {
-        const int rr = A.ld[b] == cols ? 0 : u / cols;
-        const float2* gp = A.ld[b] == cols ? src + u : src + (long long)rr * A.ld[b] + (u - rr * cols);
-        const unsigned sa = (unsigned)__cvta_generic_to_shared(d + u);
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" :: "r"(sa), "l"(gp) : "memory");
-      }
-    }
-  };
-  auto issue = [&](int c) {
-    if (c < nchunks) {
-      const long long rn = r0 + (long long)c * kTfUpdChunk;
-      stage_rows(rn, (int)min((long long)kTfUpdChunk, r1 - rn), stage0 + (size_t)(c % NS) * stage_elems);
-    }
-    asm volatile("cp.async.commit_group;\n" ::: "memory");
-  };
-  for (int c = 0; c < NS - 1; ++c) issue(c);
-  for (int ch = 0; ch < nchunks; ++ch) {
-    const long long rc = r0 + (long long)ch * kTfUpdChunk;
-    const int rows = (int)min((long long)kTfUpdChunk, r1 - rc);
-    // chunk ch has landed once at most NS - 2 groups are pending; the barrier also means every
-    // warp is done with chunk ch - 1, whose stage the next copy reuses
-    cp_async_wait_pending(NS - 2);
-    __syncthreads();
-    issue(ch + NS - 1);
-    const int tr = warp * 16;                    // this warp's 16-row M tile in the chunk
-    if (tr < rows) {
-      const float* sr = reinterpret_cast<const float*>(stage0 + (size_t)(ch % NS) * stage_elems);
-      const int ra = tr + g, rb = tr + g + 8;
-      const bool oka = ra < rows, okb = rb < rows;
-      float acc[6][4], acc2[6][4];
-#pragma unroll
-      for (int j = 0; j < 6; ++j) {
-        const int col = j * 4 + t;
-        float2 ya = make_float2(0.f, 0.f), yb = make_float2(0.f, 0.f);
-        if (accumulate && j < NT && col < q) {
-          if (oka) ya = Y[(rc + ra) * ldy + col];
-          if (okb) yb = Y[(rc + rb) * ldy + col];
-        }
-        acc[j][0] = ya.x; acc[j][1] = ya.y; acc[j][2] = yb.x; acc[j][3] = yb.y;
-#pragma unroll
-        for (int e2 = 0; e2 < 4; ++e2) acc2[j][e2] = 0.f;
-      }
-      int kbase = 0;
-      for (int b = 0; b < A.nblk; ++b) {
-        const int kb = 2 * A.cols[b];
-        const float* rsa = sr + 2 * kst[b] + (oka ? ra : 0) * kb;
-        const float* rsb = sr + 2 * kst[b] + (okb ? rb : 0) * kb;
-        for (int k = 0; k < kb; k += 8) {
-          const float v0 = (oka && k + t < kb) ? rsa[k + t] : 0.f;
-          const float v1 = (okb && k + t < kb) ? rsb[k + t] : 0.f;
-          const float v2 = (oka && k + t + 4 < kb) ? rsa[k + t + 4] : 0.f;
-          const float v3 = (okb && k + t + 4 < kb) ? rsb[k + t + 4] : 0.f;
-          unsigned ah[4], al[4];
-          tf32_split(v0, ah[0], al[0]);
-          tf32_split(v1, ah[1], al[1]);
-          tf32_split(v2, ah[2], al[2]);
-          tf32_split(v3, ah[3], al[3]);
-          const int kr = kbase + k;
-#pragma unroll
-          for (int j = 0; j < 6; ++j) {
-            if (j < NT) {
-              const int i0 = (kr + t) * NQ + j * 8 + g, i1 = (kr + t + 4) * NQ + j * 8 + g;
-              const unsigned bh[2] = {sCh[i0], sCh[i1]}, bl[2] = {sCl[i0], sCl[i1]};
-              mma_tf32x3(acc[j], ah, al, bh, bl);
-              if (Y2) {
-                const unsigned bh2[2] = {sCh2[i0], sCh2[i1]}, bl2[2] = {sCl2[i0], sCl2[i1]};
-                mma_tf32x3(acc2[j], ah, al, bh2, bl2);
-              }
-            }
-          }
-        }
-        kbase += kb;
-      }
-#pragma unroll
-      for (int j = 0; j < 6; ++j) {
-        const int col = j * 4 + t;
-        if (j < NT && col < q) {
-          if (oka) Y[(rc + ra) * ldy + col] = make_float2(acc[j][0], acc[j][1]);
-          if (okb) Y[(rc + rb) * ldy + col] = make_float2(acc[j][2], acc[j][3]);
-          if (Y2) {
-            if (oka) Y2[(rc + ra) * ldy + col] = make_float2(acc2[j][0], acc2[j][1]);
-            if (okb) Y2[(rc + rb) * ldy + col] = make_float2(acc2[j][2], acc2[j][3]);
-          }
-        }
-      }
-    }
+  __syncthreads();
+#define QDKP_TF_CASE(nt)                                                                          \
+  case nt:                                                                                        \
+    if (nout == 2 && accumulate) {                                                                \
+      update_tf32_core<nt, 1, true>(sKp, sB, KS, q, r0, r1, Y, Y2, ldy);                          \
+      update_tf32_core<nt, 1, false>(sKp, sB + per_out, KS, q, r0, r1, Y2, Y2, ldy);              \
+    } else if (nout == 2) update_tf32_core<nt, 2, false>(sKp, sB, KS, q, r0, r1, Y, Y2, ldy);     \
+    else if (accumulate) update_tf32_core<nt, 1, true>(sKp, sB, KS, q, r0, r1, Y, Y2, ldy);       \
+    else update_tf32_core<nt, 1, false>(sKp, sB, KS, q, r0, r1, Y, Y2, ldy);                      \
+    break;
+  switch (NT) {
+    QDKP_TF_CASE(1) QDKP_TF_CASE(2) QDKP_TF_CASE(3) QDKP_TF_CASE(4) QDKP_TF_CASE(5) QDKP_TF_CASE(6)
+    default: break;
   }
-  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+#undef QDKP_TF_CASE
 }
 
 // (MR, MC, threads) for a product: the smallest tile rectangles that fit 8 warps, else 16.

@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstring>
 #include <limits>
+#include <type_traits>
 #include <vector>
 
 #include "engine_dev.cuh"
@@ -354,27 +355,27 @@ __device__ bool upd_lists(const ESlot& d, int which, BlockList<T>& A, const doub
   }
 }
 
-__global__ void __launch_bounds__(kUpdThreads)
+// One launch per precision present; CTAs of the other precision's slots return at once.
+template <typename T>
+__global__ void __launch_bounds__(kUpdThreads, 2)
 e_update_kernel(const ESlot* __restrict__ S, int ns, int which) {
   extern __shared__ __align__(16) unsigned char usm_e[];
   const int k = slot_of(S, ns, blockIdx.x, &ESlot::row0);
   const ESlot& d = S[k];
+  constexpr int prec = std::is_same<T, float>::value ? QDKP_C64 : QDKP_C128;
+  if (d.prec != prec) return;
   const double2* Cf[3];
   const double2* C2[3] = {nullptr, nullptr, nullptr};
   int q, accumulate, neg;
   const long long r0 = (long long)(blockIdx.x - d.row0) * d.rows_per_cta;
   const long long r1 = min(d.n, r0 + d.rows_per_cta);
-  if (d.prec == QDKP_C64) {
-    BlockList<float> A;
-    float2 *Y, *Y2;
-    if (!upd_lists<float>(d, which, A, Cf, q, Y, accumulate, neg, C2, Y2)) return;
+  BlockList<T> A;
+  cplx<T> *Y, *Y2;
+  if (!upd_lists<T>(d, which, A, Cf, q, Y, accumulate, neg, C2, Y2)) return;
+  if constexpr (std::is_same<T, float>::value)
     update_rows_tf32(A, Cf, q, r0, r1, Y, (long long)q, accumulate, neg, usm_e, C2, Y2);
-  } else {
-    BlockList<double> A;
-    double2 *Y, *Y2;
-    if (!upd_lists<double>(d, which, A, Cf, q, Y, accumulate, neg, C2, Y2)) return;
+  else
     update_rows(A, Cf, q, r0, r1, Y, (long long)q, accumulate, neg, usm_e, C2, Y2);
-  }
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -733,10 +734,16 @@ int launch_gram_multi(qdkp_engine* e, int which, cudaStream_t st) {
 int launch_update_multi(qdkp_engine* e, int which, cudaStream_t st) {
   const bool fused = which == UP_XPNEW || which == UP_AXPNEW;
   const int P = (fused ? 3 : 1) * e->m_max, nout = fused ? 2 : 1;
-  const size_t smem = std::max(update_smem_bytes(P, e->m_max, (int)sizeof(double2), nout),
-                               update_tf32_smem_bytes(P, e->m_max, nout));
-  e_update_kernel<<<e->row_ctas, kUpdThreads, smem, st>>>(e->d_slots, e->ns, which);
-  count_launch();
+  if (e->hx_ns[0]) {
+    const size_t smem = update_smem_bytes(P, e->m_max, (int)sizeof(double2), nout);
+    e_update_kernel<double><<<e->row_ctas, kUpdThreads, smem, st>>>(e->d_slots, e->ns, which);
+    count_launch();
+  }
+  if (e->hx_ns[1]) {
+    const size_t smem = update_tf32_smem_bytes(P, e->m_max, nout);
+    e_update_kernel<float><<<e->row_ctas, kUpdThreads, smem, st>>>(e->d_slots, e->ns, which);
+    count_launch();
+  }
   QDKP_CUDA_TRY(cudaGetLastError());
   return QDKP_OK;
 }
@@ -869,7 +876,8 @@ int qdkp_engine_create(int max_slots, int device, qdkp_engine** out) {
   cudaFuncSetAttribute(e_gram_kernel<3, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
   cudaFuncSetAttribute(e_gram_kernel<3, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
   cudaFuncSetAttribute(e_gram_kernel<6, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-  cudaFuncSetAttribute(e_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+  cudaFuncSetAttribute(e_update_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+  cudaFuncSetAttribute(e_update_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
   cudaFuncSetAttribute(e_rr_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
   cudaFuncSetAttribute(e_rchol_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
   cudaFuncSetAttribute(e_pchol_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
