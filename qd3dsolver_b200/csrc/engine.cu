@@ -544,6 +544,22 @@ SlotLayout slot_layout(int64_t n, int m, int prec) {
   return L;
 }
 
+// The used slots are split into up to kEGroups groups whose ticks run on streams of their own:
+// the groups share no data, so while one group is in its latency-bound kernels (the
+// Rayleigh-Ritz eigensolve and the small Cholesky, reduction and decision kernels, one CTA per
+// slot) the other group's tall kernels fill the GPU. A slot's kernels and partitions are the
+// same in any group, so grouping changes no result.
+constexpr int kEGroups = 2;
+
+struct EGroup {
+  ESlot* d_slots = nullptr;            // this group's run of the compact slot array
+  HXSlot* d_hx = nullptr;              // [precision][phase][slot]: 2 x 4 x max_slots descriptors
+  int ns = 0, norm_ctas = 0, gram_ctas = 0, row_ctas = 0;
+  int hx_ns[2] = {0, 0}, hx_tiles[2] = {0, 0};   // per precision (QDKP_C128, QDKP_C64)
+  int m_max = 1;
+  std::vector<int> widths;             // distinct block widths among the group's slots
+};
+
 }  // namespace
 }  // namespace qdkp
 
@@ -551,19 +567,17 @@ struct qdkp_engine {
   int device = 0;
   int max_slots = 0;
   std::vector<qdkp::SlotHost> slots;
-  qdkp::ESlot* d_slots = nullptr;      // compact array of the used slots
-  qdkp::HXSlot* d_hx = nullptr;        // [precision][phase][slot]: 2 x 4 x max_slots H.X descriptors
+  qdkp::ESlot* d_slots = nullptr;      // compact array of the used slots (group after group)
+  qdkp::HXSlot* d_hx = nullptr;        // H.X descriptors, kEGroups x 8 x max_slots
   int* d_one = nullptr;                // constant 1 (skip flag)
-  std::vector<int> order;              // slot ids in compact order
-  int ns = 0, norm_ctas = 0, gram_ctas = 0, row_ctas = 0;
-  int hx_ns[2] = {0, 0}, hx_tiles[2] = {0, 0};   // per precision (QDKP_C128, QDKP_C64)
-  int maxT = 2, m_max = 1;
-  std::vector<int> widths;             // distinct block widths among the used slots
+  int ns = 0;                          // used slots
+  int ngroups = 0;
+  qdkp::EGroup grp[qdkp::kEGroups];
   bool dirty = true;
   // CUDA graph of `graph_ticks` ticks over the current slot layout, replayed by
   // qdkp_engine_step on the engine's own stream (ordered after the caller's stream by events)
-  cudaStream_t gstream = nullptr;
-  cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+  cudaStream_t gstream = nullptr, gstream2 = nullptr;   // group 0 and group 1
+  cudaEvent_t ev_in = nullptr, ev_out = nullptr, ev_fork = nullptr, ev_join = nullptr;
   cudaGraphExec_t graph = nullptr;
   int graph_ticks = 0;
   bool use_graph = true;
@@ -636,16 +650,18 @@ int read_sync(void* host, const void* dev, size_t bytes, cudaStream_t st) {
   return QDKP_OK;
 }
 
-int rebuild(qdkp_engine* e, cudaStream_t st) {
+// descriptors of group g (slots `ids`, compact-array positions from `base` on)
+int build_group(qdkp_engine* e, int g, const std::vector<int>& ids, int base, cudaStream_t st) {
+  EGroup& G = e->grp[g];
+  G = EGroup();
+  G.d_slots = e->d_slots + base;
+  G.d_hx = e->d_hx + (size_t)g * 8 * e->max_slots;
   std::vector<ESlot> compact;
   std::vector<HXSlot> hx(8 * (size_t)e->max_slots);
-  e->order.clear();
   int norm0 = 0, gram0 = 0, row0 = 0, m_max = 1;
   int tile0[2] = {0, 0}, kp[2] = {0, 0};
-
-  for (int i = 0; i < e->max_slots; ++i) {
+  for (int i : ids) {
     SlotHost& h = e->slots[i];
-    if (!h.used) continue;
     ESlot d = h.d;
     d.norm0 = norm0; norm0 += d.nparts;
     d.gram0 = gram0; gram0 += d.gparts;
@@ -654,7 +670,6 @@ int rebuild(qdkp_engine* e, cudaStream_t st) {
     compact.push_back(d);
     const int pi = d.prec == QDKP_C64 ? 1 : 0;
     const int k = kp[pi]++;
-    e->order.push_back(i);
     const qdkp_operator* op = h.op;
     m_max = std::max(m_max, d.m);
     const int tiles = apply_tiles(op->n_sites, d.m);
@@ -684,30 +699,52 @@ int rebuild(qdkp_engine* e, cudaStream_t st) {
     }
     tile0[pi] += tiles;
   }
-  e->ns = (int)compact.size();
-  e->norm_ctas = norm0; e->gram_ctas = gram0; e->row_ctas = row0;
-  for (int pi = 0; pi < 2; ++pi) { e->hx_ns[pi] = kp[pi]; e->hx_tiles[pi] = tile0[pi]; }
-  e->m_max = m_max;
-  e->widths.clear();
+  G.ns = (int)compact.size();
+  G.norm_ctas = norm0; G.gram_ctas = gram0; G.row_ctas = row0;
+  for (int pi = 0; pi < 2; ++pi) { G.hx_ns[pi] = kp[pi]; G.hx_tiles[pi] = tile0[pi]; }
+  G.m_max = m_max;
   for (const ESlot& d : compact)
-    if (std::find(e->widths.begin(), e->widths.end(), d.m) == e->widths.end()) e->widths.push_back(d.m);
-  std::sort(e->widths.begin(), e->widths.end());
-  const int RP = (6 * m_max + 7) / 8 * 8;
-  const int TR = RP / 8;
-  const int tper = (TR + kGramWarpsR - 1) / kGramWarpsR;
-  e->maxT = tper <= 2 ? 2 : tper <= 3 ? 3 : tper <= 4 ? 4 : 6;
-  if (e->ns) {
-    QDKP_CUDA_TRY(cudaMemcpyAsync(e->d_slots, compact.data(), compact.size() * sizeof(ESlot),
+    if (std::find(G.widths.begin(), G.widths.end(), d.m) == G.widths.end()) G.widths.push_back(d.m);
+  std::sort(G.widths.begin(), G.widths.end());
+  if (G.ns) {
+    QDKP_CUDA_TRY(cudaMemcpyAsync(G.d_slots, compact.data(), compact.size() * sizeof(ESlot),
                                   cudaMemcpyHostToDevice, st));
-    QDKP_CUDA_TRY(cudaMemcpyAsync(e->d_hx, hx.data(), hx.size() * sizeof(HXSlot),
+    QDKP_CUDA_TRY(cudaMemcpyAsync(G.d_hx, hx.data(), hx.size() * sizeof(HXSlot),
                                   cudaMemcpyHostToDevice, st));
+  }
+  return QDKP_OK;
+}
+
+// Split the used slots into groups, balancing rows x block width greedily in slot order.
+int rebuild(qdkp_engine* e, cudaStream_t st) {
+  std::vector<int> ids[kEGroups];
+  double load[kEGroups] = {};
+  int used = 0;
+  for (int i = 0; i < e->max_slots; ++i) used += e->slots[i].used ? 1 : 0;
+  const int ng = std::max(1, std::min(kEGroups, used));
+  for (int i = 0; i < e->max_slots; ++i) {
+    const SlotHost& h = e->slots[i];
+    if (!h.used) continue;
+    int g = 0;
+    for (int c = 1; c < ng; ++c) if (load[c] < load[g]) g = c;
+    ids[g].push_back(i);
+    load[g] += (double)h.d.n * h.d.m;
+  }
+  e->ns = used;
+  e->ngroups = ng;
+  int base = 0;
+  for (int g = 0; g < kEGroups; ++g) {
+    if (g >= ng) { e->grp[g] = EGroup(); continue; }
+    const int rc = build_group(e, g, ids[g], base, st);
+    if (rc) return rc;
+    base += (int)ids[g].size();
   }
   e->dirty = false;
   return QDKP_OK;
 }
 
-int launch_gram_multi(qdkp_engine* e, int which, cudaStream_t st) {
-  for (int m : e->widths) {
+int launch_gram_multi(const EGroup& G, int which, cudaStream_t st) {
+  for (int m : G.widths) {
     int P = m, Q = m;
     if (which == GR_BA) { P = 3 * m; Q = 2 * m; }
     else if (which == GR_BB) { P = 2 * m; Q = m; }
@@ -716,32 +753,32 @@ int launch_gram_multi(qdkp_engine* e, int which, cudaStream_t st) {
                                  gram_smem_bytes(P, Q, (int)sizeof(float2)));
     int MR, MC, threads;
     gram_shape(P, Q, MR, MC, threads);
-    if (MR == 3 && MC == 3) e_gram_kernel<3, 3><<<e->gram_ctas, threads, smem, st>>>(e->d_slots, e->ns, which, m);
-    else if (MR == 3) e_gram_kernel<3, 6><<<e->gram_ctas, threads, smem, st>>>(e->d_slots, e->ns, which, m);
-    else e_gram_kernel<6, 6><<<e->gram_ctas, threads, smem, st>>>(e->d_slots, e->ns, which, m);
+    if (MR == 3 && MC == 3) e_gram_kernel<3, 3><<<G.gram_ctas, threads, smem, st>>>(G.d_slots, G.ns, which, m);
+    else if (MR == 3) e_gram_kernel<3, 6><<<G.gram_ctas, threads, smem, st>>>(G.d_slots, G.ns, which, m);
+    else e_gram_kernel<6, 6><<<G.gram_ctas, threads, smem, st>>>(G.d_slots, G.ns, which, m);
     count_launch();
   }
-  const int RP = (6 * e->m_max + 7) / 8 * 8;
+  const int RP = (6 * G.m_max + 7) / 8 * 8;
   const int elems = RP * RP;
-  e_gram_reduce1<<<dim3((elems + 255) / 256, kEGramSplit, e->ns), 256, 0, st>>>(e->d_slots, which);
-  const int pq = (3 * e->m_max) * (3 * e->m_max);
-  e_gram_reduce2<<<dim3((pq + 127) / 128, e->ns), 128, 0, st>>>(e->d_slots, which);
+  e_gram_reduce1<<<dim3((elems + 255) / 256, kEGramSplit, G.ns), 256, 0, st>>>(G.d_slots, which);
+  const int pq = (3 * G.m_max) * (3 * G.m_max);
+  e_gram_reduce2<<<dim3((pq + 127) / 128, G.ns), 128, 0, st>>>(G.d_slots, which);
   count_launch(2);
   QDKP_CUDA_TRY(cudaGetLastError());
   return QDKP_OK;
 }
 
-int launch_update_multi(qdkp_engine* e, int which, cudaStream_t st) {
+int launch_update_multi(const EGroup& G, int which, cudaStream_t st) {
   const bool fused = which == UP_XPNEW || which == UP_AXPNEW;
-  const int P = (fused ? 3 : 1) * e->m_max, nout = fused ? 2 : 1;
-  if (e->hx_ns[0]) {
-    const size_t smem = update_smem_bytes(P, e->m_max, (int)sizeof(double2), nout);
-    e_update_kernel<double><<<e->row_ctas, kUpdThreads, smem, st>>>(e->d_slots, e->ns, which);
+  const int P = (fused ? 3 : 1) * G.m_max, nout = fused ? 2 : 1;
+  if (G.hx_ns[0]) {
+    const size_t smem = update_smem_bytes(P, G.m_max, (int)sizeof(double2), nout);
+    e_update_kernel<double><<<G.row_ctas, kUpdThreads, smem, st>>>(G.d_slots, G.ns, which);
     count_launch();
   }
-  if (e->hx_ns[1]) {
-    const size_t smem = update_tf32_smem_bytes(P, e->m_max, nout);
-    e_update_kernel<float><<<e->row_ctas, kUpdThreads, smem, st>>>(e->d_slots, e->ns, which);
+  if (G.hx_ns[1]) {
+    const size_t smem = update_tf32_smem_bytes(P, G.m_max, nout);
+    e_update_kernel<float><<<G.row_ctas, kUpdThreads, smem, st>>>(G.d_slots, G.ns, which);
     count_launch();
   }
   QDKP_CUDA_TRY(cudaGetLastError());
@@ -749,55 +786,56 @@ int launch_update_multi(qdkp_engine* e, int which, cudaStream_t st) {
 }
 
 // one H.X phase of a tick: a multi-slot launch per precision present
-int launch_hx_phase(qdkp_engine* e, int phase, cudaStream_t st) {
+int launch_hx_phase(const qdkp_engine* e, const EGroup& G, int phase, cudaStream_t st) {
   for (int pi = 0; pi < 2; ++pi) {
-    if (!e->hx_ns[pi]) continue;
-    int rc = launch_apply_multi(e->d_hx + ((size_t)pi * 4 + phase) * e->max_slots, e->hx_ns[pi],
-                                e->hx_tiles[pi], pi ? QDKP_C64 : QDKP_C128, st);
+    if (!G.hx_ns[pi]) continue;
+    int rc = launch_apply_multi(G.d_hx + ((size_t)pi * 4 + phase) * e->max_slots, G.hx_ns[pi],
+                                G.hx_tiles[pi], pi ? QDKP_C64 : QDKP_C128, st);
     if (rc) return rc;
   }
   return QDKP_OK;
 }
 
-int tick(qdkp_engine* e, cudaStream_t st) {
-  const int ns = e->ns;
+// one LOBPCG iteration of every running slot of group G
+int tick(const qdkp_engine* e, const EGroup& G, cudaStream_t st) {
+  const int ns = G.ns;
   if (!ns) return QDKP_OK;
   int rc;
 #define ETRY(x) do { rc = (x); if (rc != QDKP_OK) return rc; } while (0)
-  const size_t small_smem = 2 * (size_t)e->m_max * e->m_max * sizeof(double2);
-  const size_t rr_smem = 2 * (size_t)(3 * e->m_max) * (3 * e->m_max) * sizeof(double2);
-  e_norm_kernel<<<e->norm_ctas, kTallThreads, 0, st>>>(e->d_slots, ns);
-  e_decide_kernel<<<ns, 32, 0, st>>>(e->d_slots);
-  e_row_kernel<<<e->row_ctas, kTallThreads, 0, st>>>(e->d_slots, ns, RW_COPYBEST);
-  e_row_kernel<<<e->row_ctas, kTallThreads, 0, st>>>(e->d_slots, ns, RW_RESID);
+  const size_t small_smem = 2 * (size_t)G.m_max * G.m_max * sizeof(double2);
+  const size_t rr_smem = 2 * (size_t)(3 * G.m_max) * (3 * G.m_max) * sizeof(double2);
+  e_norm_kernel<<<G.norm_ctas, kTallThreads, 0, st>>>(G.d_slots, ns);
+  e_decide_kernel<<<ns, 32, 0, st>>>(G.d_slots);
+  e_row_kernel<<<G.row_ctas, kTallThreads, 0, st>>>(G.d_slots, ns, RW_COPYBEST);
+  e_row_kernel<<<G.row_ctas, kTallThreads, 0, st>>>(G.d_slots, ns, RW_RESID);
   count_launch(4);
   QDKP_CUDA_TRY(cudaGetLastError());
-  ETRY(launch_hx_phase(e, 0, st));
-  ETRY(launch_hx_phase(e, 1, st));
-  e_row_kernel<<<e->row_ctas, kTallThreads, 0, st>>>(e->d_slots, ns, RW_GATHERP);
+  ETRY(launch_hx_phase(e, G, 0, st));
+  ETRY(launch_hx_phase(e, G, 1, st));
+  e_row_kernel<<<G.row_ctas, kTallThreads, 0, st>>>(G.d_slots, ns, RW_GATHERP);
   count_launch();
-  ETRY(launch_gram_multi(e, GR_XR, st));
-  ETRY(launch_update_multi(e, UP_RPROJ, st));
-  ETRY(launch_gram_multi(e, GR_RR, st));
-  e_rchol_kernel<<<ns, kSmallThreads, small_smem, st>>>(e->d_slots);
+  ETRY(launch_gram_multi(G, GR_XR, st));
+  ETRY(launch_update_multi(G, UP_RPROJ, st));
+  ETRY(launch_gram_multi(G, GR_RR, st));
+  e_rchol_kernel<<<ns, kSmallThreads, small_smem, st>>>(G.d_slots);
   count_launch();
-  ETRY(launch_update_multi(e, UP_RNORM, st));
-  ETRY(launch_hx_phase(e, 2, st));
-  ETRY(launch_hx_phase(e, 3, st));
-  ETRY(launch_gram_multi(e, GR_PP, st));
-  e_pchol_kernel<<<ns, kSmallThreads, small_smem, st>>>(e->d_slots);
+  ETRY(launch_update_multi(G, UP_RNORM, st));
+  ETRY(launch_hx_phase(e, G, 2, st));
+  ETRY(launch_hx_phase(e, G, 3, st));
+  ETRY(launch_gram_multi(G, GR_PP, st));
+  e_pchol_kernel<<<ns, kSmallThreads, small_smem, st>>>(G.d_slots);
   count_launch();
-  ETRY(launch_update_multi(e, UP_PNORM, st));
-  ETRY(launch_update_multi(e, UP_APNORM, st));
-  ETRY(launch_gram_multi(e, GR_BA, st));
-  ETRY(launch_gram_multi(e, GR_BB, st));
-  ETRY(launch_gram_multi(e, GR_WW, st));
-  ETRY(launch_gram_multi(e, GR_WAW, st));
-  e_rr_kernel<<<ns, kSmallThreads, rr_smem, st>>>(e->d_slots);
+  ETRY(launch_update_multi(G, UP_PNORM, st));
+  ETRY(launch_update_multi(G, UP_APNORM, st));
+  ETRY(launch_gram_multi(G, GR_BA, st));
+  ETRY(launch_gram_multi(G, GR_BB, st));
+  ETRY(launch_gram_multi(G, GR_WW, st));
+  ETRY(launch_gram_multi(G, GR_WAW, st));
+  e_rr_kernel<<<ns, kSmallThreads, rr_smem, st>>>(G.d_slots);
   count_launch();
   QDKP_CUDA_TRY(cudaGetLastError());
-  ETRY(launch_update_multi(e, UP_XPNEW, st));
-  ETRY(launch_update_multi(e, UP_AXPNEW, st));
+  ETRY(launch_update_multi(G, UP_XPNEW, st));
+  ETRY(launch_update_multi(G, UP_AXPNEW, st));
 #undef ETRY
   return QDKP_OK;
 }
@@ -807,19 +845,41 @@ int tick(qdkp_engine* e, cudaStream_t st) {
 
 namespace qdkp {
 
+// `ticks` ticks of every group: group 0 on `st`, group 1 on the engine's second stream, forked
+// from and joined back to `st` (the groups share no data, so their ticks interleave freely)
+static int run_ticks(qdkp_engine* e, int ticks, cudaStream_t st) {
+  int rc = QDKP_OK;
+  if (e->ngroups > 1) {
+    QDKP_CUDA_TRY(cudaEventRecord(e->ev_fork, st));
+    QDKP_CUDA_TRY(cudaStreamWaitEvent(e->gstream2, e->ev_fork, 0));
+  }
+  for (int t = 0; t < ticks && rc == QDKP_OK; ++t) rc = tick(e, e->grp[0], st);
+  for (int t = 0; t < ticks && rc == QDKP_OK && e->ngroups > 1; ++t) rc = tick(e, e->grp[1], e->gstream2);
+  if (e->ngroups > 1) {
+    // join even after an error, so that a capture in progress ends with no stream left forked
+    const cudaError_t r1 = cudaEventRecord(e->ev_join, e->gstream2);
+    const cudaError_t r2 = cudaStreamWaitEvent(st, e->ev_join, 0);
+    if (rc == QDKP_OK && (r1 != cudaSuccess || r2 != cudaSuccess)) {
+      set_error(std::string("engine stream join: ") + cudaGetErrorString(r1 != cudaSuccess ? r1 : r2));
+      rc = QDKP_ERR_CUDA;
+    }
+  }
+  return rc;
+}
+
 static void drop_graph(qdkp_engine* e) {
   if (e->graph) cudaGraphExecDestroy(e->graph);
   e->graph = nullptr;
   e->graph_ticks = 0;
 }
 
-// Capture `ticks` ticks of the current layout into e->graph (on the engine's stream).
+// Capture `ticks` ticks of the current layout into e->graph (from the engine's stream; the
+// second group's branch is forked off and joined back inside the graph).
 static int capture_ticks(qdkp_engine* e, int ticks) {
   drop_graph(e);
   QDKP_CUDA_TRY(cudaStreamBeginCapture(e->gstream, cudaStreamCaptureModeThreadLocal));
-  int rc = QDKP_OK;
   const long long l0 = launches_so_far();
-  for (int t = 0; t < ticks && rc == QDKP_OK; ++t) rc = tick(e, e->gstream);
+  const int rc = run_ticks(e, ticks, e->gstream);
   // captured launches are not executions: take them back off the counter
   const long long captured = launches_so_far() - l0;
   count_launch((int)-captured);
@@ -856,18 +916,24 @@ int qdkp_engine_create(int max_slots, int device, qdkp_engine** out) {
   e->max_slots = max_slots;
   e->slots.resize(max_slots);
   cudaError_t err = cudaMalloc(&e->d_slots, sizeof(ESlot) * max_slots);
-  if (err == cudaSuccess) err = cudaMalloc(&e->d_hx, sizeof(HXSlot) * 8 * max_slots);
+  if (err == cudaSuccess) err = cudaMalloc(&e->d_hx, sizeof(HXSlot) * kEGroups * 8 * max_slots);
   if (err == cudaSuccess) err = cudaMalloc(&e->d_one, sizeof(int));
   if (err == cudaSuccess) { const int one = 1; err = cudaMemcpy(e->d_one, &one, sizeof(int), cudaMemcpyHostToDevice); }
   if (err == cudaSuccess) err = cudaStreamCreateWithFlags(&e->gstream, cudaStreamNonBlocking);
+  if (err == cudaSuccess) err = cudaStreamCreateWithFlags(&e->gstream2, cudaStreamNonBlocking);
   if (err == cudaSuccess) err = cudaEventCreateWithFlags(&e->ev_in, cudaEventDisableTiming);
   if (err == cudaSuccess) err = cudaEventCreateWithFlags(&e->ev_out, cudaEventDisableTiming);
+  if (err == cudaSuccess) err = cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming);
+  if (err == cudaSuccess) err = cudaEventCreateWithFlags(&e->ev_join, cudaEventDisableTiming);
   if (err != cudaSuccess) {
     set_error(std::string("engine tables: ") + cudaGetErrorString(err));
     cudaFree(e->d_slots); cudaFree(e->d_hx); cudaFree(e->d_one);
     if (e->gstream) cudaStreamDestroy(e->gstream);
+    if (e->gstream2) cudaStreamDestroy(e->gstream2);
     if (e->ev_in) cudaEventDestroy(e->ev_in);
     if (e->ev_out) cudaEventDestroy(e->ev_out);
+    if (e->ev_fork) cudaEventDestroy(e->ev_fork);
+    if (e->ev_join) cudaEventDestroy(e->ev_join);
     delete e;
     return QDKP_ERR_CUDA;
   }
@@ -890,8 +956,11 @@ int qdkp_engine_destroy(qdkp_engine* e) {
   cudaSetDevice(e->device);
   drop_graph(e);
   if (e->gstream) { cudaStreamSynchronize(e->gstream); cudaStreamDestroy(e->gstream); }
+  if (e->gstream2) { cudaStreamSynchronize(e->gstream2); cudaStreamDestroy(e->gstream2); }
   if (e->ev_in) cudaEventDestroy(e->ev_in);
   if (e->ev_out) cudaEventDestroy(e->ev_out);
+  if (e->ev_fork) cudaEventDestroy(e->ev_fork);
+  if (e->ev_join) cudaEventDestroy(e->ev_join);
   cudaFree(e->d_slots);
   cudaFree(e->d_hx);
   cudaFree(e->d_one);
@@ -1007,13 +1076,7 @@ int qdkp_engine_step(qdkp_engine* e, int ticks, void* stream) {
     if (rc) return rc;
   }
   if (ticks == 0 || e->ns == 0) return QDKP_OK;
-  if (!e->use_graph) {
-    for (int t = 0; t < ticks; ++t) {
-      int rc = tick(e, st);
-      if (rc) return rc;
-    }
-    return QDKP_OK;
-  }
+  if (!e->use_graph) return run_ticks(e, ticks, st);
   // the tick sequence is fixed for a slot layout: replay it as one graph launch
   if (!e->graph || e->graph_ticks != ticks) {
     QDKP_CUDA_TRY(cudaStreamSynchronize(st));   // descriptor uploads of rebuild() landed

@@ -70,19 +70,23 @@ def test_engine_alone_equals_mix(ops):
 
 
 def test_graph_replay_equals_direct_launches(ops):
-    """Ticks replayed from a captured CUDA graph give exactly the directly launched result."""
+    """Ticks replayed from a captured CUDA graph give exactly the directly launched result,
+    with one solve (one slot group) and with two (two groups on two streams)."""
     from qd3dsolver_b200 import serving
-    H, ref = ops['small'], ops['meta']['interior_vb']
-    out = []
-    for graphs in (True, False):
-        eng = serving.Engine(2, graphs=graphs)
-        r = serving.Request(H, k=4, sigma=ref['sigma'], tol=1e-9, maxiter=4000)
-        serving.solve_batch([r], engine=eng, ticks_per_poll=6)
-        eng.close()
-        out.append(r.result)
-    assert out[0]['iterations'] == out[1]['iterations']
-    assert np.abs(out[0]['E'] - out[1]['E']).max() <= 1e-13
-    assert np.abs(out[0]['residuals'] - out[1]['residuals']).max() <= 1e-13
+    H, meta = ops['small'], ops['meta']
+    for bands in (('interior_vb',), ('interior_vb', 'interior_cb')):
+        out = []
+        for graphs in (True, False):
+            eng = serving.Engine(2, graphs=graphs)
+            rs = [serving.Request(H, k=4, sigma=meta[b]['sigma'], tol=1e-9, maxiter=4000)
+                  for b in bands]
+            serving.solve_batch(rs, engine=eng, ticks_per_poll=6)
+            eng.close()
+            out.append([r.result for r in rs])
+        for a, b in zip(*out):
+            assert a['iterations'] == b['iterations']
+            assert np.abs(a['E'] - b['E']).max() <= 1e-13
+            assert np.abs(a['residuals'] - b['residuals']).max() <= 1e-13
 
 
 def test_mixed_precision_reaches_the_reference_levels(ops):
