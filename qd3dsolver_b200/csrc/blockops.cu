@@ -285,7 +285,7 @@ int launch_update(const BlockList<T>& A, const double2* const* C, int q, long lo
   for (int b = 0; b < 3; ++b) cl.c[b] = b < A.nblk ? C[b] : nullptr;
   const int P = A.total();
   const size_t smem = std::is_same<T, float>::value ? update_tf32_smem_bytes(P, q)
-                                                    : update_smem_bytes(P, q, (int)sizeof(cplx<T>));
+                                                    : update_smem_bytes(P, q);
   static bool attr = false;
   if (!attr) {
     QDKP_CUDA_TRY(cudaFuncSetAttribute(update_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -326,153 +326,177 @@ static __device__ int block_eigh(const double2* __restrict__ A, const double2* _
 
 
 
-// Y' = A' C'' on the FP64 tensor cores for rows [r0, r1), with A' (rows x 2P) the real view of
-// [A_0 | A_1 | A_2] and C'' (2P x 2q) the real representation of the stacked complex
-// coefficients: C''_{2i,2j} = Re C_ij, C''_{2i,2j+1} = Im C_ij, C''_{2i+1,2j} = -Im C_ij,
-// C''_{2i+1,2j+1} = Re C_ij (negated when neg). Rows stream through shared memory in chunks of
-// kUpdChunk (one 8-row m8n8k4 tile per warp), double buffered with cp.async; a chunk is staged
-// completely before any of its rows is written, and a CTA owns its rows, so Y may alias one of
-// the inputs.
+// Y' = A' C'' for rows [r0, r1) of complex128 blocks on the FP64 MMA (mma.sync.m8n8k4.f64),
+// with A' (rows x 2P) the real view of [A_0 | A_1 | A_2] and C'' (2P x 2q) the real
+// representation of the stacked complex coefficients: C''_{2i,2j} = Re C_ij,
+// C''_{2i,2j+1} = Im C_ij, C''_{2i+1,2j} = -Im C_ij, C''_{2i+1,2j+1} = Re C_ij (negated when
+// neg). Nothing is staged: a warp owns 8-row M tiles (tiles warp, warp + warps, ... of the CTA's
+// rows) and loads its A fragments from global memory into registers, a ring of k-step pairs
+// ahead of the MMAs. The k order is permuted over pairs of k steps: a pair covers complex
+// columns c0 .. c0 + 3 of one block, MMA k = t of its first step is Re A[.][c0 + t] and of its
+// second step Im A[.][c0 + t] (g = lane / 4, t = lane % 4), so a lane's A values of the pair are
+// one 16-byte load, A[row g][c0 + t]. C'' is stored in that order as one 16-byte word per (pair,
+// 8-column N tile, lane): {C''[2 (c0 + t)][n g], C''[2 (c0 + t) + 1][n g]}. A row is read (by
+// the four lanes of its quad) before any of its outputs is written and no other warp touches
+// it, so Y may alias an input.
 constexpr int kUpdRows = 8;
 constexpr int kUpdThreads = 256;
 constexpr int kUpdWarps = kUpdThreads / 32;
-constexpr int kUpdChunk = kUpdRows * kUpdWarps;     // 64 rows per stage
+constexpr int kUpdChunk = kUpdRows * kUpdWarps;     // row granularity of a CTA's span
+constexpr int kDmRing = 8;                          // k-step pairs in flight per warp
 
+// k-step pairs of a list of at most three blocks with P columns in all (ceil(cols / 4) each)
+__host__ __device__ __forceinline__ int dmma_pairs_bound(int P) { return (P + 3) / 4 + 2; }
+__host__ __device__ __forceinline__ size_t update_smem_bytes(int P, int q, int nout = 1) {
+  return (size_t)nout * dmma_pairs_bound(P) * ((q + 3) / 4) * 32 * sizeof(double2);
+}
 
-template <typename T>
-static __device__ void update_rows(const BlockList<T>& A, const double2* const* C, int q,
-                                   long long r0, long long r1, cplx<T>* Y, long long ldy,
-                                   int accumulate, int neg, unsigned char* smem,
-                                   const double2* const* C2 = nullptr, cplx<T>* Y2 = nullptr) {
-  // optional second output Y2 = A C2 (same rows, same q; a NULL block of C2 is zero): the
-  // fused X / P Ritz update reads [X | R | P] once for both
-  const int P = A.total();
-  const int KP = 2 * P;
-  const int KPp = (KP + 3) / 4 * 4;
-  const int NQ = (2 * q + 7) / 8 * 8;
-  const int nout = Y2 ? 2 : 1;
-  double* sC = reinterpret_cast<double*>(smem);
-  double* sC2 = sC + (size_t)(KPp + 4) * NQ;
-  const size_t coef_bytes = (size_t)nout * (KPp + 4) * NQ * sizeof(double);
-  cplx<T>* stage0 = reinterpret_cast<cplx<T>*>(smem + coef_bytes);
-  const size_t stage_elems = (size_t)kUpdChunk * P;
-  const int NS = stage_count_fit(stage_elems * sizeof(cplx<T>), dyn_smem_bytes() - coef_bytes);
+// one k-step pair of an update's A list: columns c0 .. c0 + 3 of a block (p points at c0)
+struct DmKStep {
+  const double2* p;
+  int ld;
+  int rem;          // columns of the block from c0 on
+};
+
+template <int NT, int NOUT, bool ACC>
+static __device__ __forceinline__ void update_dmma_core(const DmKStep* __restrict__ sK,
+                                                        const double2* __restrict__ sB, int KS,
+                                                        int q, long long r0, long long r1,
+                                                        double2* Y, double2* Y2, long long ldy) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const double sg = neg ? -1.0 : 1.0;
-  int off[3], kst[3];
-  int tot = 0;
-  for (int b = 0; b < A.nblk; ++b) { off[b] = tot; tot += A.cols[b]; }
-  // KPp + 4 rows: a k step may run up to 3 rows past the last block (multiplied by zeros)
-  for (int e = threadIdx.x; e < nout * (KPp + 4) * NQ; e += blockDim.x) sC[e] = 0.0;
-  __syncthreads();
-  for (int o = 0; o < nout; ++o) {
-    const double2* const* Co = o ? C2 : C;
-    double* so = o ? sC2 : sC;
-    for (int e = threadIdx.x; e < P * q; e += blockDim.x) {
-      const int i = e / q, j = e - i * q;
-      int b = 0;
-      while (b < A.nblk - 1 && i >= off[b] + A.cols[b]) ++b;
-      if (!Co[b]) continue;
-      const double2 c = Co[b][(i - off[b]) * q + j];
-      so[(2 * i) * NQ + 2 * j] = sg * c.x;
-      so[(2 * i) * NQ + 2 * j + 1] = sg * c.y;
-      so[(2 * i + 1) * NQ + 2 * j] = -sg * c.y;
-      so[(2 * i + 1) * NQ + 2 * j + 1] = sg * c.x;
-    }
-  }
-  for (int b = 0; b < A.nblk; ++b) kst[b] = off[b] * kUpdChunk;   // block start in a stage
-  const int g = lane >> 2, t4 = lane & 3;
-  const int NT = NQ / 8;
-  const long long nrows = r1 - r0;
-  const int nchunks = (int)((nrows + kUpdChunk - 1) / kUpdChunk);
-  // the flat copy of gram_copy_rows with kUpdChunk rows per block run
-  auto stage_rows = [&](long long r, int nr, cplx<T>* dst) {
-    for (int b = 0; b < A.nblk; ++b) {
-      const int cols = A.cols[b];
-      const int units = nr * cols;
-      const cplx<T>* src = A.p[b] + r * A.ld[b];
-      cplx<T>* d = dst + kst[b];
-      if (sizeof(cplx<T>) == 8 && A.ld[b] == cols && (units & 1) == 0 &&
-          ((uintptr_t)src & 15) == 0 && ((uintptr_t)d & 15) == 0) {
-        for (int u = 2 * threadIdx.x; u < units; u += 2 * blockDim.x) {
-          const unsigned sa = (unsigned)__cvta_generic_to_shared(d + u);
-          asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" :: "r"(sa), "l"(src + u) : "memory");
+  const int g = lane >> 2, t = lane & 3;
+  const int nw = blockDim.x >> 5;
+  const int ntiles = (int)((r1 - r0 + kUpdRows - 1) / kUpdRows);
+  const int mine = ntiles > warp ? (ntiles - warp + nw - 1) / nw : 0;
+  const int nitems = mine * KS;
+  if (nitems == 0) return;
+  constexpr int RING = NT * NOUT <= 6 ? kDmRing : kDmRing / 2;
+  double2 fa[RING];
+  int l_tile = warp, l_s = 0;
+  auto fetch = [&](double2& xa) {
+    const DmKStep k = sK[l_s];
+    const long long ra = r0 + (long long)l_tile * kUpdRows + g;
+    xa = (t < k.rem && ra < r1) ? __ldcs(k.p + ra * k.ld + t) : make_double2(0.0, 0.0);
+    if (++l_s == KS) { l_s = 0; l_tile += nw; }
+  };
+#pragma unroll
+  for (int d = 0; d < RING; ++d)
+    if (d < nitems) fetch(fa[d]);
+  double acc[NOUT][NT][2];
+  double2 yo[ACC ? NT : 1];
+#pragma unroll
+  for (int o = 0; o < NOUT; ++o)
+#pragma unroll
+    for (int j = 0; j < NT; ++j) acc[o][j][0] = acc[o][j][1] = 0.0;
+  int c_s = 0, c_tile = warp;
+  for (int base = 0; base < nitems; base += RING) {
+#pragma unroll
+    for (int d = 0; d < RING; ++d) {
+      const int it = base + d;
+      if (it >= nitems) break;
+      const double2 a = fa[d];
+      if (it + RING < nitems) fetch(fa[d]);
+      const long long ra = r0 + (long long)c_tile * kUpdRows + g;
+      if (ACC && c_s == 0) {
+#pragma unroll
+        for (int j = 0; j < NT; ++j) {
+          const int col = j * 4 + t;
+          yo[j] = (col < q && ra < r1) ? Y[ra * ldy + col] : make_double2(0.0, 0.0);
         }
-        continue;
       }
-      for (int u = threadIdx.x; u < units; u += blockDim.x) {
-        const int rr = A.ld[b] == cols ? 0 : u / cols;
-        const cplx<T>* gp = A.ld[b] == cols ? src + u : src + (long long)rr * A.ld[b] + (u - rr * cols);
-        const unsigned sa = (unsigned)__cvta_generic_to_shared(d + u);
-        if (sizeof(cplx<T>) == 16)
-          asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" :: "r"(sa), "l"(gp) : "memory");
-        else
-          asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" :: "r"(sa), "l"(gp) : "memory");
+      const double2* bp = sB + (size_t)c_s * NT * 32 + lane;
+#pragma unroll
+      for (int j = 0; j < NT; ++j) {
+        const double2 b = bp[j * 32];
+        dmma(acc[0][j][0], acc[0][j][1], a.x, b.x);
+        dmma(acc[0][j][0], acc[0][j][1], a.y, b.y);
+        if (NOUT == 2) {
+          const double2 b2 = bp[(size_t)KS * NT * 32 + j * 32];
+          dmma(acc[NOUT - 1][j][0], acc[NOUT - 1][j][1], a.x, b2.x);
+          dmma(acc[NOUT - 1][j][0], acc[NOUT - 1][j][1], a.y, b2.y);
+        }
       }
-    }
-  };
-  auto issue = [&](int c) {
-    if (c < nchunks) {
-      const long long rn = r0 + (long long)c * kUpdChunk;
-      stage_rows(rn, (int)min((long long)kUpdChunk, r1 - rn), stage0 + (size_t)(c % NS) * stage_elems);
-    }
-    asm volatile("cp.async.commit_group;\n" ::: "memory");
-  };
-  for (int c = 0; c < NS - 1; ++c) issue(c);
-  for (int ch = 0; ch < nchunks; ++ch) {
-    const long long rc = r0 + (long long)ch * kUpdChunk;
-    const int rows = (int)min((long long)kUpdChunk, r1 - rc);
-    // chunk ch has landed once at most NS - 2 groups are pending; the barrier also means every
-    // warp is done with chunk ch - 1, whose stage the next copy reuses
-    cp_async_wait_pending(NS - 2);
-    __syncthreads();
-    issue(ch + NS - 1);
-    const int tr = warp * kUpdRows;             // this warp's 8-row tile in the chunk
-    if (tr < rows) {
-      const T* sr = reinterpret_cast<const T*>(stage0 + (size_t)(ch % NS) * stage_elems);
-      const int row = tr + g;
-      const bool rok = row < rows;
-      const long long rowg = rc + row;
-      double acc[6][2], acc2[6][2];
+      if (++c_s == KS) {
 #pragma unroll
-      for (int j = 0; j < 6; ++j) {
-        const int col = j * 4 + t4;
-        cplx<T> y0 = czero<T>();
-        if (accumulate && j < NT && col < q && rok) y0 = Y[rowg * ldy + col];
-        acc[j][0] = (double)y0.x; acc[j][1] = (double)y0.y;
-        acc2[j][0] = 0.0; acc2[j][1] = 0.0;
-      }
-      // A fragment of an m8n8k4 MMA: lane (g, t4) holds A'[row g][k0 + t4]
-      int kbase = 0;
-      for (int b = 0; b < A.nblk; ++b) {
-        const int kb = 2 * A.cols[b];
-        const T* rs = sr + 2 * kst[b] + (rok ? row : 0) * kb;
-        for (int k = 0; k < kb; k += 4) {
-          const double a = (rok && k + t4 < kb) ? (double)rs[k + t4] : 0.0;
-          const double* cr = sC + (kbase + k + t4) * NQ + g;
-#pragma unroll
-          for (int j = 0; j < 6; ++j)
-            if (j < NT) dmma(acc[j][0], acc[j][1], a, cr[j * 8]);
-          if (Y2) {
-            const double* cr2 = sC2 + (kbase + k + t4) * NQ + g;
-#pragma unroll
-            for (int j = 0; j < 6; ++j)
-              if (j < NT) dmma(acc2[j][0], acc2[j][1], a, cr2[j * 8]);
+        for (int j = 0; j < NT; ++j) {
+          const int col = j * 4 + t;
+          if (col < q && ra < r1) {
+            double2 v = make_double2(acc[0][j][0], acc[0][j][1]);
+            if (ACC) { v.x += yo[j].x; v.y += yo[j].y; }
+            Y[ra * ldy + col] = v;
+            if (NOUT == 2) Y2[ra * ldy + col] = make_double2(acc[NOUT - 1][j][0], acc[NOUT - 1][j][1]);
           }
-        }
-        kbase += kb;
-      }
 #pragma unroll
-      for (int j = 0; j < 6; ++j) {
-        const int col = j * 4 + t4;
-        if (j < NT && col < q && rok) {
-          Y[rowg * ldy + col] = mk<T>((T)acc[j][0], (T)acc[j][1]);
-          if (Y2) Y2[rowg * ldy + col] = mk<T>((T)acc2[j][0], (T)acc2[j][1]);
+          for (int o = 0; o < NOUT; ++o) acc[o][j][0] = acc[o][j][1] = 0.0;
         }
+        c_s = 0;
+        c_tile += nw;
       }
     }
   }
-  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
+// Y (+)= sg A C over rows [r0, r1) and, with C2/Y2, Y2 = sg A C2 (one pass over A; the fused
+// X / P Ritz update reads [X | R | P] once for both). C[b] is the cols_b x q row-major
+// coefficient block of A's block b (NULL: the block does not enter); q <= kMaxBlock. Called by
+// every thread of the CTA; smem holds update_smem_bytes. The two-output form that also
+// accumulates into Y takes two passes over A, so there Y must not alias an input.
+static __device__ void update_rows(const BlockList<double>& A, const double2* const* C, int q,
+                                   long long r0, long long r1, double2* Y, long long ldy,
+                                   int accumulate, int neg, unsigned char* smem,
+                                   const double2* const* C2 = nullptr, double2* Y2 = nullptr) {
+  __shared__ int2 sK[kMaxSmall / 4 + 3];
+  __shared__ DmKStep sKp[kMaxSmall / 4 + 3];
+  __shared__ int sKS;
+  const int nout = Y2 ? 2 : 1;
+  const int NT = (q + 3) / 4;
+  if (threadIdx.x == 0) {
+    int s = 0;
+    for (int b = 0; b < A.nblk; ++b)
+      for (int c0 = 0; c0 < A.cols[b]; c0 += 4) {
+        sKp[s].p = A.p[b] + c0; sKp[s].ld = (int)A.ld[b]; sKp[s].rem = A.cols[b] - c0;
+        sK[s++] = make_int2(b, c0);
+      }
+    sKS = s;
+  }
+  __syncthreads();
+  const int KS = sKS;
+  double2* sB = reinterpret_cast<double2*>(smem);
+  const double sg = neg ? -1.0 : 1.0;
+  const int per_out = KS * NT * 32;
+  for (int e = threadIdx.x; e < nout * per_out; e += blockDim.x) {
+    const int o = e / per_out, r = e - o * per_out;
+    const int s = r / (NT * 32), r2 = r - s * NT * 32;
+    const int j = r2 >> 5, ln = r2 & 31;
+    const int gg = ln >> 2, tt = ln & 3;
+    const int2 k = sK[s];
+    const int cols = k.x == 0 ? A.cols[0] : k.x == 1 ? A.cols[1] : A.cols[2];
+    const double2* Cb = (o ? C2 : C)[k.x];
+    const int i = k.y + tt, jj = j * 4 + (gg >> 1);
+    double2 w = make_double2(0.0, 0.0);
+    if (Cb && i < cols && jj < q) {
+      const double2 c = Cb[(size_t)i * q + jj];
+      const double re = sg * c.x, im = sg * c.y;
+      if (gg & 1) w = make_double2(im, re);      // C''[2i][2jj+1], C''[2i+1][2jj+1]
+      else w = make_double2(re, -im);            // C''[2i][2jj],   C''[2i+1][2jj]
+    }
+    sB[e] = w;
+  }
+  __syncthreads();
+#define QDKP_DM_CASE(nt)                                                                          \
+  case nt:                                                                                        \
+    if (nout == 2 && accumulate) {                                                                \
+      update_dmma_core<nt, 1, true>(sKp, sB, KS, q, r0, r1, Y, Y2, ldy);                          \
+      update_dmma_core<nt, 1, false>(sKp, sB + per_out, KS, q, r0, r1, Y2, Y2, ldy);              \
+    } else if (nout == 2) update_dmma_core<nt, 2, false>(sKp, sB, KS, q, r0, r1, Y, Y2, ldy);     \
+    else if (accumulate) update_dmma_core<nt, 1, true>(sKp, sB, KS, q, r0, r1, Y, Y2, ldy);       \
+    else update_dmma_core<nt, 1, false>(sKp, sB, KS, q, r0, r1, Y, Y2, ldy);                      \
+    break;
+  switch (NT) {
+    QDKP_DM_CASE(1) QDKP_DM_CASE(2) QDKP_DM_CASE(3) QDKP_DM_CASE(4) QDKP_DM_CASE(5) QDKP_DM_CASE(6)
+    default: break;
+  }
+#undef QDKP_DM_CASE
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -497,12 +521,6 @@ __host__ __device__ __forceinline__ int gram_chunk_rows(int P, int Q, int elem_b
   int r = kGramStageTarget / ((P + Q) * elem_bytes);
   r = r / 8 * 8;
   return r < kGramRows ? kGramRows : (r > 512 ? 512 : r);
-}
-__host__ __device__ __forceinline__ size_t update_smem_bytes(int P, int q, int elem_bytes,
-                                                          int nout = 1) {
-  const size_t KPp = (2 * P + 3) / 4 * 4 + 4, NQ = (2 * q + 7) / 8 * 8;
-  const size_t stage = (size_t)kUpdChunk * P * elem_bytes;
-  return nout * KPp * NQ * sizeof(double) + stage_count(stage) * stage;
 }
 
 __host__ __device__ __forceinline__ size_t gram_smem_bytes(int P, int Q, int elem_bytes) {

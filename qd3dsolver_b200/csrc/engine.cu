@@ -772,7 +772,7 @@ int launch_update_multi(const EGroup& G, int which, cudaStream_t st) {
   const bool fused = which == UP_XPNEW || which == UP_AXPNEW;
   const int P = (fused ? 3 : 1) * G.m_max, nout = fused ? 2 : 1;
   if (G.hx_ns[0]) {
-    const size_t smem = update_smem_bytes(P, G.m_max, (int)sizeof(double2), nout);
+    const size_t smem = update_smem_bytes(P, G.m_max, nout);
     e_update_kernel<double><<<G.row_ctas, kUpdThreads, smem, st>>>(G.d_slots, G.ns, which);
     count_launch();
   }
