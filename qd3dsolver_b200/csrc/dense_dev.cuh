@@ -335,20 +335,25 @@ static __device__ int block_eigh(const double2* __restrict__ A, const double2* _
 // ahead of the MMAs. The k order is permuted over pairs of k steps: a pair covers complex
 // columns c0 .. c0 + 3 of one block, MMA k = t of its first step is Re A[.][c0 + t] and of its
 // second step Im A[.][c0 + t] (g = lane / 4, t = lane % 4), so a lane's A values of the pair are
-// one 16-byte load, A[row g][c0 + t]. C'' is stored in that order as one 16-byte word per (pair,
-// 8-column N tile, lane): {C''[2 (c0 + t)][n g], C''[2 (c0 + t) + 1][n g]}. A row is read (by
-// the four lanes of its quad) before any of its outputs is written and no other warp touches
-// it, so Y may alias an input.
+// one 16-byte load, A[row g][c0 + t]. Those loads stream through a ring of kDmRing pairs in
+// shared memory private to the warp: each lane cp.async-copies exactly the 16 bytes it later
+// reads, so its own cp.async.wait_group orders them and no barrier is needed, and the ring holds
+// twice the bytes in flight that registers could. C'' is stored in the pair's k order as one
+// 16-byte word per (pair, 8-column N tile, lane): {C''[2 (c0 + t)][n g],
+// C''[2 (c0 + t) + 1][n g]}. A row is read (by the four lanes of its quad) before any of its
+// outputs is written and no other warp touches it, so Y may alias an input.
 constexpr int kUpdRows = 8;
 constexpr int kUpdThreads = 256;
 constexpr int kUpdWarps = kUpdThreads / 32;
 constexpr int kUpdChunk = kUpdRows * kUpdWarps;     // row granularity of a CTA's span
-constexpr int kDmRing = 8;                          // k-step pairs in flight per warp
+constexpr int kDmRing = 16;                         // k-step pairs in flight per warp (2^k)
+constexpr size_t kDmRingBytes = (size_t)kUpdWarps * kDmRing * 32 * sizeof(double2);
 
 // k-step pairs of a list of at most three blocks with P columns in all (ceil(cols / 4) each)
 __host__ __device__ __forceinline__ int dmma_pairs_bound(int P) { return (P + 3) / 4 + 2; }
+// the warps' load rings, then the packed coefficients
 __host__ __device__ __forceinline__ size_t update_smem_bytes(int P, int q, int nout = 1) {
-  return (size_t)nout * dmma_pairs_bound(P) * ((q + 3) / 4) * 32 * sizeof(double2);
+  return kDmRingBytes + (size_t)nout * dmma_pairs_bound(P) * ((q + 3) / 4) * 32 * sizeof(double2);
 }
 
 // one k-step pair of an update's A list: columns c0 .. c0 + 3 of a block (p points at c0)
@@ -360,7 +365,8 @@ struct DmKStep {
 
 template <int NT, int NOUT, bool ACC>
 static __device__ __forceinline__ void update_dmma_core(const DmKStep* __restrict__ sK,
-                                                        const double2* __restrict__ sB, int KS,
+                                                        const double2* __restrict__ sB,
+                                                        double2* __restrict__ ring, int KS,
                                                         int q, long long r0, long long r1,
                                                         double2* Y, double2* Y2, long long ldy) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -370,18 +376,26 @@ static __device__ __forceinline__ void update_dmma_core(const DmKStep* __restric
   const int mine = ntiles > warp ? (ntiles - warp + nw - 1) / nw : 0;
   const int nitems = mine * KS;
   if (nitems == 0) return;
-  constexpr int RING = NT * NOUT <= 6 ? kDmRing : kDmRing / 2;
-  double2 fa[RING];
+  // this lane's slots of the warp's ring: ring[slot * 32 + lane]; one commit group per item
+  ring += (size_t)warp * kDmRing * 32 + lane;
   int l_tile = warp, l_s = 0;
-  auto fetch = [&](double2& xa) {
+  auto fetch = [&](int slot) {
     const DmKStep k = sK[l_s];
     const long long ra = r0 + (long long)l_tile * kUpdRows + g;
-    xa = (t < k.rem && ra < r1) ? __ldcs(k.p + ra * k.ld + t) : make_double2(0.0, 0.0);
+    double2* dst = ring + slot * 32;
+    if (t < k.rem && ra < r1) {
+      const unsigned sa = (unsigned)__cvta_generic_to_shared(dst);
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" :: "r"(sa), "l"(k.p + ra * k.ld + t) : "memory");
+    } else {
+      *dst = make_double2(0.0, 0.0);
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
     if (++l_s == KS) { l_s = 0; l_tile += nw; }
   };
-#pragma unroll
-  for (int d = 0; d < RING; ++d)
-    if (d < nitems) fetch(fa[d]);
+  for (int d = 0; d < kDmRing; ++d) {
+    if (d < nitems) fetch(d);
+    else asm volatile("cp.async.commit_group;\n" ::: "memory");
+  }
   double acc[NOUT][NT][2];
   double2 yo[ACC ? NT : 1];
 #pragma unroll
@@ -389,13 +403,12 @@ static __device__ __forceinline__ void update_dmma_core(const DmKStep* __restric
 #pragma unroll
     for (int j = 0; j < NT; ++j) acc[o][j][0] = acc[o][j][1] = 0.0;
   int c_s = 0, c_tile = warp;
-  for (int base = 0; base < nitems; base += RING) {
-#pragma unroll
-    for (int d = 0; d < RING; ++d) {
-      const int it = base + d;
-      if (it >= nitems) break;
-      const double2 a = fa[d];
-      if (it + RING < nitems) fetch(fa[d]);
+  {
+    for (int it = 0; it < nitems; ++it) {
+      const int slot = it & (kDmRing - 1);
+      // item it's group is complete once at most kDmRing - 1 younger groups are pending
+      asm volatile("cp.async.wait_group %0;\n" :: "n"(kDmRing - 1) : "memory");
+      const double2 a = ring[slot * 32];
       const long long ra = r0 + (long long)c_tile * kUpdRows + g;
       if (ACC && c_s == 0) {
 #pragma unroll
@@ -416,6 +429,9 @@ static __device__ __forceinline__ void update_dmma_core(const DmKStep* __restric
           dmma(acc[NOUT - 1][j][0], acc[NOUT - 1][j][1], a.y, b2.y);
         }
       }
+      // refill the slot only now: the MMAs above consumed `a`, so its shared-memory read is done
+      if (it + kDmRing < nitems) fetch(slot);
+      else asm volatile("cp.async.commit_group;\n" ::: "memory");
       if (++c_s == KS) {
 #pragma unroll
         for (int j = 0; j < NT; ++j) {
@@ -434,6 +450,7 @@ static __device__ __forceinline__ void update_dmma_core(const DmKStep* __restric
       }
     }
   }
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
 
 // Y (+)= sg A C over rows [r0, r1) and, with C2/Y2, Y2 = sg A C2 (one pass over A; the fused
@@ -461,7 +478,8 @@ static __device__ void update_rows(const BlockList<double>& A, const double2* co
   }
   __syncthreads();
   const int KS = sKS;
-  double2* sB = reinterpret_cast<double2*>(smem);
+  double2* ring = reinterpret_cast<double2*>(smem);
+  double2* sB = reinterpret_cast<double2*>(smem + kDmRingBytes);
   const double sg = neg ? -1.0 : 1.0;
   const int per_out = KS * NT * 32;
   for (int e = threadIdx.x; e < nout * per_out; e += blockDim.x) {
@@ -486,11 +504,11 @@ static __device__ void update_rows(const BlockList<double>& A, const double2* co
 #define QDKP_DM_CASE(nt)                                                                          \
   case nt:                                                                                        \
     if (nout == 2 && accumulate) {                                                                \
-      update_dmma_core<nt, 1, true>(sKp, sB, KS, q, r0, r1, Y, Y2, ldy);                          \
-      update_dmma_core<nt, 1, false>(sKp, sB + per_out, KS, q, r0, r1, Y2, Y2, ldy);              \
-    } else if (nout == 2) update_dmma_core<nt, 2, false>(sKp, sB, KS, q, r0, r1, Y, Y2, ldy);     \
-    else if (accumulate) update_dmma_core<nt, 1, true>(sKp, sB, KS, q, r0, r1, Y, Y2, ldy);       \
-    else update_dmma_core<nt, 1, false>(sKp, sB, KS, q, r0, r1, Y, Y2, ldy);                      \
+      update_dmma_core<nt, 1, true>(sKp, sB, ring, KS, q, r0, r1, Y, Y2, ldy);                          \
+      update_dmma_core<nt, 1, false>(sKp, sB + per_out, ring, KS, q, r0, r1, Y2, Y2, ldy);              \
+    } else if (nout == 2) update_dmma_core<nt, 2, false>(sKp, sB, ring, KS, q, r0, r1, Y, Y2, ldy);     \
+    else if (accumulate) update_dmma_core<nt, 1, true>(sKp, sB, ring, KS, q, r0, r1, Y, Y2, ldy);       \
+    else update_dmma_core<nt, 1, false>(sKp, sB, ring, KS, q, r0, r1, Y, Y2, ldy);                      \
     break;
   switch (NT) {
     QDKP_DM_CASE(1) QDKP_DM_CASE(2) QDKP_DM_CASE(3) QDKP_DM_CASE(4) QDKP_DM_CASE(5) QDKP_DM_CASE(6)
