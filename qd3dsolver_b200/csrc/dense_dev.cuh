@@ -106,133 +106,184 @@ static __device__ void block_upper_inverse(const double2* S, int n, double2* out
 }
 
 
-// Parallel cyclic Jacobi on the Hermitian C (smem, n x n); V (smem) accumulates rotations.
-// Round-robin ordering gives n/2 disjoint (p, q) pairs per round. A pair is rotated while
-// |C_pq| > eps sqrt(|C_pp C_qq|) (the relative-accuracy threshold, so eigenvalues far below
-// ||C|| -- the wanted end of a folded spectrum -- are resolved to working precision); the
-// iteration stops after a sweep without rotations. A round is two barriers: the pairs' rotation
-// parameters, then one update phase in which each thread owns a 2x2 block
-// C[{p_k, q_k}, {p_l, q_l}] <- J_k^H C J_l (the blocks of a round are disjoint) or a row pair of
-// V <- V J_k.
-static __device__ void block_jacobi(double2* C, double2* V, int n) {
-  __shared__ double rcs[kMaxSmall / 2 + 1], rsn[kMaxSmall / 2 + 1];
-  __shared__ double2 re[kMaxSmall / 2 + 1];
-  __shared__ int rp[kMaxSmall / 2 + 1], rq[kMaxSmall / 2 + 1];
-  __shared__ int rotated;
-  __shared__ double fro_red[kSmallThreads / 32];
-  __shared__ double floor_abs;
-  const int n2 = n + (n & 1);
-  const int npair = n2 / 2;
-  {
-    // absolute floor eps ||C||_F: off-diagonals below it are rounding noise (the accuracy
-    // LAPACK's Hermitian solvers deliver), so chasing them only adds sweeps
-    double f = 0.0;
-    for (int e = threadIdx.x; e < n * n; e += blockDim.x) f += C[e].x * C[e].x + C[e].y * C[e].y;
-    for (int o = 16; o > 0; o >>= 1) f += __shfl_xor_sync(0xffffffffu, f, o);
-    if ((threadIdx.x & 31) == 0) fro_red[threadIdx.x >> 5] = f;
+// Eigen-decomposition of the Hermitian C in S0 (n x n, shared memory), with S1 = I on entry:
+// Householder reduction to tridiagonal form (C <- H C H, Q <- Q H, H = I - tau v v^H, one column
+// per step), a diagonal phase that makes the sub-diagonal real, and the implicit QL iteration
+// with shifts of Bowdler, Martin, Reinsch and Wilkinson (the tql2 scheme) on the real symmetric
+// tridiagonal matrix. One thread runs the QL recurrences and records each sweep's plane
+// rotations; then every row of the eigenvector matrix Z applies them, so the rotations stay
+// exactly orthogonal even inside clusters of (near-)equal eigenvalues. On return S0's diagonal
+// holds the eigenvalues (unsorted) and S1 the eigenvectors of C (columns). gtmp: n * n global
+// double2 of scratch. Returns nonzero (block-uniform) if an eigenvalue needed more than 60 QL
+// iterations (only non-finite input gets there).
+static __device__ int block_tql(double2* S0, double2* S1, int n, double2* gtmp) {
+  __shared__ double2 hv[kMaxSmall], hp[kMaxSmall], hq[kMaxSmall], ph[kMaxSmall];
+  __shared__ double td[kMaxSmall], tb[kMaxSmall], rc[kMaxSmall], rs[kMaxSmall];
+  __shared__ int ri[kMaxSmall];
+  __shared__ double s_tau, s_K;
+  __shared__ int s_nrot, s_state;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  // ---- Householder reduction ----
+  for (int k = 0; k + 2 < n; ++k) {
+    if (warp == 0) {
+      double nx2 = 0.0;
+      for (int i = k + 1 + lane; i < n; i += 32) {
+        const double2 x = S0[i * n + k];
+        nx2 += x.x * x.x + x.y * x.y;
+      }
+      for (int o = 16; o > 0; o >>= 1) nx2 += __shfl_xor_sync(0xffffffffu, nx2, o);
+      const double2 x0 = S0[(k + 1) * n + k];
+      const double ax0 = sqrt(x0.x * x0.x + x0.y * x0.y);
+      const double nx = sqrt(nx2);
+      // alpha = -phase(x0) |x|; v = x - alpha e_1; v^H v = 2 |x| (|x| + |x0|)
+      const double2 phs = ax0 > 0.0 ? make_double2(x0.x / ax0, x0.y / ax0) : make_double2(1.0, 0.0);
+      for (int i = lane; i < n; i += 32) {
+        double2 v = make_double2(0.0, 0.0);
+        if (i == k + 1) v = make_double2(x0.x + phs.x * nx, x0.y + phs.y * nx);
+        else if (i > k + 1) v = S0[i * n + k];
+        hv[i] = v;
+      }
+      if (lane == 0) s_tau = nx2 > 0.0 ? 1.0 / (nx * (nx + ax0)) : 0.0;
+    }
     __syncthreads();
+    const double tau = s_tau;
+    // every thread has read tau before warp 0 can move on to the next column and rewrite it
+    __syncthreads();
+    if (tau == 0.0) continue;                      // column already reduced (uniform)
+    // p = tau C v and q = Q v, a warp per row
+    for (int i = warp; i < n; i += nwarps) {
+      double2 sp = make_double2(0.0, 0.0), sq = make_double2(0.0, 0.0);
+      for (int j = k + 1 + lane; j < n; j += 32) {
+        const double2 v = hv[j];
+        cfma(sp, S0[i * n + j], v);
+        cfma(sq, S1[i * n + j], v);
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        sp.x += __shfl_xor_sync(0xffffffffu, sp.x, o); sp.y += __shfl_xor_sync(0xffffffffu, sp.y, o);
+        sq.x += __shfl_xor_sync(0xffffffffu, sq.x, o); sq.y += __shfl_xor_sync(0xffffffffu, sq.y, o);
+      }
+      if (lane == 0) { hp[i] = make_double2(tau * sp.x, tau * sp.y); hq[i] = sq; }
+    }
+    __syncthreads();
+    if (warp == 0) {                               // K = tau / 2 v^H p
+      double2 s = make_double2(0.0, 0.0);
+      for (int i = k + 1 + lane; i < n; i += 32) cfmac(s, hv[i], hp[i]);
+      for (int o = 16; o > 0; o >>= 1) {
+        s.x += __shfl_xor_sync(0xffffffffu, s.x, o); s.y += __shfl_xor_sync(0xffffffffu, s.y, o);
+      }
+      // v^H C v is real for Hermitian C; its rounding residue in s.y is dropped
+      if (lane == 0) s_K = 0.5 * tau * s.x;
+    }
+    __syncthreads();
+    const double K = s_K;
+    // C <- C - v w^H - w v^H with w = p - K v;  Q <- Q - tau q v^H
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+      const int i = e / n, j = e - i * n;
+      const double2 vi = hv[i], vj = hv[j];
+      const double2 wi = make_double2(hp[i].x - K * vi.x, hp[i].y - K * vi.y);
+      const double2 wj = make_double2(hp[j].x - K * vj.x, hp[j].y - K * vj.y);
+      double2 c = S0[e];
+      // c -= vi conj(wj) + wi conj(vj)
+      c.x -= vi.x * wj.x + vi.y * wj.y + wi.x * vj.x + wi.y * vj.y;
+      c.y -= vi.y * wj.x - vi.x * wj.y + wi.y * vj.x - wi.x * vj.y;
+      S0[e] = c;
+      const double2 qi = hq[i];
+      double2 q = S1[e];
+      q.x -= tau * (qi.x * vj.x + qi.y * vj.y);
+      q.y -= tau * (qi.y * vj.x - qi.x * vj.y);
+      S1[e] = q;
+    }
+    __syncthreads();
+  }
+  // ---- real tridiagonal form: D^H T D with D = diag(ph), ph_{i+1} = ph_i e_i / |e_i| ----
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    td[i] = S0[i * n + i].x;
+    hv[i] = i + 1 < n ? S0[(i + 1) * n + i] : make_double2(0.0, 0.0);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double2 p = make_double2(1.0, 0.0);
+    for (int i = 0; i < n; ++i) {
+      ph[i] = p;
+      const double2 e = hv[i];
+      const double ae = sqrt(e.x * e.x + e.y * e.y);
+      tb[i] = ae;
+      if (ae > 0.0) p = cmul(p, make_double2(e.x / ae, e.y / ae));
+    }
+    tb[n - 1] = 0.0;
+  }
+  __syncthreads();
+  double* Z = reinterpret_cast<double*>(S0);       // S0 is free now: n x n real
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+    const int i = e / n, j = e - i * n;
+    S1[e] = cmul(S1[e], ph[j]);
+    Z[e] = i == j ? 1.0 : 0.0;
+  }
+  // ---- implicit QL; thread 0 carries the iteration state across sweeps ----
+  int l = 0, it = 0, fail = 0;
+  for (;;) {
     if (threadIdx.x == 0) {
-      double t = 0.0;
-      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += fro_red[w];
-      floor_abs = 2.2e-16 * sqrt(t);
+      int nrot = 0, state = 0;                     // 0: a sweep to apply, 1: finished
+      for (;;) {
+        if (l >= n) { state = 1; break; }
+        int m = l;
+        for (; m < n - 1; ++m) {
+          const double dd = fabs(td[m]) + fabs(td[m + 1]);
+          if (fabs(tb[m]) <= 2.220446049250313e-16 * dd || fabs(tb[m]) < 1e-300) break;
+        }
+        if (m == l) { ++l; it = 0; continue; }
+        if (++it > 60) { fail = 1; state = 1; break; }
+        double g = (td[l + 1] - td[l]) / (2.0 * tb[l]);
+        double r = sqrt(g * g + 1.0);
+        g = td[m] - td[l] + tb[l] / (g + (g >= 0.0 ? r : -r));
+        double s = 1.0, c = 1.0, p = 0.0;
+        bool early = false;
+        for (int i = m - 1; i >= l; --i) {
+          const double f = s * tb[i], bb = c * tb[i];
+          const double h2 = f * f + g * g;
+          if (h2 == 0.0) { td[i + 1] -= p; tb[i + 1] = 0.0; tb[m] = 0.0; early = true; break; }
+          const double inv = rsqrt(h2);
+          tb[i + 1] = h2 * inv;
+          s = f * inv; c = g * inv;
+          g = td[i + 1] - p;
+          r = (td[i] - g) * s + 2.0 * c * bb;
+          p = s * r;
+          td[i + 1] = g + p;
+          g = c * r - bb;
+          ri[nrot] = i; rc[nrot] = c; rs[nrot] = s; ++nrot;
+        }
+        if (!early) { td[l] -= p; tb[l] = g; tb[m] = 0.0; }
+        break;
+      }
+      s_nrot = nrot; s_state = state | (fail << 1);
     }
     __syncthreads();
-  }
-  const int nblk = npair * npair;             // 2x2 blocks of C
-  for (int sweep = 0; sweep < 30; ++sweep) {
-    if (threadIdx.x == 0) rotated = 0;
-    __syncthreads();
-    for (int r = 0; r < n2 - 1; ++r) {
-      if (threadIdx.x < npair) {
-        const int k = threadIdx.x;
-        int p, q;
-        if (k == 0) { p = r; q = n2 - 1; }
-        else { p = (r + k) % (n2 - 1); q = (r - k + n2 - 1) % (n2 - 1); }
-        if (p > q) { const int t = p; p = q; q = t; }
-        double cs = 1.0, sn = 0.0;
-        double2 e = make_double2(1.0, 0.0);
-        if (q < n) {
-          // squared-magnitude tests and reciprocal square roots keep the serial chain of a
-          // round short; Gram-built entries are far from the FP64 range limits (|c|^2 neither
-          // under- nor overflows where the tests pass)
-          const double2 c = C[p * n + q];
-          const double ac2 = c.x * c.x + c.y * c.y;
-          const double a = C[p * n + p].x, b = C[q * n + q].x;
-          if (ac2 > floor_abs * floor_abs && ac2 > 4.84e-32 * fabs(a * b)) {
-            const double rac = rsqrt(ac2);
-            const double tau = 0.5 * (b - a) * rac;
-            const double at = fabs(tau);
-            const double t = at > 1e150 ? 0.5 / tau
-                                        : (tau >= 0.0 ? 1.0 : -1.0) / (at + sqrt(1.0 + tau * tau));
-            cs = rsqrt(1.0 + t * t);
-            sn = t * cs;
-            e = make_double2(c.x * rac, c.y * rac);
-            if (sn != 0.0) rotated = 1;
-          }
-        }
-        rp[k] = p; rq[k] = q; rcs[k] = cs; rsn[k] = sn; re[k] = e;
+    const int nrot = s_nrot, state = s_state;
+    for (int row = threadIdx.x; row < n; row += blockDim.x) {
+      double* z = Z + row * n;
+      for (int u = 0; u < nrot; ++u) {
+        const int i = ri[u];
+        const double c = rc[u], s = rs[u];
+        const double f = z[i + 1];
+        z[i + 1] = s * z[i] + c * f;
+        z[i] = c * z[i] - s * f;
       }
-      __syncthreads();
-      // J = [[cs, sn e], [-sn conj(e), cs]] on columns (p, q); J^H = [[cs, -sn e],
-      // [sn conj(e), cs]] on rows (p, q)
-      for (int t = threadIdx.x; t < nblk + n * npair; t += blockDim.x) {
-        if (t < nblk) {
-          const int k = t / npair, l = t - k * npair;
-          const int pk = rp[k], qk = rq[k], pl = rp[l], ql = rq[l];
-          const bool rk = qk < n && rsn[k] != 0.0, rl = ql < n && rsn[l] != 0.0;
-          if (!rk && !rl) continue;
-          // entries that exist: rows pk (always < n) and qk (if < n), same for columns
-          const bool hk = qk < n, hl = ql < n;
-          double2 a = C[pk * n + pl];
-          double2 b = hl ? C[pk * n + ql] : make_double2(0.0, 0.0);
-          double2 c = hk ? C[qk * n + pl] : make_double2(0.0, 0.0);
-          double2 d = (hk && hl) ? C[qk * n + ql] : make_double2(0.0, 0.0);
-          if (rl) {                          // [a b; c d] <- [a b; c d] J_l
-            const double cs = rcs[l], sn = rsn[l];
-            const double2 e = re[l];
-            const double2 m10 = make_double2(-sn * e.x, sn * e.y);   // -sn conj(e)
-            const double2 m01 = make_double2(sn * e.x, sn * e.y);    //  sn e
-            double2 na = cscale(cs, a); cfma(na, m10, b);
-            double2 nb = cscale(cs, b); cfma(nb, m01, a);
-            double2 nc = cscale(cs, c); cfma(nc, m10, d);
-            double2 nd = cscale(cs, d); cfma(nd, m01, c);
-            a = na; b = nb; c = nc; d = nd;
-          }
-          if (rk) {                          // [a b; c d] <- J_k^H [a b; c d]
-            const double cs = rcs[k], sn = rsn[k];
-            const double2 e = re[k];
-            const double2 a01 = make_double2(-sn * e.x, -sn * e.y);  // -sn e
-            const double2 a10 = make_double2(sn * e.x, -sn * e.y);   //  sn conj(e)
-            double2 na = cscale(cs, a); cfma(na, a01, c);
-            double2 nb = cscale(cs, b); cfma(nb, a01, d);
-            double2 nc = cscale(cs, c); cfma(nc, a10, a);
-            double2 nd = cscale(cs, d); cfma(nd, a10, b);
-            a = na; b = nb; c = nc; d = nd;
-          }
-          C[pk * n + pl] = a;
-          if (hl) C[pk * n + ql] = b;
-          if (hk) C[qk * n + pl] = c;
-          if (hk && hl) C[qk * n + ql] = d;
-        } else {
-          const int u = t - nblk;
-          const int k = u / n, i = u - k * n;
-          const int p = rp[k], q = rq[k];
-          if (q >= n || rsn[k] == 0.0) continue;
-          const double cs = rcs[k], sn = rsn[k];
-          const double2 e = re[k];
-          const double2 m10 = make_double2(-sn * e.x, sn * e.y);
-          const double2 m01 = make_double2(sn * e.x, sn * e.y);
-          const double2 x = V[i * n + p], y = V[i * n + q];
-          double2 np = cscale(cs, x); cfma(np, m10, y);
-          double2 nq = cscale(cs, y); cfma(nq, m01, x);
-          V[i * n + p] = np; V[i * n + q] = nq;
-        }
-      }
-      __syncthreads();
     }
-    if (!rotated) break;
     __syncthreads();
+    if (state & 1) { fail = state >> 1; break; }
   }
+  // ---- V = (Q D) Z into S1, eigenvalues onto S0's diagonal ----
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+    const int i = e / n, j = e - i * n;
+    double2 v = make_double2(0.0, 0.0);
+    for (int k = 0; k < n; ++k) caxpy(v, Z[k * n + j], S1[i * n + k]);
+    gtmp[e] = v;
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) S1[e] = gtmp[e];
+  for (int i = threadIdx.x; i < n; i += blockDim.x) S0[i * n + i] = make_double2(td[i], 0.0);
+  __syncthreads();
+  return fail;
 }
 
 
@@ -292,7 +343,7 @@ static __device__ int block_eigh(const double2* __restrict__ A, const double2* _
   for (int e = threadIdx.x; e < n * n; e += blockDim.x)
     S1[e] = make_double2((e / n == e % n) ? 1.0 : 0.0, 0.0);
   __syncthreads();
-  block_jacobi(S0, S1, n);
+  if (block_tql(S0, S1, n, Tg)) return 2;
   for (int i = threadIdx.x; i < n; i += blockDim.x) wd[i] = S0[i * n + i].x;
   __syncthreads();
   int bad = 0;
