@@ -298,7 +298,6 @@ int qdkp_lobpcg_solve(const qdkp_operator* op, const qdkp_lobpcg_params* prm, co
   bool have_best = false;
   int it = -1;
   bool restart = true, forced = false, explicit_gram = false;
-  bool have_P = false;
   int status = QDKP_LOBPCG_MAXITER;
   const int M3 = 3 * m;
   std::vector<double2> hS((size_t)M3 * M3), hT((size_t)M3 * M3), gA, gB;
@@ -489,13 +488,11 @@ int qdkp_lobpcg_solve(const qdkp_operator* op, const qdkp_lobpcg_params* prm, co
       BlockList<double> lax = blist({{b.AX, m}, {b.AP, m}});
       lax.ld[0] = m; lax.ld[1] = m;
       TRY(launch_update(lax, C2, m, n, b.AX, m, 0, st));
-      have_P = true;
     }
     if (prm->verbosity > 1)
       fprintf(stderr, "lobpcg it %d active %d mean %.3e restart %d explicit %d\n", it, ma, mean,
               (int)restart, (int)explicit_gram);
   }
-  (void)have_P;
   // ---- final residuals of the last iterate -------------------------------------------------
   if (status != QDKP_LOBPCG_NONFINITE) {
     TRY(launch_colnorm2(b.AX, m, b.X, m, b.lam, m, n, b.npart, kNormParts, b.norms, st));
