@@ -1,6 +1,6 @@
 // Tall-skinny block kernels (norms, residual gather, Gram, block update) and one-CTA FP64
 // small dense kernels (Cholesky + triangular inverse, Hermitian generalized eigensolver by
-// parallel cyclic Jacobi) for the LOBPCG driver.
+// Householder reduction and implicit QL) for the LOBPCG driver.
 #include <algorithm>
 #include <cmath>
 #include <type_traits>

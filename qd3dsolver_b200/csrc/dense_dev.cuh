@@ -1,5 +1,6 @@
 // Device building blocks shared by the single-solve and batched LOBPCG kernels: FP64 MMA,
-// block-list element access, and the one-CTA Cholesky / triangular inverse / Jacobi routines.
+// block-list element access, and the one-CTA Cholesky / triangular inverse / Hermitian
+// eigensolver routines.
 #pragma once
 #include "blockops.cuh"
 
@@ -571,7 +572,8 @@ static __device__ void update_rows(const BlockList<double>& A, const double2* co
 // ---------------------------------------------------------------------------------------------
 // Gram core: partial C' = A'^T B' (real views: row r, column 2c + {re, im}) of rows [r0, r1) on
 // the FP64 MMA units (mma.sync.m8n8k4.f64; the tcgen05 family has no f64 kind). Rows stream
-// through shared memory in chunks of kGramRows, double buffered with cp.async: every block of
+// through shared memory in chunks (gram_chunk_rows), 2-4 stages in flight with cp.async and one
+// CTA barrier per chunk: every block of
 // the two lists is copied as a flat run of chunk-rows x cols complex values (the engine's blocks
 // are compact, ld = cols; other leading dimensions are handled row by row). Each warp owns a
 // rectangle of MR x MC 8x8 tiles of C' and a slice of the chunk's 4-row k steps, reads its
