@@ -3,7 +3,8 @@
     python -m qd3dsolver_b200.build [--verbose-ptxas]
 
 Compiles every .cu file of qd3dsolver_b200/csrc into qd3dsolver_b200/libqdkp.so. Objects go to
-qd3dsolver_b200/_build/ and are reused while their source and headers are unchanged.
+qd3dsolver_b200/_build/ and are reused while their source and headers are unchanged; objects of
+superseded sources are removed after a successful link.
 """
 import hashlib
 import os
@@ -59,6 +60,11 @@ def build(verbose_ptxas=False, force=False):
     if r.returncode != 0:
         raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
     os.replace(tmp, LIB)
+    # objects of earlier sources or headers are never reused: keep only this build's
+    keep = {os.path.basename(o) for o in objs}
+    for f in os.listdir(BUILD):
+        if f.endswith('.o') and f not in keep:
+            os.remove(os.path.join(BUILD, f))
     return LIB
 
 
