@@ -15,5 +15,8 @@ post         -- localisation and Kramers pairing (pryor_fig4.py:179-193, 222-236
 
 Parity pins: the operator is checked against H @ X fixtures generated by the reference itself
 (tests/golden/make_golden.py), and the solver wrappers against the reference's own solves on
-small grids and on the 48x48x36 pyramid workload (tests/golden/make_config1_oracle.py).
+small grids and on the seven Fig-4 pyramids of pryor_fig4.sweep with the reference's own FD-strain
+fields (tests/golden/make_fig4_golden.py). On the 48x48x36 pyramid the reference's folded solve
+does not converge (spurious finite-difference band, tests/test_spurious_band.py); its first
+LOBPCG iterations are the fixture there (tests/golden/make_config1_golden.py).
 """

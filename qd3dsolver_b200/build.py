@@ -10,6 +10,7 @@ import hashlib
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
@@ -35,7 +36,7 @@ def _headers_digest():
 def build(verbose_ptxas=False, force=False):
     os.makedirs(BUILD, exist_ok=True)
     hdr = _headers_digest()
-    objs = []
+    objs, jobs = [], []
     for f in sorted(os.listdir(CSRC)):
         if not f.endswith('.cu'):
             continue
@@ -49,11 +50,18 @@ def build(verbose_ptxas=False, force=False):
         cmd = [NVCC] + ARCH + FLAGS + ['-c', src, '-o', obj]
         if verbose_ptxas:
             cmd += ['-Xptxas', '-v']
-        r = subprocess.run(cmd, capture_output=True, text=True)
-        if r.returncode != 0:
-            raise RuntimeError(f"nvcc failed on {f}:\n{r.stdout}\n{r.stderr}")
-        if verbose_ptxas:
-            sys.stderr.write(r.stderr)
+        jobs.append((f, cmd))
+
+    def compile_one(job):
+        return job[0], subprocess.run(job[1], capture_output=True, text=True)
+
+    # one nvcc per source file, in parallel
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        for f, r in ex.map(compile_one, jobs):
+            if r.returncode != 0:
+                raise RuntimeError(f"nvcc failed on {f}:\n{r.stdout}\n{r.stderr}")
+            if verbose_ptxas:
+                sys.stderr.write(f"== {f}\n" + r.stderr)
     tmp = LIB + '.tmp'
     cmd = [NVCC] + ARCH + ['-shared', '-o', tmp] + objs + ['-lcudart']
     r = subprocess.run(cmd, capture_output=True, text=True)

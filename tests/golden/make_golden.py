@@ -8,15 +8,15 @@ solve_cases.npz / solve_cases.json -- a small InAs/GaAs pyramid (16x16x12 at h =
     by the reference's eigensolvers.solve_interior (cb and vb, k = 4) and solve_lowest on the
     4-band hole operator (hole_convention=True, k = 4): eigenvalues, residuals, iterations.
 
-Usage: python tests/golden/make_golden.py     (REFERENCE_DIR overrides /root/reference)
+Usage: python tests/golden/make_golden.py --reference DIR
 """
+import argparse
 import json
 import os
 import sys
 
 import numpy as np
 
-REFERENCE_DIR = os.environ.get('REFERENCE_DIR', '/root/reference')
 HERE = os.path.dirname(os.path.abspath(__file__))
 FIELD_KEYS = ('gamma1', 'gamma2', 'gamma3', 'P0', 'Ec', 'Ev', 'delta_so', 'b', 'd',
               'exx', 'eyy', 'ezz', 'exy', 'eyz', 'ezx', 'a_c', 'a_v')
@@ -42,7 +42,9 @@ def physical_fields(shape, h, rng, ref):
 
 
 def main():
-    sys.path.insert(0, REFERENCE_DIR)
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--reference', required=True, help='directory of the qd3Dsolver sources')
+    sys.path.insert(0, os.path.abspath(ap.parse_args().reference))
     import qdsolver_core as qd, kp_pryor as kp, kp_confined as kpc
     import strain_fourier as sf, materials as mt, eigensolvers as eig
     ref = dict(qd=qd, kp=kp, sf=sf, mt=mt)
