@@ -150,20 +150,30 @@ int qdkp_apply_folded_noalloc(const qdkp_operator* op, const void* X, int64_t ld
 /*
  * H.X kernel selection (no counterpart in the reference, which multiplies an assembled CSR).
  * Eight-band operators are applied by a staged kernel: a CTA owns a (y, z) tile of sites and a
- * few columns, walks along x and keeps a ring of x planes in shared memory. The tile shape is
- * one of QDKP_TILE_COUNT built shapes, chosen by a padding heuristic unless set here or by
- * qdkp_operator_tune; QDKP_TILE_DIRECT selects the unstaged one-thread-per-(site, column) kernel
- * (always used for 6- and 4-band slices). The choice is per operator and precision.
+ * few columns, walks along x and keeps a ring of x planes in shared memory. Tiles 0..3 fill the
+ * ring with cp.async (both precisions); tiles 4..7 (complex64 only) fill it with bulk tensor
+ * copies (TMA) and give every thread two columns of a site. A block the tensor maps cannot
+ * describe (odd leading dimension, a base not 16-byte aligned, fewer columns than a tile or a
+ * grid smaller than a tile) falls back to a cp.async tile. The tile is chosen by a heuristic
+ * unless set here or by qdkp_operator_tune; QDKP_TILE_DIRECT selects the unstaged
+ * one-thread-per-(site, column) kernel (always used for 6- and 4-band slices). The choice is per
+ * operator and precision.
  */
-enum { QDKP_TILE_AUTO = -1, QDKP_TILE_DIRECT = -2, QDKP_TILE_COUNT = 4 };
+enum { QDKP_TILE_AUTO = -1, QDKP_TILE_DIRECT = -2, QDKP_TILE_COUNT = 8 };
 int qdkp_operator_set_tile(qdkp_operator* op, int precision, int tile);
 int qdkp_operator_get_tile(const qdkp_operator* op, int precision, int* tile);
 /* Autotuner: times every tile shape and the direct kernel on the caller's device blocks X, Y
  * (n x m, `precision`) with `reps` launches each, keeps the fastest for this operator and
  * precision, and writes the per-candidate seconds per launch to seconds[QDKP_TILE_COUNT + 1]
- * (may be NULL; index QDKP_TILE_COUNT is the direct kernel). Y is overwritten. Synchronous. */
+ * (may be NULL; index QDKP_TILE_COUNT is the direct kernel; -1 marks a candidate that does not
+ * apply to this block or precision). Y is overwritten. Synchronous. */
 int qdkp_operator_tune(qdkp_operator* op, const void* X, int64_t ldx, void* Y, int64_t ldy,
                        int m, int precision, int reps, double* seconds, void* stream);
+
+/* Kernels that wait on their own bulk copies give up after about a second if a copy never lands
+ * (a fault elsewhere on the device) and set a device flag instead of hanging. *fault receives the
+ * flag of `device` (0 = none); clear = 1 resets it. Synchronous; the current device is kept. */
+int qdkp_device_fault(int device, int clear, int* fault);
 
 /* Workspace bytes qdkp_apply_host needs for an (n, m) complex128 block in `mode`. */
 size_t qdkp_apply_host_workspace_size(const qdkp_operator* op, int m, int mode);

@@ -13,7 +13,8 @@ QDKP_OK = 0
 HOLE_CONVENTION, STRAIN, INTERBAND_STRAIN, NEGATE = 1, 2, 4, 8
 C128, C64 = 0, 1
 APPLY_PLAIN, APPLY_SHIFTED, APPLY_FOLDED = 0, 1, 2
-TILE_AUTO, TILE_DIRECT, TILE_COUNT = -1, -2, 4
+TILE_AUTO, TILE_DIRECT, TILE_COUNT = -1, -2, 8
+TILE_TMA0 = 4                     # first TMA tile shape (complex64)
 LOBPCG_STATUS = {0: 'converged', 1: 'maxiter', 2: 'cholesky_breakdown',
                  3: 'eigh_breakdown', 4: 'nonfinite'}
 
@@ -69,6 +70,8 @@ _SIGNATURES = {
                                           ctypes.c_void_p, ctypes.c_int64, ctypes.c_int,
                                           ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
                                           ctypes.c_void_p]),
+    'qdkp_device_fault': (ctypes.c_int, [ctypes.c_int, ctypes.c_int,
+                                         ctypes.POINTER(ctypes.c_int)]),
     'qdkp_apply_host_workspace_size': (ctypes.c_size_t, [ctypes.c_void_p, ctypes.c_int,
                                                          ctypes.c_int]),
     'qdkp_apply_host': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,

@@ -25,6 +25,8 @@
 //                     symmetric; the first-order ones change sign). The edge terms of a plane
 //                     are summed with their scalar weights first and the constant band-mixing
 //                     matrix of that plane is applied once.
+#include <cuda.h>   // CUtensorMap and its enums (the encoder is fetched from the runtime)
+
 #include <algorithm>
 #include <type_traits>
 
@@ -835,6 +837,389 @@ __global__ void __launch_bounds__(G::THREADS, 1) kp_apply_staged_kernel(const St
   cp_async_wait_all();
 }
 
+// ---------------------------------------------------------------------------------------------
+// TMA kernel (eight bands, complex64). The same x walk as the staged kernel, with three changes:
+//   * the planes and the record rows are brought in by the tensor-memory accelerator
+//     (cp.async.bulk.tensor, one elected thread, completion on an mbarrier per ring slot) from
+//     tensor maps over this GPU's X and record; coordinates outside the grid (the halo at a wall,
+//     planes -1 and nx) read as zeros, so no thread computes an address or a neighbour mask:
+//     every weight a missing neighbour would need is zero in the record anyway;
+//   * every thread owns one site and two adjacent columns: each coefficient broadcast and record
+//     read serves both, and a band of both columns is one 16-byte shared load;
+//   * a ring of NSLOT planes keeps NSLOT - 3 planes in flight ahead of the compute.
+// Smem of a plane as the TMA box lands it: [band][y + 1][z + 1][column] (MC columns).
+// ---------------------------------------------------------------------------------------------
+template <int C, class L, class Rc>
+__device__ __forceinline__ void hx_packed_cols(const L& ld, const Rc& rc, float shift, float cb,
+                                               float2 (&Y)[C][8]) {
+  const float sq2 = 1.41421356237309504880f, sq3 = 1.73205080756887729353f;
+  const float sq32 = 1.22474487139158904910f, isq2 = 0.70710678118654752440f;
+  const f2 C2 = f2bc(sq2), CN2 = f2bc(-sq2), C3 = f2bc(sq3), C32 = f2bc(sq32);
+  const f2 CN32 = f2bc(-sq32), Ci2 = f2bc(isq2), CNi2 = f2bc(-isq2), CN1 = f2bc(-1.f);
+  const f2 CB = f2bc(cb);
+  f2 y[C][8], yi[C][8], x[C][8];
+
+  // ---- local block, the shift -sigma folded into the diagonal ---------------------------
+  ld.centre(x);
+  {
+    const float Rr = rc.own(K_RRE), Ri = rc.own(K_RIM), Sr = rc.own(K_SRE), Si = rc.own(K_SIM);
+    const float q2 = rc.own(K_Q2);
+    const f2 PA = f2bc(rc.own(K_A) + shift), P2 = f2bc(rc.own(K_A2) + shift);
+    const f2 P3 = f2bc(rc.own(K_A3) + shift), P6 = f2bc(rc.own(K_A6) + shift);
+    const f2 Q2 = f2bc(q2), NQ2 = f2bc(-q2);
+    const f2 SR = f2bc(Sr), NSR = f2bc(-Sr), SI = f2bc(Si), NSI = f2bc(-Si);
+    const f2 RR = f2bc(Rr), RI = f2bc(Ri), NRI = f2bc(-Ri);
+    const f2 S32R = f2bc(sq32 * Sr), S32I = f2bc(sq32 * Si), NS32I = f2bc(-sq32 * Si);
+    const f2 R2R = f2bc(sq2 * Rr), NR2R = f2bc(-sq2 * Rr), R2I = f2bc(sq2 * Ri);
+    const f2 NR2I = f2bc(-sq2 * Ri);
+    const f2 SI2R = f2bc(isq2 * Sr), SI2I = f2bc(isq2 * Si), NSI2I = f2bc(-isq2 * Si);
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+      const f2* xc = x[c];
+      f2* yc = y[c];
+      f2* ic = yi[c];
+      yc[0] = mul2(PA, xc[0]); yc[1] = mul2(PA, xc[1]);
+      ic[0] = 0ull; ic[1] = 0ull;
+      yc[2] = fma2(NSR, xc[3], mul2(P2, xc[2]));   ic[2] = mul2(SI, xc[3]);
+      yc[2] = fma2(RR, xc[4], yc[2]);              ic[2] = fma2(RI, xc[4], ic[2]);
+      yc[2] = fma2(S32R, xc[6], yc[2]);            ic[2] = fma2(S32I, xc[6], ic[2]);
+      yc[2] = fma2(NQ2, xc[7], yc[2]);
+      yc[3] = fma2(NSR, xc[2], mul2(P3, xc[3]));   ic[3] = mul2(NSI, xc[2]);
+      yc[3] = fma2(RR, xc[5], yc[3]);              ic[3] = fma2(RI, xc[5], ic[3]);
+      yc[3] = fma2(NR2R, xc[6], yc[3]);            ic[3] = fma2(NR2I, xc[6], ic[3]);
+      yc[3] = fma2(SI2R, xc[7], yc[3]);            ic[3] = fma2(SI2I, xc[7], ic[3]);
+      yc[4] = fma2(RR, xc[2], mul2(P3, xc[4]));    ic[4] = mul2(NRI, xc[2]);
+      yc[4] = fma2(SR, xc[5], yc[4]);              ic[4] = fma2(NSI, xc[5], ic[4]);
+      yc[4] = fma2(SI2R, xc[6], yc[4]);            ic[4] = fma2(NSI2I, xc[6], ic[4]);
+      yc[4] = fma2(R2R, xc[7], yc[4]);             ic[4] = fma2(NR2I, xc[7], ic[4]);
+      yc[5] = fma2(RR, xc[3], mul2(P2, xc[5]));    ic[5] = mul2(NRI, xc[3]);
+      yc[5] = fma2(SR, xc[4], yc[5]);              ic[5] = fma2(SI, xc[4], ic[5]);
+      yc[5] = fma2(Q2, xc[6], yc[5]);
+      yc[5] = fma2(S32R, xc[7], yc[5]);            ic[5] = fma2(NS32I, xc[7], ic[5]);
+      yc[6] = fma2(S32R, xc[2], mul2(P6, xc[6]));  ic[6] = mul2(NS32I, xc[2]);
+      yc[6] = fma2(NR2R, xc[3], yc[6]);            ic[6] = fma2(R2I, xc[3], ic[6]);
+      yc[6] = fma2(SI2R, xc[4], yc[6]);            ic[6] = fma2(SI2I, xc[4], ic[6]);
+      yc[6] = fma2(Q2, xc[5], yc[6]);
+      yc[7] = fma2(NQ2, xc[2], mul2(P6, xc[7]));
+      yc[7] = fma2(SI2R, xc[3], yc[7]);            ic[7] = mul2(NSI2I, xc[3]);
+      yc[7] = fma2(R2R, xc[4], yc[7]);             ic[7] = fma2(R2I, xc[4], ic[7]);
+      yc[7] = fma2(S32R, xc[5], yc[7]);            ic[7] = fma2(S32I, xc[5], ic[7]);
+    }
+  }
+
+  // ---- six face neighbours (a missing neighbour reads as zero, its weights are zero) ----
+#pragma unroll
+  for (int f = 0; f < 6; ++f) {
+    const int ax = f >> 1, dir = f & 1;
+    ld.face(f, x);
+    const float kp = rc.face(ax, dir, 0), k2 = rc.face(ax, dir, 1);
+    const float kq = (ax == 2 ? -2.f : 1.f) * k2;
+    const f2 KPQ = f2bc(kq - kp), NKPQ = f2bc(-kp - kq), NKP = f2bc(-kp);
+    const f2 K2Q = f2bc(sq2 * kq), NK2Q = f2bc(-sq2 * kq);
+    const float kr = (ax == 0 ? -sq3 : sq3) * k2;
+    const f2 KR = f2bc(kr), K2R = f2bc(sq2 * kr), NK2R = f2bc(-sq2 * kr);
+    const float su = rc.face(ax, dir, 2), svr = rc.face(ax, dir, 3), svi = rc.face(ax, dir, 4);
+    const f2 SVI = f2bc(svi), SVR = f2bc(svr), SU = f2bc(su), NSVR = f2bc(-svr), NSU = f2bc(-su);
+    const f2 S2SU = f2bc(sq2 * su), N3SVI = f2bc(-sq3 * svi), S3SVR = f2bc(sq3 * svr);
+    const f2 N3SVR = f2bc(-sq3 * svr), N2SVI = f2bc(-sq2 * svi), N2SVR = f2bc(-sq2 * svr);
+    const f2 S2SVI = f2bc(sq2 * svi);
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+      const f2* xc = x[c];
+      f2* yc = y[c];
+      f2* ic = yi[c];
+      yc[0] = fma2(CB, xc[0], yc[0]); yc[1] = fma2(CB, xc[1], yc[1]);
+      yc[2] = fma2(KPQ, xc[2], yc[2]); yc[2] = fma2(NK2Q, xc[7], yc[2]);
+      yc[3] = fma2(NKPQ, xc[3], yc[3]);
+      yc[4] = fma2(NKPQ, xc[4], yc[4]);
+      yc[5] = fma2(KPQ, xc[5], yc[5]); yc[5] = fma2(K2Q, xc[6], yc[5]);
+      yc[6] = fma2(NKP, xc[6], yc[6]); yc[6] = fma2(K2Q, xc[5], yc[6]);
+      yc[7] = fma2(NKP, xc[7], yc[7]); yc[7] = fma2(NK2Q, xc[2], yc[7]);
+      if (ax < 2) {
+        yc[2] = fma2(KR, xc[4], yc[2]);
+        yc[3] = fma2(KR, xc[5], yc[3]); yc[3] = fma2(NK2R, xc[6], yc[3]);
+        yc[4] = fma2(KR, xc[2], yc[4]); yc[4] = fma2(K2R, xc[7], yc[4]);
+        yc[5] = fma2(KR, xc[3], yc[5]);
+        yc[6] = fma2(NK2R, xc[3], yc[6]);
+        yc[7] = fma2(K2R, xc[4], yc[7]);
+      }
+      {
+        const f2 t = fma2(C2, xc[7], xc[2]);        // x2 + sqrt2 x7
+        const f2 u = mul2(C3, xc[4]);               // sqrt3 x4
+        yc[0] = fma2(SVI, sub2(u, t), yc[0]);
+        ic[0] = fma2(NSVR, add2(u, t), ic[0]);
+        ic[0] = fma2(SU, fma2(C2, xc[5], xc[6]), ic[0]);
+        const f2 v = mul2(C3, xc[3]);               // sqrt3 x3
+        const f2 w = fma2(CN2, xc[6], xc[5]);       // x5 - sqrt2 x6
+        yc[1] = fma2(SVI, sub2(v, w), yc[1]);
+        ic[1] = fma2(SVR, add2(v, w), ic[1]);
+        ic[1] = fma2(SU, fma2(C2, xc[2], mul2(CN1, xc[7])), ic[1]);
+      }
+      yc[2] = fma2(SVI, xc[0], yc[2]);   ic[2] = fma2(NSVR, xc[0], ic[2]); ic[2] = fma2(S2SU, xc[1], ic[2]);
+      yc[3] = fma2(N3SVI, xc[1], yc[3]); ic[3] = fma2(S3SVR, xc[1], ic[3]);
+      yc[4] = fma2(N3SVI, xc[0], yc[4]); ic[4] = fma2(N3SVR, xc[0], ic[4]);
+      yc[5] = fma2(SVI, xc[1], yc[5]);   ic[5] = fma2(S2SU, xc[0], ic[5]); ic[5] = fma2(SVR, xc[1], ic[5]);
+      yc[6] = fma2(N2SVI, xc[1], yc[6]); ic[6] = fma2(N2SVR, xc[1], ic[6]); ic[6] = fma2(SU, xc[0], ic[6]);
+      yc[7] = fma2(S2SVI, xc[0], yc[7]); ic[7] = fma2(N2SVR, xc[0], ic[7]); ic[7] = fma2(NSU, xc[1], ic[7]);
+    }
+  }
+
+  // ---- twelve edge neighbours: z = sum_e c_e x_e, then the plane's band mixing ---------
+#pragma unroll
+  for (int pl = 0; pl < 3; ++pl) {
+    f2 z[C][8];
+#pragma unroll
+    for (int c = 0; c < C; ++c)
+#pragma unroll
+      for (int b = 2; b < 8; ++b) z[c][b] = 0ull;
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      ld.edge(pl, e, x);
+      const f2 W = f2bc(rc.own(K_EDGE + 4 * pl + e));
+#pragma unroll
+      for (int c = 0; c < C; ++c)
+#pragma unroll
+        for (int b = 2; b < 8; ++b) z[c][b] = fma2(W, x[c][b], z[c][b]);
+    }
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+      const f2* zc = z[c];
+      f2* yc = y[c];
+      f2* ic = yi[c];
+      if (pl == 0) {            // R: +i z, R^H: -i z
+        ic[2] = add2(ic[2], zc[4]); ic[4] = sub2(ic[4], zc[2]);
+        ic[3] = add2(ic[3], zc[5]); ic[5] = sub2(ic[5], zc[3]);
+        ic[3] = fma2(CN2, zc[6], ic[3]); ic[6] = fma2(C2, zc[3], ic[6]);
+        ic[4] = fma2(CN2, zc[7], ic[4]); ic[7] = fma2(C2, zc[4], ic[7]);
+      } else if (pl == 1) {     // S, S^H: z
+        yc[3] = sub2(yc[3], zc[2]); yc[2] = fma2(C32, zc[6], yc[2]); yc[3] = fma2(Ci2, zc[7], yc[3]);
+        yc[5] = add2(yc[5], zc[4]); yc[6] = fma2(Ci2, zc[4], yc[6]); yc[7] = fma2(C32, zc[5], yc[7]);
+        yc[2] = sub2(yc[2], zc[3]); yc[6] = fma2(C32, zc[2], yc[6]); yc[7] = fma2(Ci2, zc[3], yc[7]);
+        yc[4] = add2(yc[4], zc[5]); yc[4] = fma2(Ci2, zc[6], yc[4]); yc[5] = fma2(C32, zc[7], yc[5]);
+      } else {                  // S: -i z, S^H: +i z
+        ic[3] = add2(ic[3], zc[2]); ic[2] = fma2(CN32, zc[6], ic[2]); ic[3] = fma2(CNi2, zc[7], ic[3]);
+        ic[5] = sub2(ic[5], zc[4]); ic[6] = fma2(CNi2, zc[4], ic[6]); ic[7] = fma2(CN32, zc[5], ic[7]);
+        ic[2] = sub2(ic[2], zc[3]); ic[6] = fma2(C32, zc[2], ic[6]); ic[7] = fma2(Ci2, zc[3], ic[7]);
+        ic[4] = add2(ic[4], zc[5]); ic[4] = fma2(Ci2, zc[6], ic[4]); ic[5] = fma2(C32, zc[7], ic[5]);
+      }
+    }
+  }
+
+  // ---- Y = y + i yi -------------------------------------------------------------------
+#pragma unroll
+  for (int c = 0; c < C; ++c)
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+      const float2 a = f2up(y[c][b]), d = f2up(yi[c][b]);
+      Y[c][b] = make_float2(a.x - d.y, a.y + d.x);
+    }
+}
+
+// mbarrier and bulk-tensor copy primitives (PTX ISA: mbarrier, cp.async.bulk.tensor)
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(bar), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+               " selp.b32 %0, 1, 0, p;\n}\n" : "=r"(ok) : "r"(bar), "r"(parity) : "memory");
+  return ok != 0;
+}
+// Bounded wait: gives up after about a second of SM clocks (a copy that never lands).
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const long long t0 = clock64();
+  while (!mbar_try_wait(bar, parity))
+    if (clock64() - t0 > 2000000000LL) return false;
+  return true;
+}
+__device__ __forceinline__ void tma_load_5d(uint32_t dst, const CUtensorMap* map, uint32_t bar,
+                                            int c0, int c1, int c2, int c3, int c4) {
+  asm volatile(
+      "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%3, %4, %5, %6, %7}], [%2];"
+      :: "r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(c0), "r"(c1), "r"(c2),
+         "r"(c3), "r"(c4) : "memory");
+}
+__device__ __forceinline__ void tma_load_4d(uint32_t dst, const CUtensorMap* map, uint32_t bar,
+                                            int c0, int c1, int c2, int c3) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%3, %4, %5, %6}], [%2];"
+      :: "r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(c0), "r"(c1), "r"(c2),
+         "r"(c3) : "memory");
+}
+
+// Set by a TMA kernel whose wait on a copy gave up (qdkp_device_fault reads and clears it).
+__device__ int g_apply_fault;
+
+template <int TY_, int TZ_, int G_, int NSLOT_>
+struct Tma {
+  static constexpr int TY = TY_, TZ = TZ_, G = G_, NSLOT = NSLOT_;
+  static constexpr int CPT = 2;                          // columns per thread
+  static constexpr int MC = CPT * G;                     // columns per CTA
+  static constexpr int PY = TY + 2, PZ = TZ + 2;
+  static constexpr int BAND = PY * PZ * MC;              // complex64 elements per band of a plane
+  static constexpr int PLANE_BYTES = 8 * BAND * 8;
+  static constexpr int RPLANE_BYTES = K_COUNT * TY * TZ * 4;
+  static constexpr int RSTRIDE = (RPLANE_BYTES + 127) / 128 * 128;
+  static constexpr int THREADS = TY * TZ * G;
+  static constexpr int BARS = NSLOT + 2;
+  static constexpr size_t SMEM = 1024 + (size_t)NSLOT * PLANE_BYTES + 2 * RSTRIDE + 8 * BARS;
+  static_assert(TZ % 4 == 0, "record rows are copied in 16-byte z runs");
+  static_assert(PLANE_BYTES % 128 == 0, "ring slots stay 128-byte aligned");
+  static_assert(NSLOT >= 4, "planes x-1, x, x+1 and at least one in flight");
+  static_assert(SMEM <= 232448, "over the opt-in shared memory of one CTA");
+};
+
+struct TmaArgs {
+  float2* __restrict__ Y;
+  int N, nx, ny, nz, ldy, m;
+  int tiles_z, chunks, xsplit, xlen;
+  int vec_store;          // Y is 16-byte aligned with an even leading dimension
+  float shift, cb;
+};
+
+template <class G>
+struct TmaLoader {
+  const unsigned long long* p[3];   // planes x-1, x, x+1 at this thread's (y, z, column pair)
+  __device__ __forceinline__ void at(const unsigned long long* q, int off, int b0,
+                                     f2 (&x)[2][8]) const {
+#pragma unroll
+    for (int b = b0; b < 8; ++b) {
+      const ulonglong2 v = *reinterpret_cast<const ulonglong2*>(q + b * G::BAND + off);
+      x[0][b] = v.x;
+      x[1][b] = v.y;
+    }
+  }
+  __device__ __forceinline__ void centre(f2 (&x)[2][8]) const { at(p[1], 0, 0, x); }
+  __device__ __forceinline__ void face(int f, f2 (&x)[2][8]) const {
+    const int ax = f >> 1, sg = (f & 1) ? -1 : 1;
+    if (ax == 0) at(p[1 + sg], 0, 0, x);
+    else if (ax == 1) at(p[1], sg * G::PZ * G::MC, 0, x);
+    else at(p[1], sg * G::MC, 0, x);
+  }
+  __device__ __forceinline__ void edge(int pl, int e, f2 (&x)[2][8]) const {
+    const int sa = (e & 1) ? -1 : 1, sb = (e & 2) ? -1 : 1;
+    if (pl == 0) at(p[1 + sa], sb * G::PZ * G::MC, 2, x);                 // a = x, b = y
+    else if (pl == 1) at(p[1 + sb], sa * G::MC, 2, x);                    // a = z, b = x
+    else at(p[1], sa * G::MC + sb * G::PZ * G::MC, 2, x);                 // a = z, b = y
+  }
+};
+
+template <class G>
+__global__ void __launch_bounds__(G::THREADS, 1)
+kp_apply_tma_kernel(const __grid_constant__ CUtensorMap tmx, const __grid_constant__ CUtensorMap tmr,
+                    const TmaArgs a) {
+  extern __shared__ unsigned char smem_raw[];
+  const uint32_t raw = smem_u32(smem_raw);
+  const uint32_t pad = ((raw + 1023u) & ~1023u) - raw;
+  unsigned char* sb = smem_raw + pad;
+  const uint32_t ring = raw + pad;
+  const uint32_t rring = ring + G::NSLOT * G::PLANE_BYTES;
+  const uint32_t bars = rring + 2 * G::RSTRIDE;          // NSLOT plane barriers, 2 record ones
+  int bid = blockIdx.x;
+  const int xs = bid % a.xsplit; bid /= a.xsplit;
+  const int ch = bid % a.chunks; bid /= a.chunks;
+  const int tzi = bid % a.tiles_z;
+  const int tyi = bid / a.tiles_z;
+  const int c0 = ch * G::MC, y0 = tyi * G::TY, z0 = tzi * G::TZ;
+  const int xa = xs * a.xlen, xb = min(a.nx, xa + a.xlen);
+  if (c0 >= a.m || xa >= xb) return;          // uniform over the CTA
+  const int t = threadIdx.x;
+  const int g = t % G::G, tz = (t / G::G) % G::TZ, ty = t / (G::G * G::TZ);
+  const int iy = y0 + ty, iz = z0 + tz, col = c0 + g * G::CPT;
+  const bool active = iy < a.ny && iz < a.nz && col < a.m;
+  const int cell = ((ty + 1) * G::PZ + (tz + 1)) * G::MC + g * G::CPT;
+
+  // plane with sequence number q (plane index xa - 1 + q) lives in slot q % NSLOT, and its
+  // barrier completes phase q / NSLOT; the record of plane xa + r in slot r & 1, phase r >> 1
+  auto plane_bar = [&](int q) { return bars + 8u * (uint32_t)(q % G::NSLOT); };
+  auto rec_bar = [&](int r) { return bars + 8u * (uint32_t)(G::NSLOT + (r & 1)); };
+  auto issue_plane = [&](int q) {
+    const uint32_t bar = plane_bar(q);
+    mbar_expect_tx(bar, G::PLANE_BYTES);
+    tma_load_5d(ring + (uint32_t)(q % G::NSLOT) * G::PLANE_BYTES, &tmx, bar, c0, z0 - 1, y0 - 1,
+                xa - 1 + q, 0);
+  };
+  auto issue_record = [&](int r) {
+    const uint32_t bar = rec_bar(r);
+    mbar_expect_tx(bar, G::RPLANE_BYTES);
+    tma_load_4d(rring + (uint32_t)(r & 1) * G::RSTRIDE, &tmr, bar, z0, y0, xa + r, 0);
+  };
+
+  if (t == 0) {
+    for (int i = 0; i < G::BARS; ++i) mbar_init(bars + 8u * i, 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  const int nplanes = xb - xa + 2;            // planes xa - 1 .. xb
+  int q_issued = 0, r_issued = 0;
+  if (t == 0) {
+    for (; q_issued < G::NSLOT - 1 && q_issued < nplanes; ++q_issued) issue_plane(q_issued);
+    issue_record(r_issued++);
+  }
+  bool ok = true;
+  for (int x = xa; x < xb; ++x) {
+    const int qx = x - xa + 1;
+    ok = ok && mbar_wait(plane_bar(qx - 1), ((qx - 1) / G::NSLOT) & 1) &&
+         mbar_wait(plane_bar(qx), (qx / G::NSLOT) & 1) &&
+         mbar_wait(plane_bar(qx + 1), ((qx + 1) / G::NSLOT) & 1);
+    // every thread is past plane x - 1: its ring slot and record slot may be refilled
+    const bool all_ok = __syncthreads_and(ok) != 0;
+    if (t == 0 && all_ok) {
+      if (q_issued < nplanes) issue_plane(q_issued++);
+      if (x + 1 < xb) issue_record(r_issued++);
+    }
+    const int r = x - xa;
+    ok = all_ok && mbar_wait(rec_bar(r), (r >> 1) & 1);
+    if (!ok || !active) continue;
+    TmaLoader<G> ld;
+    const unsigned long long* pl = reinterpret_cast<const unsigned long long*>(sb);
+    ld.p[0] = pl + (size_t)((qx - 1) % G::NSLOT) * (G::PLANE_BYTES / 8) + cell;
+    ld.p[1] = pl + (size_t)(qx % G::NSLOT) * (G::PLANE_BYTES / 8) + cell;
+    ld.p[2] = pl + (size_t)((qx + 1) % G::NSLOT) * (G::PLANE_BYTES / 8) + cell;
+    SmemRecord<float, G> rc;                    // record slot layout [k][ty][tz]
+    rc.r = reinterpret_cast<const float*>(sb + G::NSLOT * G::PLANE_BYTES + (r & 1) * G::RSTRIDE) +
+           ty * G::TZ + tz;
+    float2 yv[2][8];
+    hx_packed_cols<2>(ld, rc, a.shift, a.cb, yv);
+    const int s = (x * a.ny + iy) * a.nz + iz;
+    float2* __restrict__ ys = a.Y + ((long long)s * a.ldy + col);
+    const long long ybs = (long long)a.N * a.ldy;
+    if (a.vec_store && col + 1 < a.m) {
+#pragma unroll
+      for (int b = 0; b < 8; ++b)
+        *reinterpret_cast<float4*>(ys + b * ybs) = make_float4(yv[0][b].x, yv[0][b].y,
+                                                               yv[1][b].x, yv[1][b].y);
+    } else {
+#pragma unroll
+      for (int b = 0; b < 8; ++b) {
+        ys[b * ybs] = yv[0][b];
+        if (col + 1 < a.m) ys[b * ybs + 1] = yv[1][b];
+      }
+    }
+  }
+  if (__syncthreads_or(!ok) && t == 0) {
+    // a copy never landed: flag it, then give the copies still in flight a bounded chance to
+    // finish before the CTA's shared memory is released (thread 0 keeps the CTA resident)
+    atomicExch(&g_apply_fault, 1);
+    for (int q = max(0, q_issued - G::NSLOT); q < q_issued; ++q)
+      mbar_wait(plane_bar(q), (q / G::NSLOT) & 1);
+    for (int r = max(0, r_issued - 2); r < r_issued; ++r) mbar_wait(rec_bar(r), (r >> 1) & 1);
+  }
+}
+
 // Tile shapes the staged kernel is built for: {precision, MC, TY, TZ}.
 template <typename T> struct StagedCfgs;
 template <> struct StagedCfgs<float> {
@@ -851,6 +1236,7 @@ template <> struct StagedCfgs<double> {
 };
 constexpr int kStagedCfgs = 4;
 constexpr int kDirect = -2;      // staged_cfg value selecting the direct kernel
+constexpr int kDefaultTma = 1;   // TMA shape taken when no tile was tuned or set
 
 struct StagedGeom { int tiles_y, tiles_z, chunks, xsplit, xlen, ctas; };
 
@@ -924,6 +1310,117 @@ static int launch_staged(int cfg, const qdkp_operator* op, const T* rec, const v
   }
 }
 
+// ---- TMA kernel launch ------------------------------------------------------------------------
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                  const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link against libcuda)
+static EncodeTiledFn tensor_map_encoder() {
+  static EncodeTiledFn fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess && q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  return fn;
+}
+
+// TMA tile shapes {TY, TZ, column pairs per CTA, ring slots}; staged_cfg kTmaBase + i selects
+// shape i (complex64 only).
+struct TmaCfgs {
+  using C0 = Tma<6, 16, 2, 4>;
+  using C1 = Tma<6, 16, 2, 5>;
+  using C2 = Tma<8, 12, 2, 5>;
+  using C3 = Tma<4, 24, 2, 4>;
+};
+constexpr int kTmaBase = 4;
+constexpr int kTmaCfgs = 4;
+
+template <class G>
+static bool tma_fits(const qdkp_operator* op, const void* X, int64_t ldx, int m) {
+  // tensor-map rules: 16-byte aligned base and strides; every box no larger than its tensor
+  return op->n_bands == 8 && ((uintptr_t)X & 15) == 0 && ldx % 2 == 0 && m >= G::MC &&
+         op->ny >= G::PY && op->nz >= G::PZ && op->nzp >= G::TZ && tensor_map_encoder() != nullptr;
+}
+
+static bool tma_fits_cfg(int i, const qdkp_operator* op, const void* X, int64_t ldx, int m) {
+  switch (i) {
+    case 0: return tma_fits<TmaCfgs::C0>(op, X, ldx, m);
+    case 1: return tma_fits<TmaCfgs::C1>(op, X, ldx, m);
+    case 2: return tma_fits<TmaCfgs::C2>(op, X, ldx, m);
+    default: return tma_fits<TmaCfgs::C3>(op, X, ldx, m);
+  }
+}
+
+template <class G>
+static int launch_tma_g(const qdkp_operator* op, const void* X, int ldx, void* Y, int ldy, int m,
+                        float shift, float cb, int sms, cudaStream_t st) {
+  const EncodeTiledFn enc = tensor_map_encoder();
+  static bool attr_done = false;     // per instantiation; the attribute is per device function
+  if (!attr_done) {
+    QDKP_CUDA_TRY(cudaFuncSetAttribute(kp_apply_tma_kernel<G>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::SMEM));
+    attr_done = true;
+  }
+  const cuuint64_t N = (cuuint64_t)op->n_sites, ld = (cuuint64_t)ldx;
+  CUtensorMap tmx, tmr;
+  // X as [band][x][y][z][column] with the column innermost (8-byte elements)
+  const cuuint64_t xdim[5] = {(cuuint64_t)m, (cuuint64_t)op->nz, (cuuint64_t)op->ny,
+                              (cuuint64_t)op->nx, 8};
+  const cuuint64_t xstr[4] = {ld * 8, (cuuint64_t)op->nz * ld * 8,
+                              (cuuint64_t)op->ny * op->nz * ld * 8, N * ld * 8};
+  const cuuint32_t xbox[5] = {(cuuint32_t)G::MC, (cuuint32_t)G::PZ, (cuuint32_t)G::PY, 1, 8};
+  const cuuint32_t ones[5] = {1, 1, 1, 1, 1};
+  CUresult r = enc(&tmx, CU_TENSOR_MAP_DATA_TYPE_INT64, 5, const_cast<void*>(X), xdim, xstr,
+                   xbox, ones, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_error("cuTensorMapEncodeTiled failed for the X block (code " + std::to_string((int)r) + ")");
+    return QDKP_ERR_CUDA;
+  }
+  // the FP32 record as [entry][x][y][z_padded]
+  const cuuint64_t NP = (cuuint64_t)op->nx * op->ny * op->nzp;
+  const cuuint64_t rdim[4] = {(cuuint64_t)op->nzp, (cuuint64_t)op->ny, (cuuint64_t)op->nx,
+                              (cuuint64_t)K_COUNT};
+  const cuuint64_t rstr[3] = {(cuuint64_t)op->nzp * 4, (cuuint64_t)op->ny * op->nzp * 4, NP * 4};
+  const cuuint32_t rbox[4] = {(cuuint32_t)G::TZ, (cuuint32_t)G::TY, 1, (cuuint32_t)K_COUNT};
+  r = enc(&tmr, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, op->rec32, rdim, rstr, rbox, ones,
+          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_error("cuTensorMapEncodeTiled failed for the record (code " + std::to_string((int)r) + ")");
+    return QDKP_ERR_CUDA;
+  }
+  const StagedGeom g = staged_geom(op->nx, op->ny, op->nz, m, G::MC, G::TY, G::TZ, sms);
+  TmaArgs a;
+  a.Y = static_cast<float2*>(Y);
+  a.N = (int)op->n_sites; a.nx = op->nx; a.ny = op->ny; a.nz = op->nz;
+  a.ldy = ldy; a.m = m;
+  a.tiles_z = g.tiles_z; a.chunks = g.chunks; a.xsplit = g.xsplit; a.xlen = g.xlen;
+  a.vec_store = ((uintptr_t)Y & 15) == 0 && ldy % 2 == 0;
+  a.shift = shift; a.cb = cb;
+  kp_apply_tma_kernel<G><<<g.ctas, G::THREADS, G::SMEM, st>>>(tmx, tmr, a);
+  count_launch();
+  QDKP_CUDA_TRY(cudaGetLastError());
+  return QDKP_OK;
+}
+
+static int launch_tma(int i, const qdkp_operator* op, const void* X, int ldx, void* Y, int ldy,
+                      int m, float shift, float cb, int sms, cudaStream_t st) {
+  switch (i) {
+    case 0: return launch_tma_g<TmaCfgs::C0>(op, X, ldx, Y, ldy, m, shift, cb, sms, st);
+    case 1: return launch_tma_g<TmaCfgs::C1>(op, X, ldx, Y, ldy, m, shift, cb, sms, st);
+    case 2: return launch_tma_g<TmaCfgs::C2>(op, X, ldx, Y, ldy, m, shift, cb, sms, st);
+    default: return launch_tma_g<TmaCfgs::C3>(op, X, ldx, Y, ldy, m, shift, cb, sms, st);
+  }
+}
+
 int launch_apply_multi(const HXSlot* slots_dev, int nslots, int total_tiles, int precision,
                        cudaStream_t st) {
   if (total_tiles <= 0) return QDKP_OK;
@@ -978,11 +1475,13 @@ static int num_sms(int device) {
 // Default kernel for a launch without a tuned choice, from measurements of both kernels over
 // grids of 23x23x20 to 128x128x96 and blocks of 12 and 24 columns on B200: complex128 is FP64-
 // issue bound and the direct kernel (more resident warps) is as fast or faster everywhere;
-// complex64 takes the staged kernel on grids of 50k sites and more, where its shared-memory
-// reuse pays, with the tile shape that pads the (y, z) plane least. qdkp_operator_tune refines
-// this per operator.
-static int pick_staged_cfg(const qdkp_operator* op, int precision) {
+// complex64 takes a shared-memory kernel on grids of 50k sites and more, where its reuse pays:
+// the TMA kernel where its tensor maps fit, else the cp.async staged kernel with the tile shape
+// that pads the (y, z) plane least. qdkp_operator_tune refines this per operator.
+static int pick_staged_cfg(const qdkp_operator* op, int precision, const void* X, int64_t ldx,
+                           int m) {
   if (precision == QDKP_C128 || op->n_sites < 50000) return kDirect;
+  if (tma_fits_cfg(kDefaultTma, op, X, ldx, m)) return kTmaBase + kDefaultTma;
   // the four-column shapes (0, 1) measured fastest on every grid; pick the one that pads less
   static const int shape[2][2] = {{8, 12}, {6, 16}};   // TY, TZ
   int best = 0;
@@ -1007,7 +1506,13 @@ static int launch_apply_t(const qdkp_operator* op, const T* rec, const void* X, 
   const T shift = shifted ? (T)(-sigma) : T(0);
   const T cb = (T)apply_cb_weight(op);
   const int forced = op->staged_cfg[precision == QDKP_C64];
-  const int cfg = forced == QDKP_TILE_AUTO ? pick_staged_cfg(op, precision) : forced;
+  int cfg = forced == QDKP_TILE_AUTO ? pick_staged_cfg(op, precision, X, ldx, m) : forced;
+  if (cfg >= kTmaBase) {
+    if (std::is_same<T, float>::value && tma_fits_cfg(cfg - kTmaBase, op, X, ldx, m))
+      return launch_tma(cfg - kTmaBase, op, X, (int)ldx, Y, (int)ldy, m, (float)shift, (float)cb,
+                        num_sms(op->device), st);
+    cfg = 1;       // a block the tensor maps cannot describe: the cp.async staged kernel
+  }
   if (op->n_bands == 8 && cfg >= 0 && ((uintptr_t)X % sizeof(cplx<T>)) == 0)
     return launch_staged<T>(cfg, op, rec, X, (int)ldx, Y, (int)ldy, m, shift, cb,
                             num_sms(op->device), st);
@@ -1053,7 +1558,9 @@ extern "C" {
 int qdkp_operator_set_tile(qdkp_operator* op, int precision, int tile) {
   QDKP_CHECK_ARG(op != nullptr, "operator must not be NULL");
   QDKP_CHECK_ARG(precision == QDKP_C128 || precision == QDKP_C64, "bad precision");
-  QDKP_CHECK_ARG(tile >= QDKP_TILE_DIRECT && tile < kStagedCfgs, "tile out of range");
+  QDKP_CHECK_ARG(tile >= QDKP_TILE_DIRECT && tile < kStagedCfgs + kTmaCfgs, "tile out of range");
+  QDKP_CHECK_ARG(precision == QDKP_C64 || tile < kStagedCfgs,
+                 "the TMA tile shapes are built for complex64 only");
   op->staged_cfg[precision == QDKP_C64] = tile;
   return QDKP_OK;
 }
@@ -1080,9 +1587,15 @@ int qdkp_operator_tune(qdkp_operator* op, const void* X, int64_t ldx, void* Y, i
   int best = saved;
   float best_ms = 3.4e38f;
   int rc = QDKP_OK;
-  const int first = op->n_bands == 8 ? 0 : kStagedCfgs;   // 6/4-band slices: direct only
-  for (int c = first; c <= kStagedCfgs && rc == QDKP_OK; ++c) {
-    const int tile = c < kStagedCfgs ? c : kDirect;
+  // candidates: the staged shapes, the TMA shapes (complex64), the direct kernel last; the
+  // seconds array has one entry per candidate, -1 for one that does not apply
+  const int ncand = kStagedCfgs + kTmaCfgs + 1;
+  for (int c = 0; c < ncand && rc == QDKP_OK; ++c) {
+    const int tile = c < kStagedCfgs + kTmaCfgs ? c : kDirect;
+    if (seconds) seconds[c] = -1.0;
+    if (op->n_bands != 8 && tile != kDirect) continue;                // 6/4-band: direct only
+    if (tile >= kTmaBase && (precision != QDKP_C64 ||
+                             !tma_fits_cfg(tile - kTmaBase, op, X, ldx, m))) continue;
     op->staged_cfg[pi] = tile;
     rc = launch_apply(op, X, ldx, Y, ldy, m, 0.0, 0, precision, st);      // warm-up
     if (rc != QDKP_OK) break;
@@ -1093,7 +1606,7 @@ int qdkp_operator_tune(qdkp_operator* op, const void* X, int64_t ldx, void* Y, i
     float ms = 0.f;
     if (cudaEventRecord(e1, st) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
         cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) { rc = QDKP_ERR_CUDA; break; }
-    if (seconds) seconds[c - first] = ms * 1e-3 / reps;
+    if (seconds) seconds[c] = ms * 1e-3 / reps;
     if (ms < best_ms) { best_ms = ms; best = tile; }
   }
   cudaEventDestroy(e0);
@@ -1101,6 +1614,21 @@ int qdkp_operator_tune(qdkp_operator* op, const void* X, int64_t ldx, void* Y, i
   op->staged_cfg[pi] = rc == QDKP_OK ? best : saved;
   if (rc == QDKP_ERR_CUDA) set_error("qdkp_operator_tune: CUDA event failure");
   return rc;
+}
+
+int qdkp_device_fault(int device, int clear, int* fault) {
+  QDKP_CHECK_ARG(fault != nullptr, "NULL argument");
+  int prev = 0;
+  QDKP_CUDA_TRY(cudaGetDevice(&prev));
+  QDKP_CUDA_TRY(cudaSetDevice(device));
+  cudaError_t e = cudaMemcpyFromSymbol(fault, g_apply_fault, sizeof(int));
+  if (e == cudaSuccess && clear) {
+    const int zero = 0;
+    e = cudaMemcpyToSymbol(g_apply_fault, &zero, sizeof(int));
+  }
+  cudaSetDevice(prev);
+  QDKP_CUDA_TRY(e);
+  return QDKP_OK;
 }
 
 }  // extern "C"

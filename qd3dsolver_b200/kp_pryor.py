@@ -205,7 +205,8 @@ class KPOperator(spla.LinearOperator):
 
     def set_tile(self, tile, precision=_lib.C128):
         """Force the H.X kernel for this operator and precision: a staged tile shape
-        0..TILE_COUNT-1, TILE_DIRECT, or TILE_AUTO (padding heuristic)."""
+        0..TILE_COUNT-1 (TILE_TMA0.. are the complex64 TMA shapes), TILE_DIRECT, or TILE_AUTO
+        (heuristic)."""
         check(lib().qdkp_operator_set_tile(self.handle, precision, int(tile)),
               'qdkp_operator_set_tile')
 
@@ -230,9 +231,7 @@ class KPOperator(spla.LinearOperator):
         check(lib().qdkp_operator_tune(self.handle, X.data_ptr(), m, Y.data_ptr(), m, m, prec,
                                        int(reps), secs, stream), 'qdkp_operator_tune')
         tiles = list(range(_lib.TILE_COUNT)) + [_lib.TILE_DIRECT]
-        if self.n_bands != 8:
-            return {_lib.TILE_DIRECT: secs[0]}
-        return {t: secs[i] for i, t in enumerate(tiles)}
+        return {t: secs[i] for i, t in enumerate(tiles) if secs[i] >= 0}
 
     def negated(self):
         """-H as a second device operator (same fields, sign flipped in the stencil)."""

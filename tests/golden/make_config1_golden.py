@@ -85,8 +85,8 @@ def main():
             lam, _, hist = spla.lobpcg(F, X0, largest=False, tol=1e-7, maxiter=a.iterations,
                                        retResidualNormsHistory=True)
         dt = time.time() - t0
-        out[band] = dict(sigma=sigma, mu=np.asarray(lam).tolist(),
-                         residual_history=np.asarray(hist).tolist(), seconds=dt,
+        out[band] = dict(sigma=sigma, mu=np.real(np.asarray(lam)).tolist(),
+                         residual_history=np.abs(np.asarray(hist)).tolist(), seconds=dt,
                          seconds_per_iteration=dt / (a.iterations + 1))
         print(band, f"{dt:.1f}s", flush=True)
     out['cpu_count'] = os.cpu_count()
