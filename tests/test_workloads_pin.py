@@ -86,3 +86,17 @@ def test_fields_of_a_dot(golden, tag):
     assert wl.hole_sigma(Ev, st, f8['b'], f8['d'], f8['delta_so'], mask) == \
         pytest.approx(c['sigma_h'], abs=1e-12)
     assert float(Ec[mask].min()) == pytest.approx(c['sigma_e'], abs=1e-12)
+
+
+def test_48x48x36_pyramid_fields_match_the_reference():
+    """The 48x48x36 pyramid workload (workloads.config1) against the per-field sums, sigmas and
+    dot volume the reference recorded for the same geometry (make_config1_golden.py)."""
+    with open(os.path.join(GOLDEN, 'config1_iterates.json')) as fh:
+        ref = json.load(fh)
+    w = wl.config1()
+    assert list(w.shape) == ref['shape'] and int(w.mask.sum()) == ref['mask_cells']
+    assert w.sigma['cb'] == pytest.approx(ref['sigma_e'], abs=1e-12)
+    assert w.sigma['vb'] == pytest.approx(ref['sigma_h'], abs=1e-12)
+    for k, v in ref['field_sums'].items():
+        scale = float(np.abs(w.fields[k]).sum())
+        assert abs(float(np.sum(w.fields[k])) - v) <= 1e-12 * scale + 1e-12, k
