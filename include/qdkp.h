@@ -299,6 +299,23 @@ int qdkp_residuals(const qdkp_operator* op, const void* V, int64_t ldv, int k,
                    const double* E_in, double* rq, double* res, void* ws, size_t ws_bytes,
                    void* stream);
 
+/*
+ * Localisation and Kramers pairing of eigenvector blocks (pryor_fig4.localization,
+ * pryor_fig4.py:179-193, and pryor_fig4.kramers_levels, pryor_fig4.py:222-236).
+ * V: device (n, k) block, complex128 or complex64 (`precision`), leading dimension ldv, rows
+ * band-major as H's; mask: device array of n_sites bytes, nonzero inside the dot.
+ * loc[k] (host): sum over dot sites and bands of |V_j|^2 over the same sum over every site.
+ * E (host, may be NULL): k energies in the order to pair; consecutive entries form a pair, and
+ * levels[k/2], level_loc[k/2] receive each pair's mean energy and mean localisation and
+ * *worst_split the largest within-pair |E_2p+1 - E_2p|. Sums run in a fixed order: the result is
+ * the same for any launch and any other work on the GPU. Synchronous; k <= 128.
+ */
+size_t qdkp_state_summary_workspace_size(const qdkp_operator* op, int k);
+int qdkp_state_summary(const qdkp_operator* op, const void* V, int64_t ldv, int k, int precision,
+                       const unsigned char* mask, const double* E, double* loc, double* levels,
+                       double* level_loc, double* worst_split, void* ws, size_t ws_bytes,
+                       void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -114,6 +114,12 @@ _SIGNATURES = {
                                       ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
                                       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t,
                                       ctypes.c_void_p]),
+    'qdkp_state_summary_workspace_size': (ctypes.c_size_t, [ctypes.c_void_p, ctypes.c_int]),
+    'qdkp_state_summary': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+                                          ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                          ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                          ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                          ctypes.c_size_t, ctypes.c_void_p]),
 }
 
 # Every symbol include/qdkp.h declares (checked by the CPU test suite).

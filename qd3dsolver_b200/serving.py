@@ -26,6 +26,7 @@ import numpy as np
 
 from . import _lib
 from ._lib import check, lib
+from . import post
 from .eigensolvers import start_block, _device_residuals
 from .kp_pryor import KPOperator
 
@@ -49,6 +50,8 @@ class Request:
     precision: str = 'c128'        # 'c128', or 'mixed' (complex64 search, complex128 finish)
     mixed_tol: float = 1e-4        # residual at which a mixed request leaves complex64
     mixed_stall: int = 30          # ... or after this many iterations without a new best
+    mask: object = None            # dot mask (grid-shaped bool): results carry localisation and
+                                   # Kramers levels (pryor_fig4.localization / kramers_levels)
     # filled in by the engine
     slot: int = -1
     t_arrive: float = 0.0
@@ -210,6 +213,8 @@ class Engine:
                         ticks=dict(r.ticks), mu=lam,
                         status=_lib.LOBPCG_STATUS.get(info.status, 'unknown'),
                         converged=bool(res.max() < certify_tol))
+        if r.mask is not None:
+            r.result.update(post.state_summary(r.H, Vk, r.mask, E))
         del ws, X0
         return r
 

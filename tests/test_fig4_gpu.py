@@ -41,3 +41,55 @@ def test_fig4_b10_levels_match_reference(fig4, band):
     nb = np.sort(np.array(ref['notebook'][band]))
     assert np.abs(np.sort(lvl) - nb).max() <= 5.1e-5           # notebook prints 4 decimals
     assert np.abs(np.sort(lloc) - np.sort(np.array(ref[band]['loc']).reshape(-1, 2).mean(1))).max() < 1e-3
+
+
+@pytest.mark.parametrize('band', ['cb', 'vb'])
+def test_device_localization_and_kramers_levels(fig4, band):
+    """qdkp_state_summary (the device form of pryor_fig4.localization and kramers_levels) on the
+    GPU solve of the b = 10 nm fields: per-state localisation equals the reference's own values
+    (gauge-invariant within a Kramers pair) and the oracle's on the same vectors; levels pair up."""
+    from qd3dsolver_b200 import eigensolvers as eg, post as gpost
+    from oracle import post
+    w, H, ref = fig4
+    E, V, info = eg.solve_interior(H, k=8, sigma=w.sigma[band], tol=1e-8, maxiter=8000,
+                                   verbose=False)
+    order = np.argsort(E) if band == 'cb' else np.argsort(-E)    # pryor_fig4.bound_states
+    E, V = E[order], V[:, order]
+    s = gpost.state_summary(H, V, w.mask, E)
+    loc_o = post.localization(V, w.mask)
+    assert np.abs(s['loc'] - loc_o).max() < 1e-13
+    lvl, lloc, worst = post.kramers_levels(E, loc_o)
+    assert np.abs(s['levels'] - lvl).max() < 1e-15 and np.abs(s['level_loc'] - lloc).max() < 1e-13
+    assert s['kramers_split'] == pytest.approx(worst, abs=1e-18) and worst < 1e-7
+    r = ref[band]
+    assert np.abs(np.sort(s['levels']) - np.sort(r['levels'])).max() < 1e-6
+    assert np.abs(np.sort(s['loc']) - np.sort(r['loc'])).max() < 1e-5
+    lv, ll, wv = gpost.kramers_levels(E, s['loc'])
+    assert np.allclose(lv, s['levels']) and wv == pytest.approx(s['kramers_split'], abs=1e-18)
+
+
+def test_state_summary_block_layouts():
+    """The reduction on random blocks: complex128 and complex64, odd column counts, a leading
+    dimension wider than the block, against numpy."""
+    import torch
+    from qd3dsolver_b200 import kp_pryor as kpg, post as gpost, workloads as wl
+    w = wl.fig4_from_fixture(os.path.join(GOLDEN, 'fig4_b10_fields.npz'))
+    f = w.fields
+    H = kpg.confined_hamiltonian(kpg.GridOperators(w.shape, w.h), f, 8,
+                                 strain={k: f[k] for k in wl.STRAIN_KEYS})
+    rng = np.random.default_rng(4)
+    n = H.shape[0]
+    for k, ld, dt, tol in ((7, 9, torch.complex128, 1e-13), (12, 12, torch.complex64, 1e-6),
+                           (1, 1, torch.complex128, 1e-13)):
+        X = rng.standard_normal((n, ld)) + 1j * rng.standard_normal((n, ld))
+        X[:, :k] *= np.exp(rng.standard_normal((1, k)))
+        Xd = torch.from_numpy(X).to(dt).cuda()[:, :k]
+        Xh = Xd.cpu().numpy().astype(np.complex128)
+        rho = (np.abs(Xh.reshape(8, -1, k)) ** 2).sum(axis=0)
+        ref = rho[w.mask.ravel()].sum(axis=0) / rho.sum(axis=0)
+        E = np.sort(rng.standard_normal(k))
+        s = gpost.state_summary(H, Xd, w.mask, E)
+        assert np.abs(s['loc'] - ref).max() < tol, (k, dt)
+        if k >= 2:
+            assert np.allclose(s['levels'], E[:k // 2 * 2].reshape(-1, 2).mean(1), atol=1e-15)
+    H.close()
