@@ -316,6 +316,21 @@ int qdkp_state_summary(const qdkp_operator* op, const void* V, int64_t ldv, int 
                        double* level_loc, double* worst_split, void* ws, size_t ws_bytes,
                        void* stream);
 
+/*
+ * Local band edges at k = 0 from the operator's own fields (kp_pryor.local_band_edges,
+ * kp_pryor.py:469-531, with the hydrostatic shift already in Ev, and kp_pryor.hole_sigma,
+ * kp_pryor.py:156-191): per site the three Kramers-paired levels v1 >= v2 >= v3 of the 6x6
+ * valence block (Ev, delta_so, the Bir-Pikus terms of the strain fields with b and d).
+ * levels (device, 3 x n_sites doubles, may be NULL) receives v1, v2, v3; *top_v1 (host) the
+ * largest v1 over the sites where mask (device, n_sites bytes, may be NULL for every site) is
+ * nonzero -- hole_sigma with margin 0; *kramers_split (host, may be NULL) the largest splitting
+ * within a level pair over all sites. Operators of 8 or 6 bands. Synchronous.
+ */
+size_t qdkp_local_band_edges_workspace_size(const qdkp_operator* op);
+int qdkp_local_band_edges(const qdkp_operator* op, const unsigned char* mask, double* levels,
+                          double* top_v1, double* kramers_split, void* ws, size_t ws_bytes,
+                          void* stream);
+
 #ifdef __cplusplus
 }
 #endif

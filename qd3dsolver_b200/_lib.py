@@ -120,6 +120,10 @@ _SIGNATURES = {
                                           ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                           ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                           ctypes.c_size_t, ctypes.c_void_p]),
+    'qdkp_local_band_edges_workspace_size': (ctypes.c_size_t, [ctypes.c_void_p]),
+    'qdkp_local_band_edges': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                             ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                             ctypes.c_size_t, ctypes.c_void_p]),
 }
 
 # Every symbol include/qdkp.h declares (checked by the CPU test suite).

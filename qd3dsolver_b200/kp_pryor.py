@@ -233,6 +233,34 @@ class KPOperator(spla.LinearOperator):
         tiles = list(range(_lib.TILE_COUNT)) + [_lib.TILE_DIRECT]
         return {t: secs[i] for i, t in enumerate(tiles) if secs[i] >= 0}
 
+    def band_edges(self, mask=None, levels=False):
+        """k = 0 valence levels of every site from this operator's own fields (Ev with the
+        hydrostatic shift, strain, b, d, delta_so): returns dict(top_v1 = max v1 over `mask`
+        (hole_sigma with margin 0), kramers = largest in-pair splitting, and with levels=True
+        v1, v2, v3 as grid-shaped host arrays)."""
+        torch = _torch()
+        dev = f'cuda:{self.device}'
+        md = None
+        if mask is not None:
+            md = torch.from_numpy(np.ascontiguousarray(
+                np.asarray(mask, dtype=bool).ravel()).view(np.uint8).copy()).to(dev)
+            if md.numel() != self.n_sites:
+                raise ValueError("mask must have one entry per grid site")
+        lv = torch.empty(3 * self.n_sites, dtype=torch.float64, device=dev) if levels else None
+        need = int(lib().qdkp_local_band_edges_workspace_size(self.handle))
+        ws = torch.empty(need, dtype=torch.uint8, device=dev)
+        top, split = ctypes.c_double(), ctypes.c_double()
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        check(lib().qdkp_local_band_edges(self.handle, md.data_ptr() if md is not None else None,
+                                          lv.data_ptr() if lv is not None else None,
+                                          ctypes.byref(top), ctypes.byref(split), ws.data_ptr(),
+                                          ws.numel(), stream), 'qdkp_local_band_edges')
+        out = dict(top_v1=top.value, kramers=split.value)
+        if levels:
+            v = lv.cpu().numpy().reshape(3, *self.grid_shape)
+            out.update(v1=v[0], v2=v[1], v3=v[2])
+        return out
+
     def negated(self):
         """-H as a second device operator (same fields, sign flipped in the stencil)."""
         f = {k: (v.reshape(self.grid_shape) if v is not None else None)
@@ -295,3 +323,56 @@ def confined_hamiltonian(ops, fields, n_bands=8, hole_convention=False, strain=N
         if f[k] is not None and f[k].shape != shape:
             f[k] = np.broadcast_to(f[k], shape).copy()
     return KPOperator(shape, ops.h, n_bands, flags, f)
+
+
+def _edge_operator(strain, Ev, delta_so, b, d):
+    """A device operator carrying only the fields the k = 0 valence block reads."""
+    st = _strain_dict(strain)
+    arrs = [np.asarray(Ev, dtype=float), np.asarray(delta_so, dtype=float),
+            np.asarray(b, dtype=float), np.asarray(d, dtype=float)] + list(st.values())
+    shape = np.broadcast_shapes(*[a.shape for a in arrs])
+    grid = shape if len(shape) == 3 else (int(np.prod(shape)) if shape else 1, 1, 1)
+
+    def g(a):
+        return np.broadcast_to(np.asarray(a, dtype=float), shape).reshape(grid).copy()
+    zero = np.zeros(grid)
+    f = dict(gamma1=zero, gamma2=zero, gamma3=zero, P0=zero, Ec=zero, Ev=g(Ev),
+             delta_so=g(delta_so), b=g(b), d=g(d))
+    f.update({k: g(v) for k, v in st.items()})
+    return KPOperator(grid, 1.0, 8, _lib.STRAIN, f), shape
+
+
+def local_band_edges(strain, Ev, Ec, delta_so, a_c, a_v, b, d, hydrostatic_applied=False):
+    """kp_pryor.local_band_edges (kp_pryor.py:469-531) on the GPU: dict(cb, v1, v2, v3,
+    kramers) with v1 >= v2 >= v3 the Kramers-paired k = 0 valence levels. Same arguments and
+    broadcasting; `strain` is a StrainTensor-like object or a dict of the six components."""
+    st = _strain_dict(strain)
+    tr = st['exx'] + st['eyy'] + st['ezz']
+    Ev_s = np.asarray(Ev, dtype=float) if hydrostatic_applied else np.asarray(Ev) - a_v * tr
+    Ec_s = np.asarray(Ec, dtype=float) if hydrostatic_applied else np.asarray(Ec) + a_c * tr
+    H, shape = _edge_operator(st, Ev_s, delta_so, b, d)
+    try:
+        e = H.band_edges(levels=True)
+    finally:
+        H.close()
+    return dict(cb=np.broadcast_to(Ec_s, shape).copy(), v1=e['v1'].reshape(shape),
+                v2=e['v2'].reshape(shape), v3=e['v3'].reshape(shape), kramers=e['kramers'])
+
+
+def hole_sigma(Ev_field, strain, b_field, d_field, delta_so_field, inside_mask=None,
+               margin=0.0, hydrostatic_applied=True):
+    """kp_pryor.hole_sigma (kp_pryor.py:156-191) on the GPU: the exact local valence-band top,
+    max of v1 inside the mask, plus `margin`."""
+    st = _strain_dict(strain)
+    Ev_s = np.asarray(Ev_field, dtype=float)
+    if not hydrostatic_applied:
+        raise NotImplementedError("hole_sigma passes a_v = 0, so hydrostatic_applied=False "
+                                  "does not change the result; pass the shifted Ev")
+    H, shape = _edge_operator(st, Ev_s, delta_so_field, b_field, d_field)
+    try:
+        mask = None if inside_mask is None else np.broadcast_to(inside_mask, shape)
+        top = H.band_edges(mask=mask)['top_v1']
+    finally:
+        H.close()
+    return float(top) + margin
+
