@@ -331,6 +331,28 @@ int qdkp_local_band_edges(const qdkp_operator* op, const unsigned char* mask, do
                           double* top_v1, double* kramers_split, void* ws, size_t ws_bytes,
                           void* stream);
 
+/*
+ * Host input producers on the device: the homogeneous Fourier strain of a dot
+ * (strain_fourier.solve_strain, strain_fourier.py:142-235) and the first-order piezoelectric
+ * potential (piezoelectric.potential with polarization / charge_density, piezoelectric.py:59-99),
+ * on the periodic (nx, ny, nz) cell of spacing h (C order, z fastest).
+ *   qdkp_fourier_strain: mask (device, n_sites bytes); strain (device, 6 x n_sites doubles) gets
+ *     the ELASTIC strain exx, eyy, ezz, exy, eyz, ezx (tensor shear convention).
+ *   qdkp_piezo_potential: strain (device, 6 x n_sites, that order), e14 (device field, n_sites),
+ *     scalar eps_r; phi (device, n_sites) in volts.
+ * The 3-D transforms are cuFFT double-complex plans, made once per grid shape (cuFFT keeps its
+ * own small tables on the device) and run with the work area in the caller's workspace.
+ * Asynchronous on `stream`.
+ */
+size_t qdkp_fourier_strain_workspace_size(int nx, int ny, int nz);
+int qdkp_fourier_strain(int nx, int ny, int nz, double h, const unsigned char* mask,
+                        double eps_star, double C11, double C12, double C44, double* strain,
+                        void* ws, size_t ws_bytes, void* stream);
+size_t qdkp_piezo_potential_workspace_size(int nx, int ny, int nz);
+int qdkp_piezo_potential(int nx, int ny, int nz, double h, const double* strain,
+                         const double* e14, double eps_r, double sign, double* phi, void* ws,
+                         size_t ws_bytes, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -124,6 +124,15 @@ _SIGNATURES = {
     'qdkp_local_band_edges': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                              ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                              ctypes.c_size_t, ctypes.c_void_p]),
+    'qdkp_fourier_strain_workspace_size': (ctypes.c_size_t, [ctypes.c_int] * 3),
+    'qdkp_fourier_strain': (ctypes.c_int, [ctypes.c_int] * 3 + [ctypes.c_double, ctypes.c_void_p]
+                            + [ctypes.c_double] * 4 + [ctypes.c_void_p, ctypes.c_void_p,
+                                                       ctypes.c_size_t, ctypes.c_void_p]),
+    'qdkp_piezo_potential_workspace_size': (ctypes.c_size_t, [ctypes.c_int] * 3),
+    'qdkp_piezo_potential': (ctypes.c_int, [ctypes.c_int] * 3 + [ctypes.c_double,
+                             ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double, ctypes.c_double,
+                             ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t,
+                             ctypes.c_void_p]),
 }
 
 # Every symbol include/qdkp.h declares (checked by the CPU test suite).

@@ -63,7 +63,7 @@ def build(verbose_ptxas=False, force=False):
             if verbose_ptxas:
                 sys.stderr.write(f"== {f}\n" + r.stderr)
     tmp = LIB + '.tmp'
-    cmd = [NVCC] + ARCH + ['-shared', '-o', tmp] + objs + ['-lcudart']
+    cmd = [NVCC] + ARCH + ['-shared', '-o', tmp] + objs + ['-lcudart', '-lcufft']
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
