@@ -1145,6 +1145,29 @@ int qdkp_engine_retire(qdkp_engine* e, int slot, double* lambda_out, void* V,
     RTRY(copy1(h, d.X, m, d.best, st));
     best_iter = s.iter + 1;
   }
+  if (s.status == QDKP_LOBPCG_NONFINITE) {
+    // a non-finite residual: no Rayleigh-Ritz on it; the last iterate is returned as it is with
+    // NaN Ritz values and residuals, and the slot is freed for the next request
+    if (d.prec == QDKP_C64)
+      RTRY((launch_copy<float, double>(reinterpret_cast<const float2*>(d.X), m, m, n,
+                                       static_cast<double2*>(V), m, st)));
+    else
+      RTRY((launch_copy<double, double>(reinterpret_cast<const double2*>(d.X), m, m, n,
+                                        static_cast<double2*>(V), m, st)));
+    QDKP_CUDA_TRY(cudaStreamSynchronize(st));
+    for (int j = 0; j < m; ++j) lambda_out[j] = std::numeric_limits<double>::quiet_NaN();
+    if (residuals_out)
+      for (int j = 0; j < m; ++j) residuals_out[j] = std::numeric_limits<double>::quiet_NaN();
+    std::memset(info, 0, sizeof(*info));
+    info->iterations = std::min(s.iter + 1, h.prm.maxiter + 3);
+    info->best_iteration = best_iter;
+    info->status = s.status;
+    info->explicit_gram = s.explicit_gram;
+    info->best_mean_residual = s.smallest;
+    h.used = false;
+    e->dirty = true;
+    return QDKP_OK;
+  }
   // final Rayleigh-Ritz on the best iterate (lobpcg.py:1009-1060)
   RTRY(apply_folded(h, d.best, m, d.AX, st));
   RTRY(gram1(h, d.best, d.AX, m, d.gT, st));

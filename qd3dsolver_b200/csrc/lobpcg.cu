@@ -509,6 +509,25 @@ int qdkp_lobpcg_solve(const qdkp_operator* op, const qdkp_lobpcg_params* prm, co
     }
   }
   if (!have_best) TRY(launch_copy(b.X, m, m, n, b.best, m, st));
+  if (status == QDKP_LOBPCG_NONFINITE) {
+    // a non-finite residual: nothing to refine; the iterate is returned as it is, Ritz values NaN
+    TRY(launch_copy(b.best, m, m, n, (double2*)V, m, st));
+    for (int j = 0; j < m; ++j) lambda_out[j] = std::numeric_limits<double>::quiet_NaN();
+    const int rows = std::min(it + 1, hist_rows);
+    if (resid_history) std::memcpy(resid_history, hist.data(), (size_t)rows * m * sizeof(double));
+    info->iterations = rows;
+    info->best_iteration = have_best ? best_iter : -1;
+    info->status = status;
+    info->explicit_gram = explicit_gram;
+    info->best_mean_residual = smallest;
+    info->hx_applications = s.applies * (prm->folded ? 2 : 1);
+    info->hx_launches = s.hx_launches;
+    info->hx_bytes = s.hx_bytes;
+    QDKP_CUDA_TRY(cudaStreamSynchronize(st));
+    info->hx_seconds = prm->time_hx ? s.hx_seconds() : 0.0;
+    info->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+    return QDKP_OK;
+  }
   // ---- final Rayleigh-Ritz on the best iterate (scipy lobpcg.py:1009-1060) -----------------
   TRY(s.applyA(b.best, m, b.AX));
   TRY(s.gram(blist({{b.best, m}}, m), blist({{b.AX, m}}, m), b.gT));

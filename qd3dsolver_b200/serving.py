@@ -160,6 +160,7 @@ class Engine:
         check(lib().qdkp_engine_poll(self._h, state, status, iters, self.stream),
               'qdkp_engine_poll')
         self._iters = list(iters)
+        self._status = list(status)
         return list(state), list(status), list(iters)
 
     def promote(self, slot):
@@ -181,7 +182,8 @@ class Engine:
         slot id for a promotion, else None."""
         r = self._slots[slot][0]
         r.ticks[r.phase] = r.ticks.get(r.phase, 0) + int(getattr(self, '_iters', [0] * (slot + 1))[slot])
-        if r.phase == 'c64':
+        nonfinite = getattr(self, '_status', [0] * (slot + 1))[slot] == 4
+        if r.phase == 'c64' and not nonfinite:          # a NaN search is not promoted
             return self.promote(slot)
         self.retire(slot)
         return None
