@@ -93,3 +93,28 @@ def test_state_summary_block_layouts():
         if k >= 2:
             assert np.allclose(s['levels'], E[:k // 2 * 2].reshape(-1, 2).mean(1), atol=1e-15)
     H.close()
+
+
+@pytest.mark.parametrize('base', [6, 18])
+def test_served_mixed_passes_the_counting_rule(base):
+    """The served mixed-precision form (complex64 search, complex128 finish) on the smallest and
+    largest Fig-4 sizes, with the benchmark's tolerance: every eigenpair of both bands within
+    1e-6 eV of the reference's own solve, Kramers pairs within 1e-7 eV, and relative residual
+    ||Hv - Ev|| / ||H||_2 <= 1e-8 -- the rule by which the benchmark counts eigenpairs."""
+    from qd3dsolver_b200 import kp_pryor as kpg, serving, workloads as wl
+    import bench
+    w = wl.fig4_from_fixture(os.path.join(GOLDEN, f'fig4_b{base}_fields.npz'))
+    with open(os.path.join(GOLDEN, f'fig4_b{base}.json')) as fh:
+        ref = json.load(fh)
+    f = w.fields
+    H = kpg.confined_hamiltonian(kpg.GridOperators(w.shape, w.h), f, 8,
+                                 strain={k: f[k] for k in wl.STRAIN_KEYS})
+    reqs = [serving.Request(H, k=8, sigma=w.sigma[b], tol=bench.TOL, maxiter=8000,
+                            precision='mixed', tag=b, mask=w.mask) for b in ('cb', 'vb')]
+    serving.solve_batch(reqs, max_slots=2)
+    for r in reqs:
+        n, dE, rel, split = bench.checked_pairs(r.result['E'], r.result['residuals'],
+                                                ref[r.tag], ref['H_norm2'])
+        assert n == 8, (base, r.tag, dE, rel, split)
+        assert r.result['kramers_split'] < 1e-7 and len(r.result['levels']) == 4
+    H.close()
