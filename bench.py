@@ -290,6 +290,124 @@ def fixed_iteration_legs(torch, device, wl1, wl2, iters):
 
 
 # ----------------------------------------------------------------------------------------------
+# Batched uneven dots and the antimonide serving stream
+# ----------------------------------------------------------------------------------------------
+
+def batched_dots_leg(torch, device, ndots, budget):
+    """64 seeded In(x)Ga(1-x)As/GaAs dots (x ~ U[0.6, 1], pyramid or spherical cap, base 6-20 nm,
+    h = 0.5 nm, grids 32^3 to 96x96x72, 2-8 Kramers pairs; seed 1), bands alternating cb / vb,
+    each solve given `budget` iterations. With the materials.py GaAs barrier at h = 0.5 nm none of
+    them converges (the spurious band of tests/test_spurious_band.py), so the leg reports
+    iteration throughput: the served engine (mixed precision, all dots admitted by free HBM
+    into one continuous batch whose ticks replay as CUDA graphs) against the plain complex128
+    drop-in solving them one by one, on the same requests and budget."""
+    from qd3dsolver_b200 import eigensolvers as eg, serving, workloads as wl
+    rng = np.random.default_rng(1)
+    t0 = time.perf_counter()
+    dots = [wl.random_dot(rng, device=True) for _ in range(ndots)]
+    t_prep = time.perf_counter() - t0
+    ops = [make_operator(w) for w in dots]
+    bands = [BANDS[i % 2] for i in range(ndots)]
+
+    def reqs():
+        return [serving.Request(H, k=w.k, sigma=w.sigma[b], tol=1e-8, maxiter=budget,
+                                precision='mixed', tag=i)
+                for i, (w, H, b) in enumerate(zip(dots, ops, bands))]
+    serving.solve_batch(reqs()[:2], max_slots=2)                 # warm: kernels, graph paths
+    torch.cuda.synchronize(device)
+    e0, e1 = _events(torch)
+    e0.record()
+    served = serving.solve_batch(reqs(), max_slots=ndots, ticks_per_poll=8)
+    e1.record()
+    torch.cuda.synchronize(device)
+    t_served = e0.elapsed_time(e1) * 1e-3
+    it_s = sum(r.result['iterations'] for r in served)
+    un_s = sum(r.result['iterations'] * r.H.shape[0] for r in served)
+    e0, e1 = _events(torch)
+    e0.record()
+    it_p = un_p = 0
+    for w, H, b in zip(dots, ops, bands):
+        X0 = eg.start_block(H.shape[0], min(w.k + max(2, w.k // 2), 24), 0)
+        _, _, hist, info = eg.lobpcg_device(H, X0, folded=True, sigma=w.sigma[b], tol=1e-8,
+                                            maxiter=budget)
+        it_p += info['iterations']
+        un_p += info['iterations'] * H.shape[0]
+    e1.record()
+    torch.cuda.synchronize(device)
+    t_plain = e0.elapsed_time(e1) * 1e-3
+    sizes = [w.n for w in dots]
+    out = {'dots': ndots, 'seed': 1, 'iterations_budget': budget,
+           'unknowns_min_max': [min(sizes), max(sizes)],
+           'k_min_max': [min(w.k for w in dots), max(w.k for w in dots)],
+           'host_preparation_s': t_prep,
+           'served_mixed': {'seconds': t_served, 'iterations': it_s,
+                            'iterations_per_s': it_s / t_served,
+                            'unknown_iterations_per_s': un_s / t_served,
+                            'statuses': sorted({r.result['status'] for r in served}),
+                            'converged': sum(bool(r.result['converged']) for r in served)},
+           'plain_c128': {'seconds': t_plain, 'iterations': it_p,
+                          'iterations_per_s': it_p / t_plain,
+                          'unknown_iterations_per_s': un_p / t_plain}}
+    out['served_vs_plain_unknown_iterations'] = (out['served_mixed']['unknown_iterations_per_s'] /
+                                                 out['plain_c128']['unknown_iterations_per_s'])
+    for H in ops:
+        H.close()
+    return out
+
+
+def antimonide_stream_leg(torch, device, nreq, budget):
+    """A prefix of the seeded (seed 2) antimonide request stream: InSb / In(x)Ga(1-x)Sb lens or
+    dash dots in InAs, radius 3-15 nm, h 0.4-0.6 nm, grids 32^3 to 128^3, 2-8 Kramers pairs, cb
+    or vb with sigma as heterostructure.eight_band_states sets it, each with an iteration
+    budget (broken-gap valence targets sit in the matrix conduction continuum and end at it).
+    The requests are first solved as one batch to measure the engine's capacity; then the same
+    requests arrive by a Poisson process at 80% of that capacity and are served with
+    continuous batching (admission by free HBM). An eigenpair counts when its request
+    converged, its relative residual ||Hv - Ev|| / ||H||_2 is <= 1e-8 (||H||_2 by power
+    iteration) and its Kramers partner is within 1e-7 eV."""
+    from qd3dsolver_b200 import serving, workloads as wl
+    rng = np.random.default_rng(2)
+    t0 = time.perf_counter()
+    items = [wl.antimonide_request(rng, device=True) for _ in range(nreq)]
+    t_prep = time.perf_counter() - t0
+    ops = [make_operator(w) for w, _ in items]
+    norms = [H.norm2_estimate() for H in ops]
+
+    def reqs():
+        return [serving.Request(H, k=w.k, sigma=w.sigma[b], tol=1e-8, maxiter=budget,
+                                precision='mixed', tag=(i, b), mask=w.mask)
+                for i, ((w, b), H) in enumerate(zip(items, ops))]
+    torch.cuda.synchronize(device)
+    t0 = time.perf_counter()
+    serving.solve_batch(reqs(), max_slots=nreq, ticks_per_poll=8)
+    t_batch = time.perf_counter() - t0
+    rate = 0.8 * nreq / t_batch
+    rr = reqs()
+    arrivals = np.cumsum(np.random.default_rng(3).exponential(1.0 / rate, size=nreq))
+    _, stats = serving.serve(rr, arrivals, max_slots=nreq, ticks_per_poll=8)
+    counted = 0
+    for r, hn in zip(rr, norms):
+        res = r.result
+        if res['status'] != 'converged':
+            continue
+        E = np.asarray(res['E'])
+        ok = (np.asarray(res['residuals']) / hn) <= REL_TOL
+        o = np.argsort(E)
+        split = np.full(len(E), np.inf)
+        for i in range(len(E) - len(E) % 2):
+            split[o[i]] = abs(E[o[i]] - E[o[i ^ 1]])
+        counted += int((ok & (split <= SPLIT_TOL)).sum())
+    st = [r.result['status'] for r in rr]
+    return {'requests': nreq, 'of_stream': 2000, 'seed': 2, 'iterations_budget': budget,
+            'host_preparation_s': t_prep, 'batch_seconds': t_batch, 'rate_per_s': rate,
+            'statuses': {k: st.count(k) for k in sorted(set(st))},
+            'bands': {b: sum(1 for _, bb in items if bb == b) for b in BANDS},
+            'unknowns_min_max': [min(w.n for w, _ in items), max(w.n for w, _ in items)],
+            'eigenpairs_checked': counted, 'eigenpairs_checked_per_s': counted / stats['wall'],
+            **stats}
+
+
+# ----------------------------------------------------------------------------------------------
 # CPU: the oracle (scipy LOBPCG on the oracle CSR), timed on the host cores
 # ----------------------------------------------------------------------------------------------
 
@@ -585,6 +703,10 @@ def run_ours(args):
         legs = None if args.no_fixed else fixed_iteration_legs(torch, device, w1, w2,
                                                                args.fixed_iterations)
         big = dict(hx2=hx2, legs=legs, w1=w1)
+    dots = (batched_dots_leg(torch, device, args.dots, args.dot_budget)
+            if (rank == 0 and not args.no_dots) else None)
+    stream5 = (antimonide_stream_leg(torch, device, args.stream5, args.stream5_budget)
+               if (rank == 0 and not args.no_stream5) else None)
     cpu = finish_cpu_children(children, refs) if children else None
     if cpu is not None and big is not None and big['legs'] is not None:
         c1 = cpu_config1(big['w1'])
@@ -653,6 +775,8 @@ def run_ours(args):
             'served_vs_plain': (value / plain['value']) if plain and plain['value'] else None,
             'serving_stream': stream,
             'baseline_configs': big['legs'] if big else None,
+            'batched_dots': dots,
+            'antimonide_stream': stream5,
             'hx_config2': hx2,
             'cpu_baseline': cpu,
             'e2e': e2e,
@@ -795,6 +919,12 @@ def main():
     ap.add_argument('--no-fixed', action='store_true',
                     help='skip the fixed-iteration legs on the pyramid operators')
     ap.add_argument('--fixed-iterations', type=int, default=20)
+    ap.add_argument('--no-dots', action='store_true', help='skip the 64-dot batched leg')
+    ap.add_argument('--dots', type=int, default=64)
+    ap.add_argument('--dot-budget', type=int, default=30)
+    ap.add_argument('--no-stream5', action='store_true', help='skip the antimonide stream leg')
+    ap.add_argument('--stream5', type=int, default=24, help='requests of the antimonide stream')
+    ap.add_argument('--stream5-budget', type=int, default=400)
     ap.add_argument('--form', choices=('served', 'plain'), default='served')
     ap.add_argument('--no-plain', action='store_true', help='skip the plain-form comparison')
     ap.add_argument('--no-e2e', action='store_true', help='skip the host-buffer end-to-end run')

@@ -261,6 +261,23 @@ class KPOperator(spla.LinearOperator):
             out.update(v1=v[0], v2=v[1], v3=v[2])
         return out
 
+    def norm2_estimate(self, iters=30, seed=0):
+        """||H||_2 from `iters` power iterations on a seeded complex vector (a lower bound that
+        converges from below; used to form relative residuals ||Hv - Ev|| / (||H||_2 ||v||))."""
+        torch = _torch()
+        g = torch.Generator(device=f'cuda:{self.device}').manual_seed(seed)
+        x = torch.randn((self.shape[0], 1), dtype=torch.complex128,
+                        device=f'cuda:{self.device}', generator=g)
+        x /= x.norm()
+        lam = 0.0
+        for _ in range(iters):
+            y = self.apply(x)
+            lam = float(y.norm())
+            if lam == 0.0:
+                break
+            x = y / lam
+        return lam
+
     def negated(self):
         """-H as a second device operator (same fields, sign flipped in the stencil)."""
         f = {k: (v.reshape(self.grid_shape) if v is not None else None)

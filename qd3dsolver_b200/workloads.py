@@ -266,18 +266,32 @@ class Workload:
 
 
 def build_environment(name, mask, h, dot, matrix, piezo=False, k=8, sigma_e_outside=False,
-                      meta=None):
-    st = solve_strain(mask, misfit(dot, matrix), matrix['C11'], matrix['C12'], matrix['C44'], h)
+                      meta=None, device=False):
+    """Strain, band edges, coefficient fields and both sigmas of one dot. device=True runs the
+    strain, the piezo potential and the valence-edge sigma on the GPU (qd3dsolver_b200.fields,
+    kp_pryor.hole_sigma); the same arithmetic, for batches whose host preparation would
+    otherwise take minutes."""
+    if device:
+        from . import fields as dfields, kp_pryor as kpd
+        sd = dfields.solve_strain(mask, misfit(dot, matrix), matrix['C11'], matrix['C12'],
+                                  matrix['C44'], h)
+        st = sd.as_dict()
+    else:
+        st = solve_strain(mask, misfit(dot, matrix), matrix['C11'], matrix['C12'], matrix['C44'], h)
     trace = st['exx'] + st['eyy'] + st['ezz']
     Ec, Ev = band_edge_fields(mask, trace, dot, matrix)
     if piezo:
         e14 = np.where(mask, dot['e14'], matrix['e14'])
-        phi = piezo_potential(st, e14, matrix['eps_R'], h)
+        phi = (dfields.potential(st, e14, matrix['eps_R'], h) if device
+               else piezo_potential(st, e14, matrix['eps_R'], h))
         Ec, Ev = Ec - phi, Ev - phi
     f = material_fields(mask, dot, matrix, Ev, Ec, 8)
     f.update(st)
     sig_e = float(Ec[~mask].min()) if sigma_e_outside else float(Ec[mask].min())
-    sig_h = hole_sigma(Ev, st, f['b'], f['d'], f['delta_so'], mask)
+    if device:
+        sig_h = kpd.hole_sigma(Ev, st, f['b'], f['d'], f['delta_so'], inside_mask=mask)
+    else:
+        sig_h = hole_sigma(Ev, st, f['b'], f['d'], f['delta_so'], mask)
     return Workload(name, mask.shape, h, f, mask, sig_e, sig_h, k, meta)
 
 
@@ -311,7 +325,7 @@ def config2():
                           name='pyramid128x128x96_h0.375')
 
 
-def random_dot(rng, h=0.5, n_min=32, n_max=96, pairs=(2, 8), family='InGaAs/GaAs'):
+def random_dot(rng, h=0.5, n_min=32, n_max=96, pairs=(2, 8), family='InGaAs/GaAs', device=False):
     """One seeded dot of the batched-dot family: In(x)Ga(1-x)As (x ~ U[0.6, 1]) pyramid or
     spherical cap in GaAs, base 6-20 nm, aspect 0.2-0.5, 2-8 Kramers pairs."""
     x = rng.uniform(0.6, 1.0)
@@ -334,7 +348,52 @@ def random_dot(rng, h=0.5, n_min=32, n_max=96, pairs=(2, 8), family='InGaAs/GaAs
     dot = alloy('InGaAs', x)
     return build_environment(f"{shape_kind}_x{x:.2f}_b{base:.1f}_{nxy}x{nxy}x{nz}", mask, h,
                              dot, material('GaAs'), k=2 * npairs,
-                             meta=dict(x=x, kind=shape_kind, base=base, height=height))
+                             meta=dict(x=x, kind=shape_kind, base=base, height=height),
+                             device=device)
+
+
+def antimonide_request(rng, n_min=32, n_max=128, pairs=(2, 8), device=False):
+    """One request of the antimonide serving stream: an InSb or In(x)Ga(1-x)Sb
+    (x ~ U[0.3, 1.0]) lens or dash in InAs, radius 3-15 nm, h ~ U[0.4, 0.6] nm, grid 32^3 to
+    128^3, 2-8 Kramers pairs, the conduction or the valence band with sigma as
+    heterostructure.eight_band_states sets it (heterostructure.py:978-985: the matrix minimum
+    of Ec for cb, the exact valence top inside the dot for vb), first-order piezo potential.
+
+    Choices the stream leaves open, fixed here: half the dots are InSb and half the alloy; a
+    lens has height / radius ~ U[0.3, 0.6]; a dash has length 2 r, width ~ U[0.5, 1] x length
+    and the height of a lens of the same radius, capped by its facets. Strain is the
+    homogeneous Fourier solution with the matrix's elastic constants (the reference's
+    heterostructure.build uses its FD elasticity solver, a host preprocessing step).
+    Returns (Workload, band)."""
+    insb = rng.random() < 0.5
+    x = 1.0 if insb else rng.uniform(0.3, 1.0)
+    kind = 'lens' if rng.random() < 0.5 else 'dash'
+    r = rng.uniform(3.0, 15.0)
+    h = rng.uniform(0.4, 0.6)
+    hgt = r * rng.uniform(0.3, 0.6)
+    npairs = int(rng.integers(pairs[0], pairs[1] + 1))
+    band = 'cb' if rng.random() < 0.5 else 'vb'
+    pad = max(3.0, 0.5 * r)
+    n_xy = int(np.clip(round((2 * r + 2 * pad) / h), n_min, n_max)) // 2 * 2
+    n_z = int(np.clip(round((hgt + 2 * pad) / h), n_min, n_max)) // 2 * 2
+    cx = centered_axis(n_xy, h)
+    kz0 = int(round(min(pad, n_z * h / 2 - hgt / 2) / h))
+    cz = (np.arange(n_z) - kz0 + 0.5) * h
+    X, Y, Z = np.meshgrid(cx, cx, cz, indexing='ij')
+    if kind == 'lens':
+        mask = lens_mask(X, Y, Z, r, hgt)
+    else:
+        length = 2 * r
+        width = length * rng.uniform(0.5, 1.0)
+        cap = (width / 2.0) * np.tan(np.deg2rad(54.7356))
+        mask = dash_mask(X, Y, Z, length, width, min(hgt, 0.95 * cap))
+    dot = alloy('InGaSb', x)
+    w = build_environment(f"{kind}_{'InSb' if insb else f'InGaSb{x:.2f}'}_r{r:.1f}_h{h:.2f}_"
+                          f"{n_xy}x{n_xy}x{n_z}", mask, h, dot, material('InAs'), piezo=True,
+                          k=2 * npairs, sigma_e_outside=True,
+                          meta=dict(x=x, kind=kind, radius=r, height=hgt, band=band),
+                          device=device)
+    return w, band
 
 
 # --------------------------------------------------------------------------------------------
