@@ -136,7 +136,10 @@ int qdkp_apply(const qdkp_operator* op, const void* X, int64_t ldx, void* Y, int
  *     message, and must use qdkp_apply with a workspace.
  *   - Every GPU that loads libqdkp.so keeps those 64 MiB until the process exits.
  *   - The first call on a device looks up the array's device address (cudaGetSymbolAddress,
- *     with that device current); make that first call before any stream capture.
+ *     with that device current); make that first call before any stream capture. The address
+ *     is kept for the life of the process: a device reset (cudaDeviceReset) invalidates it, so
+ *     do not use this entry point on a device after resetting it.
+ *   - The call makes the operator's device current and restores the caller's current device.
  *   - No cudaMalloc, cudaFree or other allocating routine is called.
  *   - All calls share the one array, which keeps the last call's contents; calls that overlap
  *     on the GPU (different streams or threads, without ordering between them) race on it.

@@ -65,16 +65,22 @@ int qdkp_apply_folded_noalloc(const qdkp_operator* op, const void* X, int64_t ld
               " bytes; use qdkp_apply with a caller workspace");
     return QDKP_ERR_WORKSPACE;
   }
-  QDKP_CUDA_TRY(cudaSetDevice(op->device));
+  // the operator's device is made current for the call and the caller's current device is
+  // restored on every return path
+  int prev = -1;
+  QDKP_CUDA_TRY(cudaGetDevice(&prev));
+  if (prev != op->device) QDKP_CUDA_TRY(cudaSetDevice(op->device));
   void* T = nullptr;
   int rc = scratch_address(op->device, &T);
-  if (rc != QDKP_OK) return rc;
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
-  // Every element of T that the second launch reads is written by the first one in this
-  // call, so nothing left over from an earlier call is ever read and nothing needs clearing.
-  rc = launch_apply(op, X, ldx, T, m, m, sigma, 1, precision, st);
-  if (rc != QDKP_OK) return rc;
-  return launch_apply(op, T, m, Y, ldy, m, sigma, 1, precision, st);
+  if (rc == QDKP_OK) {
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // Every element of T that the second launch reads is written by the first one in this
+    // call, so nothing left over from an earlier call is ever read and nothing needs clearing.
+    rc = launch_apply(op, X, ldx, T, m, m, sigma, 1, precision, st);
+    if (rc == QDKP_OK) rc = launch_apply(op, T, m, Y, ldy, m, sigma, 1, precision, st);
+  }
+  if (prev != op->device) cudaSetDevice(prev);
+  return rc;
 }
 
 }  // extern "C"

@@ -73,3 +73,34 @@ def test_noalloc_rejects_blocks_beyond_the_scratch():
     rc = _call_noalloc(L, H, X, Y, 0.5, _lib.C128, torch.cuda.current_stream().cuda_stream)
     assert rc == -4
     assert b'exceed the fixed scratch' in L.qdkp_last_error()
+
+
+def test_noalloc_folded_matches_the_oracle():
+    """The allocation-free folded apply against the oracle's own (H - sigma)^2 X (the restated
+    CSR pinned to the reference's H @ X), complex128 to 1e-13, complex64 to single precision."""
+    import torch
+    from qd3dsolver_b200 import _lib
+    from oracle import kp_operator as ko
+    L = _lib.lib()
+    H = _operator()
+    z = np.load(os.path.join(GOLDEN, 'solve_cases.npz'))
+    with open(os.path.join(GOLDEN, 'solve_cases.json')) as fh:
+        meta = json.load(fh)
+    f = {k[3:]: z[k] for k in z.files if k.startswith('f8_')}
+    Ho = ko.confined_hamiltonian(tuple(meta['shape']), float(z['h']), f, 8, strain=True)
+    n = H.shape[0]
+    rng = np.random.default_rng(12)
+    sigma = 0.8123
+    Xh = rng.standard_normal((n, 5)) + 1j * rng.standard_normal((n, 5))
+    S = Ho @ Xh - sigma * Xh
+    ref = Ho @ S - sigma * S
+    stream = torch.cuda.current_stream().cuda_stream
+    for dtype, prec, tol in ((torch.complex128, _lib.C128, 1e-13), (torch.complex64, _lib.C64, 4e-6)):
+        X = torch.from_numpy(Xh).to(dtype).cuda()
+        Y = torch.empty_like(X)
+        assert _call_noalloc(L, H, X, Y, sigma, prec, stream) == 0, L.qdkp_last_error()
+        torch.cuda.synchronize()
+        err = np.abs(Y.cpu().numpy() - ref).max() / np.abs(ref).max()
+        assert err < tol, (dtype, err)
+    H.close()
+
