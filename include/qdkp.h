@@ -155,14 +155,16 @@ int qdkp_apply_folded_noalloc(const qdkp_operator* op, const void* X, int64_t ld
  * Eight-band operators are applied by a staged kernel: a CTA owns a (y, z) tile of sites and a
  * few columns, walks along x and keeps a ring of x planes in shared memory. Tiles 0..3 fill the
  * ring with cp.async (both precisions); tiles 4..7 (complex64 only) fill it with bulk tensor
- * copies (TMA) and give every thread two columns of a site. A block the tensor maps cannot
+ * copies (TMA) and give every thread two columns of a site; tiles 8..12 (complex64 only) do the
+ * same with a producer warp and per-slot full/empty barriers, the record read from global
+ * memory by the threads of its site. A block the tensor maps cannot
  * describe (odd leading dimension, a base not 16-byte aligned, fewer columns than a tile or a
  * grid smaller than a tile) falls back to a cp.async tile. The tile is chosen by a heuristic
  * unless set here or by qdkp_operator_tune; QDKP_TILE_DIRECT selects the unstaged
  * one-thread-per-(site, column) kernel (always used for 6- and 4-band slices). The choice is per
  * operator and precision.
  */
-enum { QDKP_TILE_AUTO = -1, QDKP_TILE_DIRECT = -2, QDKP_TILE_COUNT = 8 };
+enum { QDKP_TILE_AUTO = -1, QDKP_TILE_DIRECT = -2, QDKP_TILE_COUNT = 13 };
 int qdkp_operator_set_tile(qdkp_operator* op, int precision, int tile);
 int qdkp_operator_get_tile(const qdkp_operator* op, int precision, int* tile);
 /* Autotuner: times every tile shape and the direct kernel on the caller's device blocks X, Y

@@ -1043,13 +1043,19 @@ int qdkp_engine_admit(qdkp_engine* e, const qdkp_operator* op, const qdkp_lobpcg
   ATRY(gram1(h, d.X, d.AX, m, d.gT, st));
   ATRY(launch_eigh(d.gT, nullptr, m, d.w, d.E, d.scr, (int*)d.G, st));
   ATRY(read_sync(&stat, d.G, sizeof(int), st));
-  if (stat) { set_error("initial Rayleigh-Ritz failed"); return QDKP_ERR_NUMERIC; }
-  ATRY(update1(h, d.X, m, d.E, m, d.X, st));
-  ATRY(update1(h, d.AX, m, d.E, m, d.AX, st));
-  std::vector<double> w(m);
-  ATRY(read_sync(w.data(), d.w, m * sizeof(double), st));
+  // the eigensolve fails only on non-finite input (a NaN or inf in the operator's fields or in
+  // X0): the slot is admitted already stopped with status nonfinite, and retires like any other
+  const bool nonfinite = stat != 0;
+  std::vector<double> w(m, std::numeric_limits<double>::quiet_NaN());
+  if (!nonfinite) {
+    ATRY(update1(h, d.X, m, d.E, m, d.X, st));
+    ATRY(update1(h, d.AX, m, d.E, m, d.AX, st));
+    ATRY(read_sync(w.data(), d.w, m * sizeof(double), st));
+  }
   EState s0{};
-  s0.running = 1; s0.status = QDKP_LOBPCG_MAXITER; s0.iter = -1; s0.idle = 1;
+  s0.running = nonfinite ? 0 : 1;
+  s0.status = nonfinite ? QDKP_LOBPCG_NONFINITE : QDKP_LOBPCG_MAXITER;
+  s0.iter = -1; s0.idle = 1;
   s0.ma = m; s0.mp = 0; s0.restart = 1; s0.forced = 0; s0.explicit_gram = 0;
   s0.best_iter = prm->maxiter; s0.skip_recompute = 1; s0.skip_p = 1; s0.skip_pnorm = 1;
   s0.smallest = std::numeric_limits<double>::max();

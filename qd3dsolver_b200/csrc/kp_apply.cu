@@ -1220,6 +1220,150 @@ kp_apply_tma_kernel(const __grid_constant__ CUtensorMap tmx, const __grid_consta
   }
 }
 
+// ---------------------------------------------------------------------------------------------
+// TMA kernel with a producer warp (eight bands, complex64). The ring of NSLOT planes is filled
+// by one producer warp; every ring slot has a "full" barrier (the copy landed) and an "empty"
+// barrier (every compute warp is done with the plane), so compute warps never meet at a CTA-wide
+// barrier: a warp moves on to plane x + 1 as soon as that plane has landed, and releases plane
+// x - 1 when it finishes x. Each site's record row is read by its own threads straight from
+// global memory (a record entry is used by the two threads of its site only), which leaves the
+// shared memory to the plane ring: larger tiles, or two CTAs per SM.
+// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" :: "r"(bar) : "memory");
+}
+
+template <int TY_, int TZ_, int G_, int NSLOT_, int MINB_>
+struct Tma2 {
+  static constexpr int TY = TY_, TZ = TZ_, G = G_, NSLOT = NSLOT_, MINB = MINB_;
+  static constexpr int CPT = 2;
+  static constexpr int MC = CPT * G;
+  static constexpr int PY = TY + 2, PZ = TZ + 2;
+  static constexpr int BAND = PY * PZ * MC;
+  static constexpr int PLANE_BYTES = 8 * BAND * 8;
+  static constexpr int CTHREADS = TY * TZ * G;            // compute threads
+  static constexpr int CWARPS = CTHREADS / 32;
+  static constexpr int THREADS = CTHREADS + 32;           // + the producer warp
+  static constexpr size_t SMEM = 1024 + (size_t)NSLOT * PLANE_BYTES + 16 * NSLOT;
+  static_assert(CTHREADS % 32 == 0, "compute threads fill whole warps");
+  static_assert(PLANE_BYTES % 128 == 0, "ring slots stay 128-byte aligned");
+  static_assert(NSLOT >= 4, "planes x-1, x, x+1 and at least one in flight");
+  static_assert(SMEM * MINB <= 232448, "over the shared memory of one SM");
+};
+
+struct RegRecord {                 // a site's record row in registers
+  float v[K_COUNT];
+  __device__ __forceinline__ float own(int k) const { return v[k]; }
+  __device__ __forceinline__ float face(int ax, int dir, int k) const {
+    return v[K_FACE + 5 * (2 * ax + dir) + k];
+  }
+};
+
+struct Tma2Args {
+  float2* __restrict__ Y;
+  const float* __restrict__ rec;
+  int N, nx, ny, nz, nzp, NP, ldy, m;
+  int tiles_z, chunks, xsplit, xlen;
+  int vec_store;
+  float shift, cb;
+};
+
+template <class G>
+__global__ void __launch_bounds__(G::THREADS, G::MINB)
+kp_apply_tma2_kernel(const __grid_constant__ CUtensorMap tmx, const Tma2Args a) {
+  extern __shared__ unsigned char smem_raw[];
+  const uint32_t raw = smem_u32(smem_raw);
+  const uint32_t pad = ((raw + 1023u) & ~1023u) - raw;
+  unsigned char* sb = smem_raw + pad;
+  const uint32_t ring = raw + pad;
+  const uint32_t full = ring + G::NSLOT * G::PLANE_BYTES;        // NSLOT barriers
+  const uint32_t empty = full + 8 * G::NSLOT;                     // NSLOT barriers
+  int bid = blockIdx.x;
+  const int xs = bid % a.xsplit; bid /= a.xsplit;
+  const int ch = bid % a.chunks; bid /= a.chunks;
+  const int tzi = bid % a.tiles_z;
+  const int tyi = bid / a.tiles_z;
+  const int c0 = ch * G::MC, y0 = tyi * G::TY, z0 = tzi * G::TZ;
+  const int xa = xs * a.xlen, xb = min(a.nx, xa + a.xlen);
+  if (c0 >= a.m || xa >= xb) return;          // uniform over the CTA
+  const int t = threadIdx.x;
+  if (t == 0) {
+    for (int i = 0; i < G::NSLOT; ++i) {
+      mbar_init(full + 8u * i, 1);
+      mbar_init(empty + 8u * i, G::CWARPS);
+    }
+    mbar_fence_init();
+  }
+  __syncthreads();
+  const int nplanes = xb - xa + 2;            // planes xa - 1 .. xb, sequence q = plane - xa + 1
+  // plane sequence q lives in slot q % NSLOT; its full barrier completes phase q / NSLOT, and
+  // the empty barrier of that slot completes phase q / NSLOT once every compute warp is done
+  if (t >= G::CTHREADS) {
+    // ---- producer warp -----------------------------------------------------------------
+    if (t == G::CTHREADS) {
+      bool ok = true;
+      int q = 0;
+      for (; q < nplanes && ok; ++q) {
+        const int s = q % G::NSLOT;
+        if (q >= G::NSLOT) ok = mbar_wait(empty + 8u * s, ((q / G::NSLOT) - 1) & 1);
+        if (!ok) break;
+        mbar_expect_tx(full + 8u * s, G::PLANE_BYTES);
+        tma_load_5d(ring + (uint32_t)s * G::PLANE_BYTES, &tmx, full + 8u * s, c0, z0 - 1, y0 - 1,
+                    xa - 1 + q, 0);
+      }
+      // keep the CTA resident until the last copies issued have landed (or given up)
+      for (int r = max(0, q - G::NSLOT); r < q; ++r)
+        ok = mbar_wait(full + 8u * (r % G::NSLOT), (r / G::NSLOT) & 1) && ok;
+      if (!ok) atomicExch(&g_apply_fault, 1);
+    }
+    return;
+  }
+  // ---- compute warps -----------------------------------------------------------------------
+  const int lane = t & 31;
+  const int g = t % G::G, tz = (t / G::G) % G::TZ, ty = t / (G::G * G::TZ);
+  const int iy = y0 + ty, iz = z0 + tz, col = c0 + g * G::CPT;
+  const bool active = iy < a.ny && iz < a.nz && col < a.m;
+  const int cell = ((ty + 1) * G::PZ + (tz + 1)) * G::MC + g * G::CPT;
+  const unsigned long long* pl = reinterpret_cast<const unsigned long long*>(sb);
+  bool ok = true;
+  for (int x = xa; x < xb; ++x) {
+    const int qx = x - xa + 1;
+    ok = ok && mbar_wait(full + 8u * ((qx - 1) % G::NSLOT), ((qx - 1) / G::NSLOT) & 1) &&
+         mbar_wait(full + 8u * (qx % G::NSLOT), (qx / G::NSLOT) & 1) &&
+         mbar_wait(full + 8u * ((qx + 1) % G::NSLOT), ((qx + 1) / G::NSLOT) & 1);
+    if (ok && active) {
+      RegRecord rc;
+      const float* rp = a.rec + ((long long)x * a.ny + iy) * a.nzp + iz;
+#pragma unroll
+      for (int k = 0; k < K_COUNT; ++k) rc.v[k] = __ldg(rp + (long long)k * a.NP);
+      TmaLoader<G> ld;
+      ld.p[0] = pl + (size_t)((qx - 1) % G::NSLOT) * (G::PLANE_BYTES / 8) + cell;
+      ld.p[1] = pl + (size_t)(qx % G::NSLOT) * (G::PLANE_BYTES / 8) + cell;
+      ld.p[2] = pl + (size_t)((qx + 1) % G::NSLOT) * (G::PLANE_BYTES / 8) + cell;
+      float2 yv[2][8];
+      hx_packed_cols<2>(ld, rc, a.shift, a.cb, yv);
+      const int s = (x * a.ny + iy) * a.nz + iz;
+      float2* __restrict__ ys = a.Y + ((long long)s * a.ldy + col);
+      const long long ybs = (long long)a.N * a.ldy;
+      if (a.vec_store && col + 1 < a.m) {
+#pragma unroll
+        for (int b = 0; b < 8; ++b)
+          *reinterpret_cast<float4*>(ys + b * ybs) = make_float4(yv[0][b].x, yv[0][b].y,
+                                                                 yv[1][b].x, yv[1][b].y);
+      } else {
+#pragma unroll
+        for (int b = 0; b < 8; ++b) {
+          ys[b * ybs] = yv[0][b];
+          if (col + 1 < a.m) ys[b * ybs + 1] = yv[1][b];
+        }
+      }
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(empty + 8u * ((qx - 1) % G::NSLOT));   // plane x - 1 is done
+  }
+  if (!ok && lane == 0) atomicExch(&g_apply_fault, 1);
+}
+
 // Tile shapes the staged kernel is built for: {precision, MC, TY, TZ}.
 template <typename T> struct StagedCfgs;
 template <> struct StagedCfgs<float> {
@@ -1421,6 +1565,88 @@ static int launch_tma(int i, const qdkp_operator* op, const void* X, int ldx, vo
   }
 }
 
+// Producer-warp TMA shapes {TY, TZ, column pairs per CTA, ring slots, CTAs per SM};
+// staged_cfg kTma2Base + i selects shape i (complex64 only).
+struct Tma2Cfgs {
+  using D0 = Tma2<6, 16, 2, 4, 1>;
+  using D1 = Tma2<8, 16, 2, 4, 1>;
+  using D2 = Tma2<8, 16, 1, 4, 2>;
+  using D3 = Tma2<6, 16, 2, 5, 1>;
+  using D4 = Tma2<4, 24, 2, 4, 1>;
+};
+constexpr int kTma2Base = kTmaBase + kTmaCfgs;
+constexpr int kTma2Cfgs = 5;
+
+template <class G>
+static bool tma2_fits(const qdkp_operator* op, const void* X, int64_t ldx, int m) {
+  return op->n_bands == 8 && ((uintptr_t)X & 15) == 0 && ldx % 2 == 0 && m >= G::MC &&
+         op->ny >= G::PY && op->nz >= G::PZ && tensor_map_encoder() != nullptr;
+}
+
+static bool tma2_fits_cfg(int i, const qdkp_operator* op, const void* X, int64_t ldx, int m) {
+  switch (i) {
+    case 0: return tma2_fits<Tma2Cfgs::D0>(op, X, ldx, m);
+    case 1: return tma2_fits<Tma2Cfgs::D1>(op, X, ldx, m);
+    case 2: return tma2_fits<Tma2Cfgs::D2>(op, X, ldx, m);
+    case 3: return tma2_fits<Tma2Cfgs::D3>(op, X, ldx, m);
+    default: return tma2_fits<Tma2Cfgs::D4>(op, X, ldx, m);
+  }
+}
+
+template <class G>
+static int launch_tma2_g(const qdkp_operator* op, const void* X, int ldx, void* Y, int ldy, int m,
+                         float shift, float cb, int sms, cudaStream_t st) {
+  const EncodeTiledFn enc = tensor_map_encoder();
+  static bool attr_done = false;
+  if (!attr_done) {
+    QDKP_CUDA_TRY(cudaFuncSetAttribute(kp_apply_tma2_kernel<G>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::SMEM));
+    attr_done = true;
+  }
+  const cuuint64_t N = (cuuint64_t)op->n_sites, ld = (cuuint64_t)ldx;
+  CUtensorMap tmx;
+  const cuuint64_t xdim[5] = {(cuuint64_t)m, (cuuint64_t)op->nz, (cuuint64_t)op->ny,
+                              (cuuint64_t)op->nx, 8};
+  const cuuint64_t xstr[4] = {ld * 8, (cuuint64_t)op->nz * ld * 8,
+                              (cuuint64_t)op->ny * op->nz * ld * 8, N * ld * 8};
+  const cuuint32_t xbox[5] = {(cuuint32_t)G::MC, (cuuint32_t)G::PZ, (cuuint32_t)G::PY, 1, 8};
+  const cuuint32_t ones[5] = {1, 1, 1, 1, 1};
+  CUresult r = enc(&tmx, CU_TENSOR_MAP_DATA_TYPE_INT64, 5, const_cast<void*>(X), xdim, xstr,
+                   xbox, ones, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_error("cuTensorMapEncodeTiled failed for the X block (code " + std::to_string((int)r) + ")");
+    return QDKP_ERR_CUDA;
+  }
+  // one wave holds MINB CTAs per SM
+  const StagedGeom g = staged_geom(op->nx, op->ny, op->nz, m, G::MC, G::TY, G::TZ,
+                                   sms * G::MINB);
+  Tma2Args a;
+  a.Y = static_cast<float2*>(Y);
+  a.rec = op->rec32;
+  a.N = (int)op->n_sites; a.nx = op->nx; a.ny = op->ny; a.nz = op->nz;
+  a.nzp = op->nzp; a.NP = op->nx * op->ny * op->nzp;
+  a.ldy = ldy; a.m = m;
+  a.tiles_z = g.tiles_z; a.chunks = g.chunks; a.xsplit = g.xsplit; a.xlen = g.xlen;
+  a.vec_store = ((uintptr_t)Y & 15) == 0 && ldy % 2 == 0;
+  a.shift = shift; a.cb = cb;
+  kp_apply_tma2_kernel<G><<<g.ctas, G::THREADS, G::SMEM, st>>>(tmx, a);
+  count_launch();
+  QDKP_CUDA_TRY(cudaGetLastError());
+  return QDKP_OK;
+}
+
+static int launch_tma2(int i, const qdkp_operator* op, const void* X, int ldx, void* Y, int ldy,
+                       int m, float shift, float cb, int sms, cudaStream_t st) {
+  switch (i) {
+    case 0: return launch_tma2_g<Tma2Cfgs::D0>(op, X, ldx, Y, ldy, m, shift, cb, sms, st);
+    case 1: return launch_tma2_g<Tma2Cfgs::D1>(op, X, ldx, Y, ldy, m, shift, cb, sms, st);
+    case 2: return launch_tma2_g<Tma2Cfgs::D2>(op, X, ldx, Y, ldy, m, shift, cb, sms, st);
+    case 3: return launch_tma2_g<Tma2Cfgs::D3>(op, X, ldx, Y, ldy, m, shift, cb, sms, st);
+    default: return launch_tma2_g<Tma2Cfgs::D4>(op, X, ldx, Y, ldy, m, shift, cb, sms, st);
+  }
+}
+
 int launch_apply_multi(const HXSlot* slots_dev, int nslots, int total_tiles, int precision,
                        cudaStream_t st) {
   if (total_tiles <= 0) return QDKP_OK;
@@ -1507,11 +1733,16 @@ static int launch_apply_t(const qdkp_operator* op, const T* rec, const void* X, 
   const T cb = (T)apply_cb_weight(op);
   const int forced = op->staged_cfg[precision == QDKP_C64];
   int cfg = forced == QDKP_TILE_AUTO ? pick_staged_cfg(op, precision, X, ldx, m) : forced;
-  if (cfg >= kTmaBase) {
+  if (cfg >= kTma2Base) {
+    if (std::is_same<T, float>::value && tma2_fits_cfg(cfg - kTma2Base, op, X, ldx, m))
+      return launch_tma2(cfg - kTma2Base, op, X, (int)ldx, Y, (int)ldy, m, (float)shift,
+                         (float)cb, num_sms(op->device), st);
+    cfg = 1;       // a block the tensor maps cannot describe: the cp.async staged kernel
+  } else if (cfg >= kTmaBase) {
     if (std::is_same<T, float>::value && tma_fits_cfg(cfg - kTmaBase, op, X, ldx, m))
       return launch_tma(cfg - kTmaBase, op, X, (int)ldx, Y, (int)ldy, m, (float)shift, (float)cb,
                         num_sms(op->device), st);
-    cfg = 1;       // a block the tensor maps cannot describe: the cp.async staged kernel
+    cfg = 1;
   }
   if (op->n_bands == 8 && cfg >= 0 && ((uintptr_t)X % sizeof(cplx<T>)) == 0)
     return launch_staged<T>(cfg, op, rec, X, (int)ldx, Y, (int)ldy, m, shift, cb,
@@ -1558,7 +1789,8 @@ extern "C" {
 int qdkp_operator_set_tile(qdkp_operator* op, int precision, int tile) {
   QDKP_CHECK_ARG(op != nullptr, "operator must not be NULL");
   QDKP_CHECK_ARG(precision == QDKP_C128 || precision == QDKP_C64, "bad precision");
-  QDKP_CHECK_ARG(tile >= QDKP_TILE_DIRECT && tile < kStagedCfgs + kTmaCfgs, "tile out of range");
+  QDKP_CHECK_ARG(tile >= QDKP_TILE_DIRECT && tile < kStagedCfgs + kTmaCfgs + kTma2Cfgs,
+                 "tile out of range");
   QDKP_CHECK_ARG(precision == QDKP_C64 || tile < kStagedCfgs,
                  "the TMA tile shapes are built for complex64 only");
   op->staged_cfg[precision == QDKP_C64] = tile;
@@ -1589,13 +1821,16 @@ int qdkp_operator_tune(qdkp_operator* op, const void* X, int64_t ldx, void* Y, i
   int rc = QDKP_OK;
   // candidates: the staged shapes, the TMA shapes (complex64), the direct kernel last; the
   // seconds array has one entry per candidate, -1 for one that does not apply
-  const int ncand = kStagedCfgs + kTmaCfgs + 1;
+  const int nbuilt = kStagedCfgs + kTmaCfgs + kTma2Cfgs;
+  const int ncand = nbuilt + 1;
   for (int c = 0; c < ncand && rc == QDKP_OK; ++c) {
-    const int tile = c < kStagedCfgs + kTmaCfgs ? c : kDirect;
+    const int tile = c < nbuilt ? c : kDirect;
     if (seconds) seconds[c] = -1.0;
     if (op->n_bands != 8 && tile != kDirect) continue;                // 6/4-band: direct only
-    if (tile >= kTmaBase && (precision != QDKP_C64 ||
-                             !tma_fits_cfg(tile - kTmaBase, op, X, ldx, m))) continue;
+    if (tile >= kTmaBase && precision != QDKP_C64) continue;
+    if (tile >= kTma2Base && !tma2_fits_cfg(tile - kTma2Base, op, X, ldx, m)) continue;
+    if (tile >= kTmaBase && tile < kTma2Base && !tma_fits_cfg(tile - kTmaBase, op, X, ldx, m))
+      continue;
     op->staged_cfg[pi] = tile;
     rc = launch_apply(op, X, ldx, Y, ldy, m, 0.0, 0, precision, st);      // warm-up
     if (rc != QDKP_OK) break;
