@@ -921,10 +921,10 @@ def main():
     ap.add_argument('--fixed-iterations', type=int, default=20)
     ap.add_argument('--no-dots', action='store_true', help='skip the 64-dot batched leg')
     ap.add_argument('--dots', type=int, default=64)
-    ap.add_argument('--dot-budget', type=int, default=30)
+    ap.add_argument('--dot-budget', type=int, default=20)
     ap.add_argument('--no-stream5', action='store_true', help='skip the antimonide stream leg')
-    ap.add_argument('--stream5', type=int, default=24, help='requests of the antimonide stream')
-    ap.add_argument('--stream5-budget', type=int, default=400)
+    ap.add_argument('--stream5', type=int, default=12, help='requests of the antimonide stream')
+    ap.add_argument('--stream5-budget', type=int, default=150)
     ap.add_argument('--form', choices=('served', 'plain'), default='served')
     ap.add_argument('--no-plain', action='store_true', help='skip the plain-form comparison')
     ap.add_argument('--no-e2e', action='store_true', help='skip the host-buffer end-to-end run')

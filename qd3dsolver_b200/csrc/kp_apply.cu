@@ -1380,7 +1380,7 @@ template <> struct StagedCfgs<double> {
 };
 constexpr int kStagedCfgs = 4;
 constexpr int kDirect = -2;      // staged_cfg value selecting the direct kernel
-constexpr int kDefaultTma = 1;   // TMA shape taken when no tile was tuned or set
+constexpr int kDefaultTma = 3;   // TMA shape taken when no tile was tuned or set
 
 struct StagedGeom { int tiles_y, tiles_z, chunks, xsplit, xlen, ctas; };
 

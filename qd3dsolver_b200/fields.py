@@ -69,7 +69,8 @@ def potential(strain, e14, eps_r, h, sign=+1.0, device=False):
     shape = tuple(S.shape[1:])
     if len(shape) != 3:
         raise ValueError("strain components must be 3-D grids")
-    e = np.broadcast_to(np.asarray(e14, dtype=float), shape) if not hasattr(e14, 'data_ptr') else e14
+    e = (np.array(np.broadcast_to(np.asarray(e14, dtype=float), shape))
+         if not hasattr(e14, 'data_ptr') else e14)
     E = (e14 if hasattr(e14, 'data_ptr') else torch.from_numpy(np.ascontiguousarray(e))).to(
         dev, torch.float64).contiguous()
     phi = torch.empty(shape, dtype=torch.float64, device=dev)
