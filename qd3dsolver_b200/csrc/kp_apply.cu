@@ -1063,9 +1063,9 @@ __device__ __forceinline__ void tma_load_4d(uint32_t dst, const CUtensorMap* map
 // Set by a TMA kernel whose wait on a copy gave up (qdkp_device_fault reads and clears it).
 __device__ int g_apply_fault;
 
-template <int TY_, int TZ_, int G_, int NSLOT_>
+template <int TY_, int TZ_, int G_, int NSLOT_, int MINB_ = 1>
 struct Tma {
-  static constexpr int TY = TY_, TZ = TZ_, G = G_, NSLOT = NSLOT_;
+  static constexpr int TY = TY_, TZ = TZ_, G = G_, NSLOT = NSLOT_, MINB = MINB_;
   static constexpr int CPT = 2;                          // columns per thread
   static constexpr int MC = CPT * G;                     // columns per CTA
   static constexpr int PY = TY + 2, PZ = TZ + 2;
@@ -1079,7 +1079,7 @@ struct Tma {
   static_assert(TZ % 4 == 0, "record rows are copied in 16-byte z runs");
   static_assert(PLANE_BYTES % 128 == 0, "ring slots stay 128-byte aligned");
   static_assert(NSLOT >= 4, "planes x-1, x, x+1 and at least one in flight");
-  static_assert(SMEM <= 232448, "over the opt-in shared memory of one CTA");
+  static_assert(SMEM * MINB <= 232448, "over the shared memory of one SM");
 };
 
 struct TmaArgs {
@@ -1118,7 +1118,7 @@ struct TmaLoader {
 };
 
 template <class G>
-__global__ void __launch_bounds__(G::THREADS, 1)
+__global__ void __launch_bounds__(G::THREADS, G::MINB)
 kp_apply_tma_kernel(const __grid_constant__ CUtensorMap tmx, const __grid_constant__ CUtensorMap tmr,
                     const TmaArgs a) {
   extern __shared__ unsigned char smem_raw[];
@@ -1482,9 +1482,11 @@ struct TmaCfgs {
   using C1 = Tma<6, 16, 2, 5>;
   using C2 = Tma<8, 12, 2, 5>;
   using C3 = Tma<4, 24, 2, 4>;
+  using C4 = Tma<4, 12, 2, 4, 2>;      // two CTAs per SM: one CTA's plane barrier overlaps
+  using C5 = Tma<6, 8, 2, 4, 2>;       // the other's compute
 };
 constexpr int kTmaBase = 4;
-constexpr int kTmaCfgs = 4;
+constexpr int kTmaCfgs = 6;
 
 template <class G>
 static bool tma_fits(const qdkp_operator* op, const void* X, int64_t ldx, int m) {
@@ -1498,7 +1500,9 @@ static bool tma_fits_cfg(int i, const qdkp_operator* op, const void* X, int64_t 
     case 0: return tma_fits<TmaCfgs::C0>(op, X, ldx, m);
     case 1: return tma_fits<TmaCfgs::C1>(op, X, ldx, m);
     case 2: return tma_fits<TmaCfgs::C2>(op, X, ldx, m);
-    default: return tma_fits<TmaCfgs::C3>(op, X, ldx, m);
+    case 3: return tma_fits<TmaCfgs::C3>(op, X, ldx, m);
+    case 4: return tma_fits<TmaCfgs::C4>(op, X, ldx, m);
+    default: return tma_fits<TmaCfgs::C5>(op, X, ldx, m);
   }
 }
 
@@ -1541,7 +1545,8 @@ static int launch_tma_g(const qdkp_operator* op, const void* X, int ldx, void* Y
     set_error("cuTensorMapEncodeTiled failed for the record (code " + std::to_string((int)r) + ")");
     return QDKP_ERR_CUDA;
   }
-  const StagedGeom g = staged_geom(op->nx, op->ny, op->nz, m, G::MC, G::TY, G::TZ, sms);
+  const StagedGeom g = staged_geom(op->nx, op->ny, op->nz, m, G::MC, G::TY, G::TZ,
+                                   sms * G::MINB);
   TmaArgs a;
   a.Y = static_cast<float2*>(Y);
   a.N = (int)op->n_sites; a.nx = op->nx; a.ny = op->ny; a.nz = op->nz;
@@ -1561,7 +1566,9 @@ static int launch_tma(int i, const qdkp_operator* op, const void* X, int ldx, vo
     case 0: return launch_tma_g<TmaCfgs::C0>(op, X, ldx, Y, ldy, m, shift, cb, sms, st);
     case 1: return launch_tma_g<TmaCfgs::C1>(op, X, ldx, Y, ldy, m, shift, cb, sms, st);
     case 2: return launch_tma_g<TmaCfgs::C2>(op, X, ldx, Y, ldy, m, shift, cb, sms, st);
-    default: return launch_tma_g<TmaCfgs::C3>(op, X, ldx, Y, ldy, m, shift, cb, sms, st);
+    case 3: return launch_tma_g<TmaCfgs::C3>(op, X, ldx, Y, ldy, m, shift, cb, sms, st);
+    case 4: return launch_tma_g<TmaCfgs::C4>(op, X, ldx, Y, ldy, m, shift, cb, sms, st);
+    default: return launch_tma_g<TmaCfgs::C5>(op, X, ldx, Y, ldy, m, shift, cb, sms, st);
   }
 }
 
