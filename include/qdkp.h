@@ -154,8 +154,8 @@ int qdkp_apply_folded_noalloc(const qdkp_operator* op, const void* X, int64_t ld
  * H.X kernel selection (no counterpart in the reference, which multiplies an assembled CSR).
  * Eight-band operators are applied by a staged kernel: a CTA owns a (y, z) tile of sites and a
  * few columns, walks along x and keeps a ring of x planes in shared memory. Tiles 0..3 fill the
- * ring with cp.async (both precisions); tiles 4..9 (complex64 only) fill it with bulk tensor
- * copies (TMA) and give every thread two columns of a site; tiles 10..14 (complex64 only) do the
+ * ring with cp.async (both precisions); tiles 4..11 (complex64 only) fill it with bulk tensor
+ * copies (TMA) and give every thread two columns of a site; tiles 12..16 (complex64 only) do the
  * same with a producer warp and per-slot full/empty barriers, the record read from global
  * memory by the threads of its site. A block the tensor maps cannot
  * describe (odd leading dimension, a base not 16-byte aligned, fewer columns than a tile or a
@@ -164,7 +164,7 @@ int qdkp_apply_folded_noalloc(const qdkp_operator* op, const void* X, int64_t ld
  * one-thread-per-(site, column) kernel (always used for 6- and 4-band slices). The choice is per
  * operator and precision.
  */
-enum { QDKP_TILE_AUTO = -1, QDKP_TILE_DIRECT = -2, QDKP_TILE_COUNT = 15 };
+enum { QDKP_TILE_AUTO = -1, QDKP_TILE_DIRECT = -2, QDKP_TILE_COUNT = 17 };
 int qdkp_operator_set_tile(qdkp_operator* op, int precision, int tile);
 int qdkp_operator_get_tile(const qdkp_operator* op, int precision, int* tile);
 /* Autotuner: times every tile shape and the direct kernel on the caller's device blocks X, Y

@@ -13,9 +13,9 @@ QDKP_OK = 0
 HOLE_CONVENTION, STRAIN, INTERBAND_STRAIN, NEGATE = 1, 2, 4, 8
 C128, C64 = 0, 1
 APPLY_PLAIN, APPLY_SHIFTED, APPLY_FOLDED = 0, 1, 2
-TILE_AUTO, TILE_DIRECT, TILE_COUNT = -1, -2, 15
+TILE_AUTO, TILE_DIRECT, TILE_COUNT = -1, -2, 17
 TILE_TMA0 = 4                     # first TMA tile shape (complex64)
-TILE_TMA2 = 10                    # first producer-warp TMA tile shape (complex64)
+TILE_TMA2 = 12                    # first producer-warp TMA tile shape (complex64)
 LOBPCG_STATUS = {0: 'converged', 1: 'maxiter', 2: 'cholesky_breakdown',
                  3: 'eigh_breakdown', 4: 'nonfinite'}
 

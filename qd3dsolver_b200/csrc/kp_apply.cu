@@ -1060,12 +1060,23 @@ __device__ __forceinline__ void tma_load_4d(uint32_t dst, const CUtensorMap* map
          "r"(c3) : "memory");
 }
 
+struct RegRecord {                 // a site's record row in registers
+  float v[K_COUNT];
+  __device__ __forceinline__ float own(int k) const { return v[k]; }
+  __device__ __forceinline__ float face(int ax, int dir, int k) const {
+    return v[K_FACE + 5 * (2 * ax + dir) + k];
+  }
+};
+
 // Set by a TMA kernel whose wait on a copy gave up (qdkp_device_fault reads and clears it).
 __device__ int g_apply_fault;
 
-template <int TY_, int TZ_, int G_, int NSLOT_, int MINB_ = 1>
+// RREG: the record row of each site is prefetched by its threads into registers one plane ahead
+// (no record slots in shared memory, which leaves room for larger tiles)
+template <int TY_, int TZ_, int G_, int NSLOT_, int MINB_ = 1, bool RREG_ = false>
 struct Tma {
   static constexpr int TY = TY_, TZ = TZ_, G = G_, NSLOT = NSLOT_, MINB = MINB_;
+  static constexpr bool RREG = RREG_;
   static constexpr int CPT = 2;                          // columns per thread
   static constexpr int MC = CPT * G;                     // columns per CTA
   static constexpr int PY = TY + 2, PZ = TZ + 2;
@@ -1074,8 +1085,9 @@ struct Tma {
   static constexpr int RPLANE_BYTES = K_COUNT * TY * TZ * 4;
   static constexpr int RSTRIDE = (RPLANE_BYTES + 127) / 128 * 128;
   static constexpr int THREADS = TY * TZ * G;
-  static constexpr int BARS = NSLOT + 2;
-  static constexpr size_t SMEM = 1024 + (size_t)NSLOT * PLANE_BYTES + 2 * RSTRIDE + 8 * BARS;
+  static constexpr int BARS = NSLOT + (RREG ? 0 : 2);
+  static constexpr size_t SMEM = 1024 + (size_t)NSLOT * PLANE_BYTES + (RREG ? 0 : 2 * RSTRIDE) +
+                                 8 * BARS;
   static_assert(TZ % 4 == 0, "record rows are copied in 16-byte z runs");
   static_assert(PLANE_BYTES % 128 == 0, "ring slots stay 128-byte aligned");
   static_assert(NSLOT >= 4, "planes x-1, x, x+1 and at least one in flight");
@@ -1084,6 +1096,8 @@ struct Tma {
 
 struct TmaArgs {
   float2* __restrict__ Y;
+  const float* __restrict__ rec;   // the FP32 record (read directly by RREG shapes)
+  int nzp, NP;
   int N, nx, ny, nz, ldy, m;
   int tiles_z, chunks, xsplit, xlen;
   int vec_store;          // Y is 16-byte aligned with an even leading dimension
@@ -1127,7 +1141,8 @@ kp_apply_tma_kernel(const __grid_constant__ CUtensorMap tmx, const __grid_consta
   unsigned char* sb = smem_raw + pad;
   const uint32_t ring = raw + pad;
   const uint32_t rring = ring + G::NSLOT * G::PLANE_BYTES;
-  const uint32_t bars = rring + 2 * G::RSTRIDE;          // NSLOT plane barriers, 2 record ones
+  // NSLOT plane barriers, then 2 record ones (staged records only)
+  const uint32_t bars = rring + (G::RREG ? 0 : 2 * G::RSTRIDE);
   int bid = blockIdx.x;
   const int xs = bid % a.xsplit; bid /= a.xsplit;
   const int ch = bid % a.chunks; bid /= a.chunks;
@@ -1167,7 +1182,15 @@ kp_apply_tma_kernel(const __grid_constant__ CUtensorMap tmx, const __grid_consta
   int q_issued = 0, r_issued = 0;
   if (t == 0) {
     for (; q_issued < G::NSLOT - 1 && q_issued < nplanes; ++q_issued) issue_plane(q_issued);
-    issue_record(r_issued++);
+    if (!G::RREG) issue_record(r_issued++);
+  }
+  // RREG: this thread's record row of plane x, and the one of plane x + 1 in flight
+  RegRecord rcur, rnxt;
+  const long long rsite = (long long)iy * a.nzp + iz;
+  if (G::RREG && active) {
+    const float* rp = a.rec + (long long)xa * a.ny * a.nzp + rsite;
+#pragma unroll
+    for (int k = 0; k < K_COUNT; ++k) rcur.v[k] = __ldg(rp + (long long)k * a.NP);
   }
   bool ok = true;
   for (int x = xa; x < xb; ++x) {
@@ -1179,21 +1202,33 @@ kp_apply_tma_kernel(const __grid_constant__ CUtensorMap tmx, const __grid_consta
     const bool all_ok = __syncthreads_and(ok) != 0;
     if (t == 0 && all_ok) {
       if (q_issued < nplanes) issue_plane(q_issued++);
-      if (x + 1 < xb) issue_record(r_issued++);
+      if (!G::RREG && x + 1 < xb) issue_record(r_issued++);
     }
     const int r = x - xa;
-    ok = all_ok && mbar_wait(rec_bar(r), (r >> 1) & 1);
+    if (G::RREG) ok = all_ok;
+    else ok = all_ok && mbar_wait(rec_bar(r), (r >> 1) & 1);
     if (!ok || !active) continue;
+    if (G::RREG && x + 1 < xb) {                // prefetch plane x + 1's record row
+      const float* rp = a.rec + (long long)(x + 1) * a.ny * a.nzp + rsite;
+#pragma unroll
+      for (int k = 0; k < K_COUNT; ++k) rnxt.v[k] = __ldg(rp + (long long)k * a.NP);
+    }
     TmaLoader<G> ld;
     const unsigned long long* pl = reinterpret_cast<const unsigned long long*>(sb);
     ld.p[0] = pl + (size_t)((qx - 1) % G::NSLOT) * (G::PLANE_BYTES / 8) + cell;
     ld.p[1] = pl + (size_t)(qx % G::NSLOT) * (G::PLANE_BYTES / 8) + cell;
     ld.p[2] = pl + (size_t)((qx + 1) % G::NSLOT) * (G::PLANE_BYTES / 8) + cell;
-    SmemRecord<float, G> rc;                    // record slot layout [k][ty][tz]
-    rc.r = reinterpret_cast<const float*>(sb + G::NSLOT * G::PLANE_BYTES + (r & 1) * G::RSTRIDE) +
-           ty * G::TZ + tz;
     float2 yv[2][8];
-    hx_packed_cols<2>(ld, rc, a.shift, a.cb, yv);
+    if constexpr (G::RREG) {
+      hx_packed_cols<2>(ld, rcur, a.shift, a.cb, yv);
+#pragma unroll
+      for (int k = 0; k < K_COUNT; ++k) rcur.v[k] = rnxt.v[k];
+    } else {
+      SmemRecord<float, G> rc;                  // record slot layout [k][ty][tz]
+      rc.r = reinterpret_cast<const float*>(sb + G::NSLOT * G::PLANE_BYTES + (r & 1) * G::RSTRIDE) +
+             ty * G::TZ + tz;
+      hx_packed_cols<2>(ld, rc, a.shift, a.cb, yv);
+    }
     const int s = (x * a.ny + iy) * a.nz + iz;
     float2* __restrict__ ys = a.Y + ((long long)s * a.ldy + col);
     const long long ybs = (long long)a.N * a.ldy;
@@ -1251,13 +1286,6 @@ struct Tma2 {
   static_assert(SMEM * MINB <= 232448, "over the shared memory of one SM");
 };
 
-struct RegRecord {                 // a site's record row in registers
-  float v[K_COUNT];
-  __device__ __forceinline__ float own(int k) const { return v[k]; }
-  __device__ __forceinline__ float face(int ax, int dir, int k) const {
-    return v[K_FACE + 5 * (2 * ax + dir) + k];
-  }
-};
 
 struct Tma2Args {
   float2* __restrict__ Y;
@@ -1484,9 +1512,11 @@ struct TmaCfgs {
   using C3 = Tma<4, 24, 2, 4>;
   using C4 = Tma<4, 12, 2, 4, 2>;      // two CTAs per SM: one CTA's plane barrier overlaps
   using C5 = Tma<6, 8, 2, 4, 2>;       // the other's compute
+  using C6 = Tma<8, 16, 2, 4, 1, true>;   // records in registers: 256 and 288 threads
+  using C7 = Tma<6, 24, 2, 4, 1, true>;
 };
 constexpr int kTmaBase = 4;
-constexpr int kTmaCfgs = 6;
+constexpr int kTmaCfgs = 8;
 
 template <class G>
 static bool tma_fits(const qdkp_operator* op, const void* X, int64_t ldx, int m) {
@@ -1502,7 +1532,9 @@ static bool tma_fits_cfg(int i, const qdkp_operator* op, const void* X, int64_t 
     case 2: return tma_fits<TmaCfgs::C2>(op, X, ldx, m);
     case 3: return tma_fits<TmaCfgs::C3>(op, X, ldx, m);
     case 4: return tma_fits<TmaCfgs::C4>(op, X, ldx, m);
-    default: return tma_fits<TmaCfgs::C5>(op, X, ldx, m);
+    case 5: return tma_fits<TmaCfgs::C5>(op, X, ldx, m);
+    case 6: return tma_fits<TmaCfgs::C6>(op, X, ldx, m);
+    default: return tma_fits<TmaCfgs::C7>(op, X, ldx, m);
   }
 }
 
@@ -1549,6 +1581,8 @@ static int launch_tma_g(const qdkp_operator* op, const void* X, int ldx, void* Y
                                    sms * G::MINB);
   TmaArgs a;
   a.Y = static_cast<float2*>(Y);
+  a.rec = op->rec32;
+  a.nzp = op->nzp; a.NP = op->nx * op->ny * op->nzp;
   a.N = (int)op->n_sites; a.nx = op->nx; a.ny = op->ny; a.nz = op->nz;
   a.ldy = ldy; a.m = m;
   a.tiles_z = g.tiles_z; a.chunks = g.chunks; a.xsplit = g.xsplit; a.xlen = g.xlen;
@@ -1568,7 +1602,9 @@ static int launch_tma(int i, const qdkp_operator* op, const void* X, int ldx, vo
     case 2: return launch_tma_g<TmaCfgs::C2>(op, X, ldx, Y, ldy, m, shift, cb, sms, st);
     case 3: return launch_tma_g<TmaCfgs::C3>(op, X, ldx, Y, ldy, m, shift, cb, sms, st);
     case 4: return launch_tma_g<TmaCfgs::C4>(op, X, ldx, Y, ldy, m, shift, cb, sms, st);
-    default: return launch_tma_g<TmaCfgs::C5>(op, X, ldx, Y, ldy, m, shift, cb, sms, st);
+    case 5: return launch_tma_g<TmaCfgs::C5>(op, X, ldx, Y, ldy, m, shift, cb, sms, st);
+    case 6: return launch_tma_g<TmaCfgs::C6>(op, X, ldx, Y, ldy, m, shift, cb, sms, st);
+    default: return launch_tma_g<TmaCfgs::C7>(op, X, ldx, Y, ldy, m, shift, cb, sms, st);
   }
 }
 
