@@ -154,18 +154,18 @@ constexpr int kGramParts = 296;
 template <int MR, int MC, typename T>
 __global__ void __launch_bounds__(512)
 gram_partial_kernel(const BlockList<T> A, const BlockList<T> B, long long n,
-                    long long rows_per_part, double* __restrict__ partial) {
+                    long long rows_per_part, double* __restrict__ partial, int ptc) {
   extern __shared__ __align__(16) unsigned char gsm_d[];
   const int RP = (2 * A.total() + 7) / 8 * 8, RQ = (2 * B.total() + 7) / 8 * 8;
   const long long r0 = blockIdx.x * rows_per_part;
   double* out = partial + (long long)blockIdx.x * RP * RQ;
   if constexpr (std::is_same<T, float>::value) {
-    if (gram_tf32_rects(A.total(), B.total()) <= (int)(blockDim.x >> 5)) {
+    if (gridDim.y == 1 && gram_tf32_rects(A.total(), B.total()) <= (int)(blockDim.x >> 5)) {
       gram_core_tf32(A, B, r0, min(n, r0 + rows_per_part), out, gsm_d);
       return;
     }
   }
-  gram_core<MR, MC>(A, B, r0, min(n, r0 + rows_per_part), out, gsm_d);
+  gram_core<MR, MC>(A, B, r0, min(n, r0 + rows_per_part), out, gsm_d, blockIdx.y * ptc, ptc);
 }
 
 // Stage 1: column-block sums of the partial C' slices (coalesced over the RP x RQ elements);
@@ -228,21 +228,17 @@ int launch_gram(const BlockList<T>& A, const BlockList<T>& B, long long n,
   if (!attr) {
     const int big = 200 * 1024;
     cudaFuncSetAttribute(gram_partial_kernel<3, 3, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-    cudaFuncSetAttribute(gram_partial_kernel<3, 6, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-    cudaFuncSetAttribute(gram_partial_kernel<6, 6, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
     attr = true;
   }
-  int MR, MC, threads;
-  gram_shape(P, Q, MR, MC, threads);
-  if (std::is_same<T, float>::value) {   // the TF32 core wants one warp per tile rectangle
+  const GramPlan gp = gram_plan(P, Q);
+  int threads = gp.threads;
+  if (std::is_same<T, float>::value && gp.panels == 1) {   // the TF32 core: a warp per rectangle
     const int G = gram_tf32_rects(P, Q);
     if (G > threads / 32 && G <= 16) threads = 512;
   }
   double* pd = reinterpret_cast<double*>(partial);
-  const unsigned grid = (unsigned)parts;
-  if (MR == 3 && MC == 3) gram_partial_kernel<3, 3, T><<<grid, threads, smem, st>>>(A, B, n, rpp, pd);
-  else if (MR == 3) gram_partial_kernel<3, 6, T><<<grid, threads, smem, st>>>(A, B, n, rpp, pd);
-  else gram_partial_kernel<6, 6, T><<<grid, threads, smem, st>>>(A, B, n, rpp, pd);
+  gram_partial_kernel<3, 3, T><<<dim3((unsigned)parts, gp.panels), threads, smem, st>>>(
+      A, B, n, rpp, pd, gp.ptc);
   count_launch();
   const int elems = RP * RQ;
   double* part2 = pd + (size_t)parts * elems;

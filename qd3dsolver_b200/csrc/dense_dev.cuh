@@ -643,23 +643,29 @@ __device__ __forceinline__ void gram_copy_rows(const BlockList<T>& L, long long 
   }
 }
 
-// tile rectangles: tile rows split in groups of MR, tile columns in groups of MC
+// tile rectangles: tile rows split in groups of MR, tile columns in groups of MC. A CTA covers
+// the tile columns [tc_lo, tc_lo + tc_cnt) of C' (a column panel; a wide product is split into
+// panels over blockIdx.y so that every rectangle fits one warp's registers) and writes only
+// those columns of its partial.
 template <int MR, int MC, typename T>
 static __device__ void gram_core(const BlockList<T>& A, const BlockList<T>& B,
                                  long long r0, long long r1, double* __restrict__ out,
-                                 unsigned char* smem) {
+                                 unsigned char* smem, int tc_lo = 0, int tc_cnt = 1 << 30) {
   const int P = A.total(), Q = B.total();
   const int RP = (2 * P + 7) / 8 * 8, RQ = (2 * Q + 7) / 8 * 8;
-  const int TR = RP / 8, TC = RQ / 8;
+  const int TR = RP / 8;
+  const int tc_hi = min(RQ / 8, tc_lo + tc_cnt);
+  const int TC = tc_hi - tc_lo;                   // this panel's tile columns
+  if (TC <= 0) return;                            // an empty panel (uniform over the CTA)
   const int GR = (TR + MR - 1) / MR, GC = (TC + MC - 1) / MC;
-  const int G = GR * GC;                          // tile rectangles (<= 8 by construction)
+  const int G = GR * GC;                          // tile rectangles (<= warps by construction)
   const int nwarps = blockDim.x >> 5;
   const int slices = nwarps / G;                  // warps per rectangle
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int g = lane >> 2, t4 = lane & 3;
   const int rect = warp % G, slice = warp / G;
   const bool active_warp = slice < slices;
-  const int tr0 = (rect / GC) * MR, tc0 = (rect % GC) * MC;
+  const int tr0 = (rect / GC) * MR, tc0 = tc_lo + (rect % GC) * MC;
   // stage layout: per list, per block, crow x cols complex values; A's blocks first
   const unsigned avail = dyn_smem_bytes();
   int crow = gram_chunk_rows(P, Q, (int)sizeof(cplx<T>));
@@ -688,7 +694,7 @@ static __device__ void gram_core(const BlockList<T>& A, const BlockList<T>& B,
     const int col = (tc0 + j) * 8 + g;
     int c = col >> 1, blk = 0, start = 0;
     while (blk < B.nblk - 1 && c >= B.cols[blk]) { c -= B.cols[blk]; start += B.cols[blk]; ++blk; }
-    const bool ok = active_warp && tc0 + j < TC && col < 2 * Q;
+    const bool ok = active_warp && tc0 + j < tc_hi && col < 2 * Q;
     sb_off[j] = ok ? (P + start) * crow : -1;
     sb_w[j] = B.cols[blk];
     sb_c[j] = 2 * c + (col & 1);
@@ -755,7 +761,7 @@ static __device__ void gram_core(const BlockList<T>& A, const BlockList<T>& B,
 #pragma unroll
         for (int j = 0; j < MC; ++j) {
           const int ti = tr0 + i, tj = tc0 + j;
-          if (ti < TR && tj < TC) {
+          if (ti < TR && tj < tc_hi) {
             const int rr = ti * 8 + g, cc = tj * 8 + 2 * t4;
             gsm[rr * RQ + cc] += acc[i][j][0];
             gsm[rr * RQ + cc + 1] += acc[i][j][1];
@@ -764,7 +770,10 @@ static __device__ void gram_core(const BlockList<T>& A, const BlockList<T>& B,
     }
     __syncthreads();
   }
-  for (int e = threadIdx.x; e < RP * RQ; e += blockDim.x) out[e] = gsm[e];
+  for (int e = threadIdx.x; e < RP * RQ; e += blockDim.x) {
+    const int cc = e % RQ;
+    if (cc >= 8 * tc_lo && cc < 8 * tc_hi) out[e] = gsm[e];
+  }
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -1142,16 +1151,21 @@ static __device__ void update_rows_tf32(const BlockList<float>& A, const double2
 #undef QDKP_TF_CASE
 }
 
-// (MR, MC, threads) for a product: the smallest tile rectangles that fit 8 warps, else 16.
-static inline void gram_shape(int P, int Q, int& MR, int& MC, int& threads) {
+// Launch plan of an FP64 Gram product of P x Q complex columns: 3 x 3-tile rectangles (the
+// register-resident size), 8 or 16 warps, and, for a product wider than 16 rectangles, column
+// panels of `ptc` tile columns on blockIdx.y. Depends only on P and Q.
+struct GramPlan { int threads, ptc, panels; };
+static inline GramPlan gram_plan(int P, int Q) {
   const int TR = ((2 * P + 7) / 8 * 8) / 8, TC = ((2 * Q + 7) / 8 * 8) / 8;
-  const int cand[3][2] = {{3, 3}, {3, 6}, {6, 6}};
-  for (int lim : {8, 16})
-    for (auto& c : cand) {
-      const int G = ((TR + c[0] - 1) / c[0]) * ((TC + c[1] - 1) / c[1]);
-      if (G <= lim) { MR = c[0]; MC = c[1]; threads = 32 * lim; return; }
-    }
-  MR = MC = 6; threads = 512;
+  const int GR = (TR + 2) / 3, GC = (TC + 2) / 3;
+  GramPlan g;
+  if (GR * GC <= 8) { g.threads = 256; g.ptc = TC; g.panels = 1; return g; }
+  if (GR * GC <= 16) { g.threads = 512; g.ptc = TC; g.panels = 1; return g; }
+  const int gcp = GR >= 16 ? 1 : 16 / GR;        // rectangle columns per panel
+  g.threads = 512;
+  g.ptc = 3 * gcp;
+  g.panels = (TC + g.ptc - 1) / g.ptc;
+  return g;
 }
 
 }  // namespace qdkp

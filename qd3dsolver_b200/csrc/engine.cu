@@ -253,7 +253,7 @@ __device__ bool gram_lists(const ESlot& d, int which, BlockList<T>& A, BlockList
 // sum) then depends only on the slot's own sizes, never on which other solves share the batch.
 template <int MR, int MC>
 __global__ void __launch_bounds__(512)
-e_gram_kernel(const ESlot* __restrict__ S, int ns, int which, int m_only) {
+e_gram_kernel(const ESlot* __restrict__ S, int ns, int which, int m_only, int ptc) {
   extern __shared__ __align__(16) unsigned char gsm_e[];
   const int k = slot_of(S, ns, blockIdx.x, &ESlot::gram0);
   const ESlot& d = S[k];
@@ -268,13 +268,14 @@ e_gram_kernel(const ESlot* __restrict__ S, int ns, int which, int m_only) {
     // complex64 blocks, FP64 products: the Gram matrices of the search stay exact to FP64
     // (the split TF32 form loses convergence in the explicit-Gram regime of scipy's method)
     double* po = d.gpart + (long long)part * RP * RQ;
-    gram_core<MR, MC>(A, B, r0, min(d.n, r0 + d.rows_per_gpart), po, gsm_e);
+    gram_core<MR, MC>(A, B, r0, min(d.n, r0 + d.rows_per_gpart), po, gsm_e, blockIdx.y * ptc,
+                      ptc);
   } else {
     BlockList<double> A, B;
     if (!gram_lists<double>(d, which, A, B, out)) return;
     const int RP = (2 * A.total() + 7) / 8 * 8, RQ = (2 * B.total() + 7) / 8 * 8;
     gram_core<MR, MC>(A, B, r0, min(d.n, r0 + d.rows_per_gpart),
-                      d.gpart + (long long)part * RP * RQ, gsm_e);
+                      d.gpart + (long long)part * RP * RQ, gsm_e, blockIdx.y * ptc, ptc);
   }
 }
 
@@ -751,11 +752,11 @@ int launch_gram_multi(const EGroup& G, int which, cudaStream_t st) {
     else if (which == GR_WW || which == GR_WAW) { P = 3 * m; Q = 3 * m; }
     const size_t smem = std::max(gram_smem_bytes(P, Q, (int)sizeof(double2)),
                                  gram_smem_bytes(P, Q, (int)sizeof(float2)));
-    int MR, MC, threads;
-    gram_shape(P, Q, MR, MC, threads);
-    if (MR == 3 && MC == 3) e_gram_kernel<3, 3><<<G.gram_ctas, threads, smem, st>>>(G.d_slots, G.ns, which, m);
-    else if (MR == 3) e_gram_kernel<3, 6><<<G.gram_ctas, threads, smem, st>>>(G.d_slots, G.ns, which, m);
-    else e_gram_kernel<6, 6><<<G.gram_ctas, threads, smem, st>>>(G.d_slots, G.ns, which, m);
+    // the plan for the widest product this width can form; a narrower one on the device leaves
+    // its last panels empty
+    const GramPlan gp = gram_plan(P, Q);
+    e_gram_kernel<3, 3><<<dim3(G.gram_ctas, gp.panels), gp.threads, smem, st>>>(
+        G.d_slots, G.ns, which, m, gp.ptc);
     count_launch();
   }
   const int RP = (6 * G.m_max + 7) / 8 * 8;
@@ -940,8 +941,6 @@ int qdkp_engine_create(int max_slots, int device, qdkp_engine** out) {
   // dynamic shared memory limits of the engine kernels
   const int big = 200 * 1024;
   cudaFuncSetAttribute(e_gram_kernel<3, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-  cudaFuncSetAttribute(e_gram_kernel<3, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-  cudaFuncSetAttribute(e_gram_kernel<6, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
   cudaFuncSetAttribute(e_update_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
   cudaFuncSetAttribute(e_update_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
   cudaFuncSetAttribute(e_rr_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
