@@ -832,19 +832,30 @@ def engine_probe(args):
     import torch
     from qd3dsolver_b200 import serving
     wls, _ = load_sweep()
-    ops = [make_operator(w) for w in wls]
-    eng = serving.Engine(len(wls) * len(BANDS), graphs=False)
-    reqs = [serving.Request(H, k=K, sigma=w.sigma[band], tol=TOL, maxiter=MAXITER,
-                            precision=args.precision)
-            for w, H in zip(wls, ops) for band in BANDS]
-    for r in reqs:
-        eng.admit(r)
-    eng.step(args.probe_ticks)
-    torch.cuda.synchronize()
-    print(json.dumps({'engine_probe': len(reqs), 'ticks': args.probe_ticks,
-                      'precision': args.precision}))
-    eng.close()
-    for H in ops:
+    keep = set(args.probe_solves.split(',')) if args.probe_solves else None
+    pairs = [(w, band) for w in wls for band in BANDS
+             if keep is None or f"b{int(w.meta['base'])}_{band}" in keep]
+    ops = {w.name: make_operator(w) for w, _ in pairs}
+    if args.probe_plain:
+        # the plain drop-in, one solve after the other, each for --probe-ticks iterations
+        from qd3dsolver_b200 import eigensolvers as eg
+        for w, band in pairs:
+            H = ops[w.name]
+            X0 = torch.from_numpy(eg.start_block(H.shape[0], BLOCK, 0)).cuda()
+            eg.lobpcg_device(H, X0, folded=True, sigma=w.sigma[band], tol=1e-30,
+                             maxiter=args.probe_ticks)
+        torch.cuda.synchronize()
+    else:
+        eng = serving.Engine(len(pairs), graphs=False)
+        for w, band in pairs:
+            eng.admit(serving.Request(ops[w.name], k=K, sigma=w.sigma[band], tol=TOL,
+                                      maxiter=MAXITER, precision=args.precision))
+        eng.step(args.probe_ticks)
+        torch.cuda.synchronize()
+        eng.close()
+    print(json.dumps({'engine_probe': len(pairs), 'ticks': args.probe_ticks,
+                      'precision': args.precision, 'plain': bool(args.probe_plain)}))
+    for H in ops.values():
         H.close()
 
 
@@ -939,6 +950,10 @@ def main():
     ap.add_argument('--engine-probe', action='store_true',
                     help='only run the served engine for --probe-ticks ticks (profiling)')
     ap.add_argument('--probe-ticks', type=int, default=20)
+    ap.add_argument('--probe-solves', default=None,
+                    help='comma-separated solves of the probe (e.g. b10_vb); default all 14')
+    ap.add_argument('--probe-plain', action='store_true',
+                    help='probe the plain drop-in (one solve after the other) instead')
     ap.add_argument('--ticks-per-poll', type=int, default=16)
     ap.add_argument('--mixed-tol', type=float, default=1e-4,
                     help='residual at which a mixed-precision solve leaves complex64')
