@@ -293,6 +293,20 @@ int qdkp_block_update(const void* A, int64_t lda, int P, const double* C, int q,
                       void* stream);
 
 /*
+ * The Rayleigh-Ritz eigensolve of a LOBPCG iteration, eigh(gramA, gramB) (scipy lobpcg.py:891-909):
+ * A, B host n x n complex128 Hermitian (row-major; B NULL for
+ * the identity), n <= 72. All n eigenpairs (nwant = n) by Householder + QL, or only the nwant
+ * smallest (1 <= nwant < n) by multisection and inverse iteration, the form the LOBPCG iterations
+ * use (they keep the block-size smallest). w (host, n doubles) ascending in its first nwant
+ * entries; V (host, n x n complex128, row-major) eigenvectors in its first nwant columns,
+ * B-orthonormal. Returns QDKP_OK, or QDKP_ERR_NUMERIC when B is not positive definite or the
+ * spectrum is not finite. Synchronous on `stream`; workspace qdkp_block_eigh_workspace_size(n).
+ */
+size_t qdkp_block_eigh_workspace_size(int n);
+int qdkp_block_eigh(const double* A, const double* B, int n, int nwant, double* w, double* V,
+                    void* ws, size_t ws_bytes, void* stream);
+
+/*
  * Rayleigh quotients and residual norms of H for the columns of V (device, n x k complex128,
  * leading dimension ldv): rq[j] = v^H H v / v^H v and res[j] = ||H v_j - E_j v_j|| on the
  * normalised v_j, with E = E_in if non-NULL else rq (eigensolvers.residual_norms /

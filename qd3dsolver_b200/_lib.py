@@ -105,6 +105,10 @@ _SIGNATURES = {
                                        ctypes.c_void_p, ctypes.c_int64, ctypes.c_int,
                                        ctypes.c_int64, ctypes.c_int, ctypes.c_void_p,
                                        ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]),
+    'qdkp_block_eigh_workspace_size': (ctypes.c_size_t, [ctypes.c_int]),
+    'qdkp_block_eigh': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                       ctypes.c_size_t, ctypes.c_void_p]),
     'qdkp_block_update_workspace_size': (ctypes.c_size_t, [ctypes.c_int, ctypes.c_int]),
     'qdkp_block_update': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int,
                                          ctypes.c_void_p, ctypes.c_int, ctypes.c_int64,

@@ -325,23 +325,24 @@ int launch_chol_inv(const double2* G, int n, double2* Uinv, int* status, cudaStr
   return QDKP_OK;
 }
 
-// w ascending, V columns permuted accordingly; generalized problem through B = U^H U.
+// w ascending, V columns permuted accordingly; generalized problem through B = U^H U (with
+// 0 < nwant < n only the first nwant pairs are computed).
 __global__ void __launch_bounds__(kSmallThreads)
 eigh_kernel(const double2* __restrict__ A, const double2* __restrict__ B, int n,
             double* __restrict__ w, double2* __restrict__ Vout, double2* __restrict__ scratch,
-            int* __restrict__ status) {
+            int* __restrict__ status, int nwant) {
   extern __shared__ double2 esm[];
-  const int st = block_eigh(A, B, n, w, Vout, scratch, esm, esm + n * n);
+  const int st = block_eigh(A, B, n, w, Vout, scratch, esm, esm + n * n, nwant);
   if (threadIdx.x == 0) *status = st;
 }
 
 int launch_eigh(const double2* A, const double2* B, int n, double* w, double2* V,
-                double2* scratch, int* status, cudaStream_t st) {
+                double2* scratch, int* status, cudaStream_t st, int nwant) {
   if (n < 1 || n > kMaxSmall) { set_error("eigh dimension out of range"); return QDKP_ERR_ARG; }
   const size_t smem = 2 * (size_t)n * n * sizeof(double2);
   QDKP_CUDA_TRY(cudaFuncSetAttribute(eigh_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)smem));
-  eigh_kernel<<<1, kSmallThreads, smem, st>>>(A, B, n, w, V, scratch, status);
+  eigh_kernel<<<1, kSmallThreads, smem, st>>>(A, B, n, w, V, scratch, status, nwant);
   count_launch();
   QDKP_CUDA_TRY(cudaGetLastError());
   return QDKP_OK;
@@ -413,6 +414,48 @@ int qdkp_block_gram(const void* A, int64_t lda, int P, const void* B, int64_t ld
   if (rc != QDKP_OK) return rc;
   QDKP_CUDA_TRY(cudaMemcpyAsync(out, dout, (size_t)P * Q * sizeof(double2), cudaMemcpyDeviceToHost, st));
   QDKP_CUDA_TRY(cudaStreamSynchronize(st));
+  return QDKP_OK;
+}
+
+size_t qdkp_block_eigh_workspace_size(int n) {
+  if (n < 1 || n > kMaxSmall) return 0;
+  const size_t mat = ((size_t)n * n * sizeof(double2) + 255) / 256 * 256;
+  return 5 * mat + ((size_t)n * sizeof(double) + 255) / 256 * 256 + 256;
+}
+
+int qdkp_block_eigh(const double* A, const double* B, int n, int nwant, double* w, double* V,
+                    void* ws, size_t ws_bytes, void* stream) {
+  QDKP_CHECK_ARG(A && w && V && ws, "NULL argument");
+  QDKP_CHECK_ARG(n >= 1 && n <= kMaxSmall, "n must be in [1, 72]");
+  QDKP_CHECK_ARG(nwant >= 1 && nwant <= n, "nwant must be in [1, n]");
+  if (ws_bytes < qdkp_block_eigh_workspace_size(n)) {
+    set_error("qdkp_block_eigh: workspace too small");
+    return QDKP_ERR_WORKSPACE;
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const size_t mb = (size_t)n * n * sizeof(double2);
+  const size_t mat = (mb + 255) / 256 * 256;
+  char* p = static_cast<char*>(ws);
+  double2* dA = reinterpret_cast<double2*>(p);
+  double2* dB = reinterpret_cast<double2*>(p + mat);
+  double2* dV = reinterpret_cast<double2*>(p + 2 * mat);
+  double2* scr = reinterpret_cast<double2*>(p + 3 * mat);     // 2 n^2
+  double* dw = reinterpret_cast<double*>(p + 5 * mat);
+  int* dstat = reinterpret_cast<int*>(p + 5 * mat + ((size_t)n * sizeof(double) + 255) / 256 * 256);
+  QDKP_CUDA_TRY(cudaMemcpyAsync(dA, A, mb, cudaMemcpyHostToDevice, st));
+  if (B) QDKP_CUDA_TRY(cudaMemcpyAsync(dB, B, mb, cudaMemcpyHostToDevice, st));
+  const int rc = launch_eigh(dA, B ? dB : nullptr, n, dw, dV, scr, dstat, st, nwant < n ? nwant : 0);
+  if (rc != QDKP_OK) return rc;
+  int hstat = 0;
+  QDKP_CUDA_TRY(cudaMemcpyAsync(w, dw, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, st));
+  QDKP_CUDA_TRY(cudaMemcpyAsync(V, dV, mb, cudaMemcpyDeviceToHost, st));
+  QDKP_CUDA_TRY(cudaMemcpyAsync(&hstat, dstat, sizeof(int), cudaMemcpyDeviceToHost, st));
+  QDKP_CUDA_TRY(cudaStreamSynchronize(st));
+  if (hstat != 0) {
+    set_error(hstat == 1 ? "qdkp_block_eigh: B is not positive definite"
+                         : "qdkp_block_eigh: non-finite spectrum");
+    return QDKP_ERR_NUMERIC;
+  }
   return QDKP_OK;
 }
 

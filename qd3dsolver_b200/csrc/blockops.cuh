@@ -79,7 +79,8 @@ int launch_update(const BlockList<T>& A, const double2* const* C, int q, long lo
 
 // Small dense (one CTA). Matrices row-major with ld = n. status: 0 ok, 1 failure.
 int launch_chol_inv(const double2* G, int n, double2* Uinv, int* status, cudaStream_t st);
+// nwant > 0: only the nwant smallest eigenpairs are needed (w[0..nwant), V's first columns)
 int launch_eigh(const double2* A, const double2* B, int n, double* w, double2* V,
-                double2* scratch, int* status, cudaStream_t st);
+                double2* scratch, int* status, cudaStream_t st, int nwant = 0);
 
 }  // namespace qdkp

@@ -288,12 +288,594 @@ static __device__ int block_tql(double2* S0, double2* S1, int n, double2* gtmp) 
 }
 
 
+// =============================================================================================
+// Rayleigh-Ritz eigensolve for the wanted eigenpairs only: LOBPCG keeps the m smallest of the
+// 3m Ritz pairs, so the tridiagonal problem is solved for those alone, by multisection with
+// Sturm counts and inverse iteration, which run in parallel where the QL recurrence is serial.
+// Every routine is CTA-wide for 512 threads (16 warps); block-uniform return codes.
+// =============================================================================================
+constexpr int kRrWarps = 16;
+
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ double warp_min(double v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+// integer mixing (xorshift-multiply) for deterministic pseudo-random start vectors
+__device__ __forceinline__ unsigned mix32(unsigned x) {
+  x ^= x >> 16; x *= 0x7feb352du; x ^= x >> 15; x *= 0x846ca68bu; x ^= x >> 16;
+  return x;
+}
+__device__ __forceinline__ double start_value(int i, int j) {
+  return (double)(mix32((unsigned)(i * 131 + j * 7919 + 17)) >> 8) * (1.0 / 8388608.0) - 1.0;
+}
+
+struct RrShared {
+  double td[kMaxSmall], tb[kMaxSmall], e2[kMaxSmall], tau[kMaxSmall], rinv[kMaxSmall];
+  double lam[kMaxSmall];
+  double2 esub[kMaxSmall], ph[kMaxSmall], xcol[kMaxSmall], psm[kMaxSmall];
+  double G[kMaxBlock * kMaxBlock];
+  double lo, hi;
+  int bad;
+};
+
+// Upper Cholesky B = U^H U in place (S, ld n), one barrier per column: step k subtracts
+// conj(S_ki) S_kj / S_kk from S_ij (k < i <= j) with the unscaled pivot row; the rows are scaled
+// by 1 / sqrt(S_kk) at the end. rinv = 1 / U_kk. Returns nonzero on a bad pivot.
+static __device__ int rr_cholesky(double2* __restrict__ S, int n, double* __restrict__ rinv) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwp = blockDim.x >> 5;
+  for (int k = 0; k < n; ++k) {
+    const double d = S[k * n + k].x;
+    if (!(d > 0.0) || !isfinite(d)) { __syncthreads(); return 1; }
+    const double inv = 1.0 / d;
+    for (int i = k + 1 + warp; i < n; i += nwp) {
+      const double2 a = S[k * n + i];
+      for (int j = i + lane; j < n; j += 32) {
+        const double2 b = S[k * n + j];
+        double2 t = S[i * n + j];
+        t.x -= (a.x * b.x + a.y * b.y) * inv;
+        t.y -= (a.x * b.y - a.y * b.x) * inv;
+        S[i * n + j] = t;
+      }
+    }
+    __syncthreads();
+  }
+  for (int k = threadIdx.x; k < n; k += blockDim.x) rinv[k] = 1.0 / sqrt(S[k * n + k].x);
+  __syncthreads();
+  for (int i = warp; i < n; i += nwp)
+    for (int j = i + lane; j < n; j += 32) {
+      const double r = rinv[i];
+      if (j == i) S[i * n + j] = make_double2(1.0 / r, 0.0);
+      else { S[i * n + j].x *= r; S[i * n + j].y *= r; }
+    }
+  __syncthreads();
+  return 0;
+}
+
+// Rows of A (ld n) times U^-1 (U upper, pivots as reciprocals rinv): a warp per row (rows
+// warp + 16 r), the row in registers (lane l holds columns l + 32 q), w_k = a_k / U_kk broadcast
+// by a shuffle, then a_j -= w_k U_kj. Written conjugate-transposed (row i into column i) when
+// `trans`, in place otherwise; every row is read before any is written.
+template <int R, int CC>
+static __device__ void rr_rows_solve(double2* __restrict__ A, const double2* __restrict__ U,
+                                     int n, const double* __restrict__ rinv, bool trans) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double2 a[R][CC];
+#pragma unroll
+  for (int r = 0; r < R; ++r)
+#pragma unroll
+    for (int q = 0; q < CC; ++q) {
+      const int i = warp + kRrWarps * r, j = lane + 32 * q;
+      a[r][q] = (i < n && j < n) ? A[i * n + j] : make_double2(0.0, 0.0);
+    }
+  __syncthreads();
+  for (int k = 0; k < n; ++k) {
+    const int kl = k & 31, kq = k >> 5;
+    const double rk = rinv[k];
+    double2 u[CC];
+#pragma unroll
+    for (int q = 0; q < CC; ++q) {
+      const int j = lane + 32 * q;
+      u[q] = (j > k && j < n) ? U[k * n + j] : make_double2(0.0, 0.0);
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      double2 ak = a[r][0];
+#pragma unroll
+      for (int q = 1; q < CC; ++q) if (kq == q) ak = a[r][q];
+      ak.x = __shfl_sync(0xffffffffu, ak.x, kl) * rk;
+      ak.y = __shfl_sync(0xffffffffu, ak.y, kl) * rk;
+#pragma unroll
+      for (int q = 0; q < CC; ++q) {
+        if (lane + 32 * q == k) a[r][q] = ak;
+        a[r][q].x -= ak.x * u[q].x - ak.y * u[q].y;
+        a[r][q].y -= ak.x * u[q].y + ak.y * u[q].x;
+      }
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < R; ++r)
+#pragma unroll
+    for (int q = 0; q < CC; ++q) {
+      const int i = warp + kRrWarps * r, j = lane + 32 * q;
+      if (i < n && j < n) {
+        if (trans) A[j * n + i] = make_double2(a[r][q].x, -a[r][q].y);
+        else A[i * n + j] = a[r][q];
+      }
+    }
+  __syncthreads();
+}
+
+// Householder tridiagonalisation of the Hermitian part of Csm (read once), held in registers:
+// warp w owns rows w + 16 r, lane l columns l + 32 q. Step k forms the reflector
+// H = I - tau v v^H (v^H v = 2 / tau) from column k in every warp (identical butterfly sums),
+// p = tau C v row-wise, K = tau / 2 v^H p, w = p - K v and C <- C - v w^H - w v^H; two barriers
+// per column. Reflector k (v_j, j > k) is stored in row n - 1 - k of Rf's strict lower triangle
+// (v_j at column j - k - 1), tau_k in sh.tau. On return sh.td / sh.tb / sh.e2 hold the real
+// tridiagonal T = D^H (Q^H C Q) D, sh.ph the phases D (the off-diagonal made real and >= 0).
+template <int R, int CC>
+static __device__ void rr_tridiag(const double2* __restrict__ Csm, int n,
+                                  double2* __restrict__ Rf, RrShared& sh) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double2 c[R][CC];
+#pragma unroll
+  for (int r = 0; r < R; ++r)
+#pragma unroll
+    for (int q = 0; q < CC; ++q) {
+      const int i = warp + kRrWarps * r, j = lane + 32 * q;
+      if (i < n && j < n) {
+        const double2 a = Csm[i * n + j], b = Csm[j * n + i];
+        c[r][q] = make_double2(0.5 * (a.x + b.x), 0.5 * (a.y - b.y));
+      } else {
+        c[r][q] = make_double2(0.0, 0.0);
+      }
+    }
+  if (warp == 0)                                   // column 0 is row 0 conjugated
+#pragma unroll
+    for (int q = 0; q < CC; ++q) {
+      const int j = lane + 32 * q;
+      if (j < n) sh.xcol[j] = j > 0 ? make_double2(c[0][q].x, -c[0][q].y) : make_double2(0.0, 0.0);
+    }
+  __syncthreads();
+  for (int k = 0; k + 2 < n; ++k) {
+    const int j0 = k + 1;
+    double2 vs[CC];
+    double nx2 = 0.0;
+#pragma unroll
+    for (int q = 0; q < CC; ++q) {
+      const int j = lane + 32 * q;
+      vs[q] = (j > k && j < n) ? sh.xcol[j] : make_double2(0.0, 0.0);
+      nx2 += vs[q].x * vs[q].x + vs[q].y * vs[q].y;
+    }
+    nx2 = warp_sum(nx2);
+    const double2 x0 = sh.xcol[j0];
+    const double ax0 = sqrt(x0.x * x0.x + x0.y * x0.y);
+    const double nx = sqrt(nx2);
+    // alpha = -phase(x0) |x|, v = x - alpha e_1
+    const double2 phs = ax0 > 0.0 ? make_double2(x0.x / ax0, x0.y / ax0) : make_double2(1.0, 0.0);
+    const double tau = nx2 > 0.0 ? 1.0 / (nx * (nx + ax0)) : 0.0;
+    const double2 v0 = make_double2(x0.x + phs.x * nx, x0.y + phs.y * nx);
+#pragma unroll
+    for (int q = 0; q < CC; ++q)
+      if (lane + 32 * q == j0) vs[q] = v0;
+    double2 vr[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int i = warp + kRrWarps * r;
+      vr[r] = (i > j0 && i < n) ? sh.xcol[i] : (i == j0 ? v0 : make_double2(0.0, 0.0));
+    }
+    if (warp == 0) {
+#pragma unroll
+      for (int q = 0; q < CC; ++q) {
+        const int j = lane + 32 * q;
+        if (j > k && j < n) Rf[(n - 1 - k) * n + (j - k - 1)] = vs[q];
+      }
+      if (lane == 0) sh.tau[k] = tau;
+    }
+    double2 pr[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      double sx = 0.0, sy = 0.0;
+      if (warp + kRrWarps * r >= k)                // rows above k are reduced already
+#pragma unroll
+        for (int q = 0; q < CC; ++q) {
+          sx += c[r][q].x * vs[q].x - c[r][q].y * vs[q].y;
+          sy += c[r][q].x * vs[q].y + c[r][q].y * vs[q].x;
+        }
+      pr[r] = make_double2(sx, sy);
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      pr[r].x = tau * warp_sum(pr[r].x);
+      pr[r].y = tau * warp_sum(pr[r].y);
+    }
+    if (lane == 0)
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const int i = warp + kRrWarps * r;
+        if (i < n) sh.psm[i] = pr[r];
+      }
+    __syncthreads();
+    double2 pc[CC];
+    double s = 0.0;                                // Re v^H p (v^H C v is real)
+#pragma unroll
+    for (int q = 0; q < CC; ++q) {
+      const int j = lane + 32 * q;
+      pc[q] = j < n ? sh.psm[j] : make_double2(0.0, 0.0);
+      s += vs[q].x * pc[q].x + vs[q].y * pc[q].y;
+    }
+    const double K = 0.5 * tau * warp_sum(s);
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      if (warp + kRrWarps * r < k) continue;
+      const double2 wi = make_double2(pr[r].x - K * vr[r].x, pr[r].y - K * vr[r].y);
+      const double2 vi = vr[r];
+#pragma unroll
+      for (int q = 0; q < CC; ++q) {
+        const double2 vj = vs[q];
+        const double2 wj = make_double2(pc[q].x - K * vj.x, pc[q].y - K * vj.y);
+        c[r][q].x -= vi.x * wj.x + vi.y * wj.y + wi.x * vj.x + wi.y * vj.y;
+        c[r][q].y -= vi.y * wj.x - vi.x * wj.y + wi.y * vj.x - wi.x * vj.y;
+      }
+    }
+    // row k is final (diagonal and sub-diagonal); row k + 1, conjugated, is the next column
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int i = warp + kRrWarps * r;
+      if (i == k) {
+#pragma unroll
+        for (int q = 0; q < CC; ++q) {
+          const int j = lane + 32 * q;
+          if (j == k) sh.td[k] = c[r][q].x;
+          if (j == k + 1) sh.esub[k] = make_double2(c[r][q].x, -c[r][q].y);
+        }
+      }
+      if (i == k + 1) {
+#pragma unroll
+        for (int q = 0; q < CC; ++q) {
+          const int j = lane + 32 * q;
+          if (j < n) sh.xcol[j] = j > k + 1 ? make_double2(c[r][q].x, -c[r][q].y) : make_double2(0.0, 0.0);
+        }
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int r = 0; r < R; ++r) {                    // the last two rows
+    const int i = warp + kRrWarps * r;
+#pragma unroll
+    for (int q = 0; q < CC; ++q) {
+      const int j = lane + 32 * q;
+      if (n >= 2 && i == n - 2) {
+        if (j == n - 2) sh.td[n - 2] = c[r][q].x;
+        if (j == n - 1) sh.esub[n - 2] = make_double2(c[r][q].x, -c[r][q].y);
+      }
+      if (i == n - 1 && j == n - 1) sh.td[n - 1] = c[r][q].x;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double2 p = make_double2(1.0, 0.0);
+    for (int i = 0; i < n; ++i) {
+      sh.ph[i] = p;
+      if (i + 1 < n) {
+        const double2 e = sh.esub[i];
+        const double ae = sqrt(e.x * e.x + e.y * e.y);
+        sh.tb[i] = ae;
+        sh.e2[i] = ae * ae;
+        if (ae > 0.0) p = cmul(p, make_double2(e.x / ae, e.y / ae));
+      }
+    }
+    sh.tb[n - 1] = 0.0;
+    sh.e2[n - 1] = 0.0;
+  }
+  __syncthreads();
+}
+
+// Eigenvalues of the tridiagonal below x: sign changes of the leading-minor determinants
+// p_{i+1} = (d_i - x) p_i - e_{i-1}^2 p_{i-1} (the Sturm sequence; an FMA per step where the
+// ratio form needs a division), both kept in [2^-600, 2^600] by a common power-of-two scale; a
+// zero is replaced by -2^-300 times its predecessor (a zero pivot counts as negative).
+static __device__ __forceinline__ int rr_sturm(const double* __restrict__ td,
+                                               const double* __restrict__ e2, int n, double x) {
+  const double big = 0x1p600, small = 0x1p-600;
+  double pm = 1.0, p = td[0] - x;
+  if (p == 0.0) p = -0x1p-300;
+  bool neg = p < 0.0;
+  int c = neg;
+#pragma unroll 4
+  for (int i = 1; i < n; ++i) {
+    double pn = fma(td[i] - x, p, -e2[i - 1] * pm);
+    pn = pn == 0.0 ? -0x1p-300 * p : pn;
+    const double m = fmax(fabs(pn), fabs(p));
+    const double f = m > big ? small : (m < small ? big : 1.0);
+    pm = p * f; p = pn * f;
+    const bool ng = p < 0.0;
+    c += ng != neg;
+    neg = ng;
+  }
+  return c;
+}
+
+// The nwant smallest eigenpairs of A x = lambda B x (B = nullptr: the identity), A and B n x n
+// Hermitian (global, ld n): w[0..nwant) ascending and Vout[:, 0..nwant) (ld n; the other columns
+// are zeroed). Steps: B = U^H U (rr_cholesky); C^H = (U^-H A U^-1)^H by two row solves
+// (rr_rows_solve); Householder to the real tridiagonal T (rr_tridiag); eigenvalues by
+// multisection (G lanes per eigenvalue, Sturm counts, G + 1 sub-intervals per round, down to
+// 2 eps ||T||); eigenvectors by two inverse-iteration steps (a thread per eigenvalue, LU of
+// T - lambda I with partial pivoting, pseudo-random start), orthonormalised by two Cholesky-QR
+// passes; V = U^-1 Q D Z with the reflectors applied in reverse order. Returns 0, 1 (B not
+// positive definite), 2 (non-finite T) or 3 (inverse-iteration vectors not independent: the
+// caller then solves the full problem). S0 / S1: n x n shared matrices.
+template <int R, int CC>
+static __device__ int rr_wanted(const double2* __restrict__ A, const double2* __restrict__ B,
+                                int n, int nwant, double* __restrict__ w,
+                                double2* __restrict__ Vout, double2* S0, double2* S1,
+                                RrShared& sh) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwp = blockDim.x >> 5;
+  const double eps = 1.1102230246251565e-16;
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) S1[e] = A[e];
+  if (B) {
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) S0[e] = B[e];
+    __syncthreads();
+    if (rr_cholesky(S0, n, sh.rinv)) return 1;
+    rr_rows_solve<R, CC>(S1, S0, n, sh.rinv, true);      // W^H with W = A U^-1
+    rr_rows_solve<R, CC>(S1, S0, n, sh.rinv, false);     // W^H U^-1 = C^H
+  } else {
+    __syncthreads();
+  }
+  rr_tridiag<R, CC>(S1, n, S0, sh);     // reflectors below S0's diagonal, U above it
+  // ---- Gershgorin bounds ----
+  if (warp == 0) {
+    double lo = INFINITY, hi = -INFINITY;
+    for (int i = lane; i < n; i += 32) {
+      const double r = (i > 0 ? sh.tb[i - 1] : 0.0) + (i + 1 < n ? sh.tb[i] : 0.0);
+      lo = fmin(lo, sh.td[i] - r);
+      hi = fmax(hi, sh.td[i] + r);
+    }
+    lo = warp_min(lo);
+    hi = warp_max(hi);
+    if (lane == 0) {
+      const double tn = fmax(fabs(lo), fabs(hi));
+      sh.lo = lo - 4.0 * eps * tn * n - 1e-300;
+      sh.hi = hi + 4.0 * eps * tn * n + 1e-300;
+      sh.bad = !(isfinite(lo) && isfinite(hi));
+    }
+  }
+  __syncthreads();
+  if (sh.bad) return 2;
+  const double tn = fmax(fabs(sh.lo), fabs(sh.hi));
+  // ---- multisection: lanes t of group g evaluate a + (b - a)(t + 1) / (G + 1) ----
+  int G = 32;
+  while (G > 1 && nwant * G > (int)blockDim.x) G >>= 1;
+  {
+    const int g = threadIdx.x / G, t = threadIdx.x % G;
+    const int base = lane / G * G;
+    const unsigned gmask = (G == 32 ? 0xffffffffu : ((1u << G) - 1u) << base);
+    const bool act = g < nwant;
+    double a = sh.lo, b = sh.hi;
+    for (int round = 0; round < 64; ++round) {
+      const bool conv = !act || (b - a) <= fmax(2.0 * eps * tn, 4.0 * eps * fmax(fabs(a), fabs(b)));
+      if (__all_sync(0xffffffffu, conv)) break;
+      const double x = a + (b - a) * ((double)(t + 1) / (double)(G + 1));
+      const int cnt = rr_sturm(sh.td, sh.e2, n, x);
+      const unsigned below = __ballot_sync(0xffffffffu, cnt <= g) & gmask;   // x below lambda_g
+      const int hiT = below ? 31 - __clz(below) - base : -1;
+      const unsigned above = ~below & gmask;
+      const int loT = above ? __ffs(above) - 1 - base : G;
+      const double na = hiT >= 0 ? a + (b - a) * ((double)(hiT + 1) / (double)(G + 1)) : a;
+      const double nb = loT < G ? a + (b - a) * ((double)(loT + 1) / (double)(G + 1)) : b;
+      a = conv ? a : na;
+      b = conv ? b : nb;
+    }
+    if (act && t == 0) sh.lam[g] = 0.5 * (a + b);
+  }
+  __syncthreads();
+  // ---- inverse iteration: arrays interleaved [i][j] in S1 (free after the tridiagonalisation) ----
+  const int zs = (n * nwant + 1) & ~1;
+  double* Z = reinterpret_cast<double*>(S1);
+  double* ur = Z + zs;                  // 1 / pivot of U's row i
+  double* u1 = ur + n * nwant;          // U_{i,i+1}
+  double* u2 = u1 + n * nwant;          // U_{i,i+2} (from row exchanges)
+  const double tiny = eps * tn + 1e-300;
+  if ((int)threadIdx.x < nwant) {
+    const int j = threadIdx.x;
+    const double mu = sh.lam[j];
+    for (int i = 0; i < n; ++i) Z[i * nwant + j] = start_value(i, j);
+    for (int step = 0; step < 2; ++step) {
+      // forward: factor T - mu I row by row, exchanging rows when the sub-diagonal is larger,
+      // and eliminate the right-hand side alongside
+      double a = sh.td[0] - mu, bcur = n > 1 ? sh.tb[0] : 0.0;
+      double y = Z[j];
+      for (int i = 0; i + 1 < n; ++i) {
+        const double cc = sh.tb[i];
+        const double an = sh.td[i + 1] - mu;
+        const double bn = i + 2 < n ? sh.tb[i + 1] : 0.0;
+        const double yn = Z[(i + 1) * nwant + j];
+        const bool sw = fabs(a) < fabs(cc);
+        const double ap = fabs(a) < tiny ? (a < 0.0 ? -tiny : tiny) : a;
+        const double ri = 1.0 / (sw ? cc : ap);
+        const double l = (sw ? a : cc) * ri;
+        ur[i * nwant + j] = ri;
+        u1[i * nwant + j] = sw ? an : bcur;
+        u2[i * nwant + j] = sw ? bn : 0.0;
+        Z[i * nwant + j] = sw ? yn : y;
+        const double na = sw ? bcur - l * an : an - l * bcur;
+        const double ny = sw ? y - l * yn : yn - l * y;
+        bcur = sw ? -l * bn : bn;
+        a = na;
+        y = ny;
+      }
+      const double ap = fabs(a) < tiny ? (a < 0.0 ? -tiny : tiny) : a;
+      ur[(n - 1) * nwant + j] = 1.0 / ap;
+      u1[(n - 1) * nwant + j] = 0.0;
+      u2[(n - 1) * nwant + j] = 0.0;
+      Z[(n - 1) * nwant + j] = y;
+      double x1 = 0.0, x2 = 0.0, mx = 0.0;          // back substitution
+      for (int i = n - 1; i >= 0; --i) {
+        const double x = (Z[i * nwant + j] - u1[i * nwant + j] * x1 - u2[i * nwant + j] * x2) * ur[i * nwant + j];
+        Z[i * nwant + j] = x;
+        x2 = x1;
+        x1 = x;
+        mx = fmax(mx, fabs(x));
+      }
+      const double sc = mx > 0.0 && isfinite(mx) ? 1.0 / mx : 0.0;
+      for (int i = 0; i < n; ++i) Z[i * nwant + j] *= sc;
+    }
+  }
+  __syncthreads();
+  // ---- Cholesky-QR, twice: G = Z^T Z (a thread per entry), G = R^T R (warp 0; the diagonal
+  //      holds 1 / R_kk), Z <- Z R^-1 (a thread per row, the row in registers) ----
+  const int ng = nwant * (nwant + 1) / 2;
+  for (int pass = 0; pass < 2; ++pass) {
+    for (int e = threadIdx.x; e < ng; e += blockDim.x) {
+      int a = 0, rem = e;
+      while (rem >= nwant - a) { rem -= nwant - a; ++a; }
+      const int b = a + rem;
+      double d = 0.0;
+      for (int i = 0; i < n; ++i) d = fma(Z[i * nwant + a], Z[i * nwant + b], d);
+      sh.G[a * nwant + b] = d;
+      sh.G[b * nwant + a] = d;
+    }
+    __syncthreads();
+    if (warp == 0) {
+      int bad = 0;
+      for (int k = 0; k < nwant; ++k) {
+        const double d0 = sh.G[k * nwant + k];
+        __syncwarp();
+        // the vectors have max-abs 1 (first pass) or unit norm (second): a pivot this small means
+        // a vector (nearly) in the span of the previous ones
+        if (!(d0 > 1e-10) || !isfinite(d0)) bad = 1;
+        const double ri = bad ? 0.0 : 1.0 / sqrt(d0);
+        for (int j = k + lane; j < nwant; j += 32) sh.G[k * nwant + j] = j == k ? ri : sh.G[k * nwant + j] * ri;
+        __syncwarp();
+        for (int j = k + 1 + lane; j < nwant; j += 32) {
+          const double gkj = sh.G[k * nwant + j];
+          for (int i = k + 1; i <= j; ++i) sh.G[i * nwant + j] -= sh.G[k * nwant + i] * gkj;
+        }
+        __syncwarp();
+      }
+      if (lane == 0) sh.bad = bad;
+    }
+    __syncthreads();
+    if (sh.bad) return 3;
+    if ((int)threadIdx.x < n) {
+      const int i = threadIdx.x;
+      double z[kMaxBlock];
+#pragma unroll
+      for (int k = 0; k < kMaxBlock; ++k) z[k] = k < nwant ? Z[i * nwant + k] : 0.0;
+#pragma unroll
+      for (int k = 0; k < kMaxBlock; ++k) {
+        if (k < nwant) {
+          z[k] *= sh.G[k * nwant + k];
+#pragma unroll
+          for (int jj = k + 1; jj < kMaxBlock; ++jj)
+            if (jj < nwant) z[jj] -= z[k] * sh.G[k * nwant + jj];
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < kMaxBlock; ++k) if (k < nwant) Z[i * nwant + k] = z[k];
+    }
+    __syncthreads();
+  }
+  // ---- V = U^-1 Q D Z: a warp per column, the column in registers (lane l holds rows l + 32 q):
+  //      phases, reflectors n-3 .. 0, back substitution ----
+  for (int j = warp; j < nwant; j += nwp) {
+    double2 y[CC];
+#pragma unroll
+    for (int q = 0; q < CC; ++q) {
+      const int i = lane + 32 * q;
+      const double z = i < n ? Z[i * nwant + j] : 0.0;
+      y[q] = i < n ? make_double2(sh.ph[i].x * z, sh.ph[i].y * z) : make_double2(0.0, 0.0);
+    }
+    for (int k = n - 3; k >= 0; --k) {
+      const double tk = sh.tau[k];
+      const double2* vrow = S0 + (n - 1 - k) * n - (k + 1);   // v_i at vrow[i], i > k
+      double2 v[CC];
+      double sx = 0.0, sy = 0.0;                                // v^H y
+#pragma unroll
+      for (int q = 0; q < CC; ++q) {
+        const int i = lane + 32 * q;
+        v[q] = (i > k && i < n) ? vrow[i] : make_double2(0.0, 0.0);
+        sx += v[q].x * y[q].x + v[q].y * y[q].y;
+        sy += v[q].x * y[q].y - v[q].y * y[q].x;
+      }
+      sx = tk * warp_sum(sx);
+      sy = tk * warp_sum(sy);
+#pragma unroll
+      for (int q = 0; q < CC; ++q) {
+        y[q].x -= v[q].x * sx - v[q].y * sy;
+        y[q].y -= v[q].x * sy + v[q].y * sx;
+      }
+    }
+    if (B) {
+      for (int k = n - 1; k >= 0; --k) {
+        const int kl = k & 31, kq = k >> 5;
+        double2 yk = y[0];
+#pragma unroll
+        for (int q = 1; q < CC; ++q) if (kq == q) yk = y[q];
+        const double r = sh.rinv[k];
+        const double2 xk = make_double2(__shfl_sync(0xffffffffu, yk.x, kl) * r,
+                                        __shfl_sync(0xffffffffu, yk.y, kl) * r);
+#pragma unroll
+        for (int q = 0; q < CC; ++q) {
+          const int i = lane + 32 * q;
+          if (i == k) y[q] = xk;
+          const double2 u = i < k ? S0[i * n + k] : make_double2(0.0, 0.0);
+          y[q].x -= u.x * xk.x - u.y * xk.y;
+          y[q].y -= u.x * xk.y + u.y * xk.x;
+        }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < CC; ++q) {
+      const int i = lane + 32 * q;
+      if (i < n) Vout[i * n + j] = y[q];
+    }
+  }
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+    const int i = e / n, j = e - i * n;
+    if (j >= nwant) Vout[e] = make_double2(0.0, 0.0);
+  }
+  for (int j = threadIdx.x; j < nwant; j += blockDim.x) w[j] = sh.lam[j];
+  __syncthreads();
+  return 0;
+}
+
+// rr_wanted when it applies (nwant < n, the inverse-iteration arrays fit S1, 512 threads);
+// returns -1 when it does not apply
+static __device__ int block_eigh_wanted(const double2* __restrict__ A,
+                                        const double2* __restrict__ B, int n, int nwant,
+                                        double* __restrict__ w, double2* __restrict__ Vout,
+                                        double2* S0, double2* S1) {
+  __shared__ RrShared sh;
+  if (nwant < 1 || nwant >= n || nwant > kMaxBlock || (int)blockDim.x != 32 * kRrWarps ||
+      ((n * nwant + 1) & ~1) + 3 * n * nwant > 2 * n * n)
+    return -1;
+  if (n <= 48) return rr_wanted<3, 2>(A, B, n, nwant, w, Vout, S0, S1, sh);
+  return rr_wanted<5, 3>(A, B, n, nwant, w, Vout, S0, S1, sh);
+}
+
 // w ascending, V columns permuted accordingly; generalized problem through B = U^H U.
 // Returns 0 (ok), 1 (B not positive definite) or 2 (non-finite eigenvalue); block-uniform.
-// S0, S1: n x n shared-memory matrices; scratch: 2 n^2 global elements.
+// S0, S1: n x n shared-memory matrices; scratch: 2 n^2 global elements. With 0 < nwant < n only
+// the nwant smallest pairs are required (w[0..nwant), V's first nwant columns): block_eigh_wanted
+// computes them, the QL path below is taken when it does not apply or its vectors collapse.
 static __device__ int block_eigh(const double2* __restrict__ A, const double2* __restrict__ B,
                                  int n, double* __restrict__ w, double2* __restrict__ Vout,
-                                 double2* __restrict__ scratch, double2* S0, double2* S1) {
+                                 double2* __restrict__ scratch, double2* S0, double2* S1,
+                                 int nwant = 0) {
+  if (nwant > 0 && nwant < n) {
+    const int r = block_eigh_wanted(A, B, n, nwant, w, Vout, S0, S1);
+    if (r == 0 || r == 1) return r;                // else: the full problem below
+  }
   double2* Ug = scratch;           // Uinv (global)
   double2* Tg = scratch + n * n;   // A Uinv (global)
   __shared__ int rank[kMaxSmall];

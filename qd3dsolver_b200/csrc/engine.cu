@@ -476,7 +476,8 @@ __global__ void __launch_bounds__(kSmallThreads) e_rr_kernel(const ESlot* __rest
   for (int attempt = 0; attempt < 2; ++attempt) {
     int dim;
     e_assemble(d, st, use_restart, dim);
-    const int r = block_eigh(d.gA, d.gB, dim, d.w, d.E, d.scr, rsm, rsm + dim * dim);
+    // only the first m Ritz pairs are kept
+    const int r = block_eigh(d.gA, d.gB, dim, d.w, d.E, d.scr, rsm, rsm + dim * dim, d.m);
     if (threadIdx.x == 0) { ok = r == 0; dim_s = dim; }
     __syncthreads();
     if (ok || use_restart) break;

@@ -436,7 +436,7 @@ int qdkp_lobpcg_solve(const qdkp_operator* op, const qdkp_lobpcg_params* prm, co
       assemble(hS, hT, m, ma, mp, restart, explicit_gram, lam, gA, gB, dim);
       TRY(s.put(b.gA, gA.data(), gA.size() * sizeof(double2)));
       TRY(s.put(b.gB, gB.data(), gB.size() * sizeof(double2)));
-      TRY(launch_eigh(b.gA, b.gB, dim, b.w, b.E, b.scr, b.status, st));
+      TRY(launch_eigh(b.gA, b.gB, dim, b.w, b.E, b.scr, b.status, st, m));   // m pairs kept
       TRY(s.sync_read(hstat, b.status, sizeof(int)));
       solved = hstat[0] == 0;
     }
