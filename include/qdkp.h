@@ -363,6 +363,33 @@ int qdkp_local_band_edges(const qdkp_operator* op, const unsigned char* mask, do
  * own small tables on the device) and run with the work area in the caller's workspace.
  * Asynchronous on `stream`.
  */
+/*
+ * Inhomogeneous elastic strain by the FD (Q1 finite-element) energy minimisation of
+ * elasticity_fd.solve_strain_fd (elasticity_fd.py:211-419): trilinear hexahedra with 2x2x2 Gauss
+ * quadrature on the periodic (nx, ny, nz) cell of spacing h, the dot (mask, device, n_sites
+ * bytes, on element centres) with its own cubic constants C_dot[3] = (C11, C12, C44) and the
+ * matrix with C_matrix[3], the dilatational eigenstrain -eps_star inside the dot; solved by CG
+ * preconditioned with the exact Fourier inverse of the volume-averaged homogeneous operator, to
+ * ||r|| / ||f|| < tol or maxiter iterations. strain (device, 6 x n_sites) gets the ELASTIC strain
+ * exx, eyy, ezz, exy, eyz, ezx at the element centres; total (device, may be NULL) the total
+ * strain (no eigenstrain term). info (host) receives iterations, relative residual, the dropped
+ * preconditioner modes (1 = only k = 0), a breakdown code (0 none; 1 preconditioner not positive
+ * definite; 2 non-positive curvature; 3 preconditioner lost definiteness) and converged
+ * (residual below tol, no breakdown, no dropped mode but k = 0). Synchronous on `stream`.
+ */
+typedef struct {
+  int iterations;
+  double residual;
+  int modes_dropped;
+  int breakdown;
+  int converged;
+} qdkp_fd_info;
+size_t qdkp_fd_strain_workspace_size(int nx, int ny, int nz);
+int qdkp_fd_strain(int nx, int ny, int nz, double h, const unsigned char* mask, double eps_star,
+                   const double* C_dot, const double* C_matrix, double tol, int maxiter,
+                   double* strain, double* total, qdkp_fd_info* info, void* ws, size_t ws_bytes,
+                   void* stream);
+
 size_t qdkp_fourier_strain_workspace_size(int nx, int ny, int nz);
 int qdkp_fourier_strain(int nx, int ny, int nz, double h, const unsigned char* mask,
                         double eps_star, double C11, double C12, double C44, double* strain,

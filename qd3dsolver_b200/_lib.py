@@ -32,6 +32,12 @@ class LobpcgParams(ctypes.Structure):
                 ('stall_iterations', ctypes.c_int)]
 
 
+class FdInfo(ctypes.Structure):
+    _fields_ = [('iterations', ctypes.c_int), ('residual', ctypes.c_double),
+                ('modes_dropped', ctypes.c_int), ('breakdown', ctypes.c_int),
+                ('converged', ctypes.c_int)]
+
+
 class LobpcgInfo(ctypes.Structure):
     _fields_ = [('iterations', ctypes.c_int), ('best_iteration', ctypes.c_int),
                 ('status', ctypes.c_int), ('explicit_gram', ctypes.c_int),
@@ -105,6 +111,12 @@ _SIGNATURES = {
                                        ctypes.c_void_p, ctypes.c_int64, ctypes.c_int,
                                        ctypes.c_int64, ctypes.c_int, ctypes.c_void_p,
                                        ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]),
+    'qdkp_fd_strain_workspace_size': (ctypes.c_size_t, [ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    'qdkp_fd_strain': (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                      ctypes.c_void_p, ctypes.c_double, ctypes.c_void_p,
+                                      ctypes.c_void_p, ctypes.c_double, ctypes.c_int,
+                                      ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(FdInfo),
+                                      ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]),
     'qdkp_block_eigh_workspace_size': (ctypes.c_size_t, [ctypes.c_int]),
     'qdkp_block_eigh': (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
                                        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,

@@ -8,6 +8,8 @@
 namespace qdkp {
 
 // Per-slot mutable state (device memory, written by the decision kernels).
+constexpr int kEGramSplit = 16;      // groups of Gram partials summed by their last CTA
+
 struct EState {
   int running;          // 1 while the slot iterates
   int status;           // QDKP_LOBPCG_* once it stopped
@@ -26,6 +28,9 @@ struct EState {
   int idx[kMaxBlock];
   double lam[kMaxBlock];
   double norms[kMaxBlock];
+  // CTAs of the current Gram product done, per partial group; the last slot counts the groups
+  // reduced. The CTA that completes a count resets it to 0.
+  int gram_done[kEGramSplit + 1];
 };
 
 // Per-slot constant descriptor (built on the host at admission, device resident).
