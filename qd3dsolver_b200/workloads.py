@@ -266,15 +266,27 @@ class Workload:
 
 
 def build_environment(name, mask, h, dot, matrix, piezo=False, k=8, sigma_e_outside=False,
-                      meta=None, device=False):
+                      meta=None, device=False, strain='fourier'):
     """Strain, band edges, coefficient fields and both sigmas of one dot. device=True runs the
     strain, the piezo potential and the valence-edge sigma on the GPU (qd3dsolver_b200.fields,
     kp_pryor.hole_sigma); the same arithmetic, for batches whose host preparation would
-    otherwise take minutes."""
+    otherwise take minutes. strain='fd' (device only) is the inhomogeneous FD elasticity with the
+    dot's and the matrix's own constants at tol 1e-10, as heterostructure.build computes it
+    (heterostructure.py:284-291); 'fourier' the homogeneous solution with the matrix's."""
+    if strain not in ('fourier', 'fd'):
+        raise ValueError("strain must be 'fourier' or 'fd'")
+    if strain == 'fd' and not device:
+        raise ValueError("strain='fd' runs on the device only (device=True)")
     if device:
         from . import fields as dfields, kp_pryor as kpd
-        sd = dfields.solve_strain(mask, misfit(dot, matrix), matrix['C11'], matrix['C12'],
-                                  matrix['C44'], h)
+        if strain == 'fd':
+            sd = dfields.solve_strain_fd(mask, misfit(dot, matrix),
+                                         (dot['C11'], dot['C12'], dot['C44']),
+                                         (matrix['C11'], matrix['C12'], matrix['C44']), h,
+                                         tol=1e-10)
+        else:
+            sd = dfields.solve_strain(mask, misfit(dot, matrix), matrix['C11'], matrix['C12'],
+                                      matrix['C44'], h)
         st = sd.as_dict()
     else:
         st = solve_strain(mask, misfit(dot, matrix), matrix['C11'], matrix['C12'], matrix['C44'], h)
@@ -349,7 +361,7 @@ def random_dot(rng, h=0.5, n_min=32, n_max=96, pairs=(2, 8), family='InGaAs/GaAs
     return build_environment(f"{shape_kind}_x{x:.2f}_b{base:.1f}_{nxy}x{nxy}x{nz}", mask, h,
                              dot, material('GaAs'), k=2 * npairs,
                              meta=dict(x=x, kind=shape_kind, base=base, height=height),
-                             device=device)
+                             device=device, strain='fd' if device else 'fourier')
 
 
 def antimonide_request(rng, n_min=32, n_max=128, pairs=(2, 8), device=False):
@@ -361,9 +373,9 @@ def antimonide_request(rng, n_min=32, n_max=128, pairs=(2, 8), device=False):
 
     Choices the stream leaves open, fixed here: half the dots are InSb and half the alloy; a
     lens has height / radius ~ U[0.3, 0.6]; a dash has length 2 r, width ~ U[0.5, 1] x length
-    and the height of a lens of the same radius, capped by its facets. Strain is the
-    homogeneous Fourier solution with the matrix's elastic constants (the reference's
-    heterostructure.build uses its FD elasticity solver, a host preprocessing step).
+    and the height of a lens of the same radius, capped by its facets. Strain: with device=True
+    the inhomogeneous FD elasticity, as the reference's heterostructure.build computes it; on the
+    host the homogeneous Fourier solution with the matrix's elastic constants.
     Returns (Workload, band)."""
     insb = rng.random() < 0.5
     x = 1.0 if insb else rng.uniform(0.3, 1.0)
@@ -392,7 +404,7 @@ def antimonide_request(rng, n_min=32, n_max=128, pairs=(2, 8), device=False):
                           f"{n_xy}x{n_xy}x{n_z}", mask, h, dot, material('InAs'), piezo=True,
                           k=2 * npairs, sigma_e_outside=True,
                           meta=dict(x=x, kind=kind, radius=r, height=hgt, band=band),
-                          device=device)
+                          device=device, strain='fd' if device else 'fourier')
     return w, band
 
 
@@ -426,19 +438,28 @@ def fig4_grid(base, h=1.0, pad=8.0):
     return pyramid_mask(X, Y, Z, base)
 
 
-def fig4_environment(base, h=1.0, pad=8.0, piezo=True):
+def fig4_environment(base, h=1.0, pad=8.0, piezo=True, strain='fourier'):
     """Pryor's b-nm pyramid (Table I parameters, first-order piezo potential applied as
     U = -phi to both edges, sigma_e = Ec[dot].min(), sigma_h = exact valence edge), as
     pryor_fig4.environment builds it (pryor_fig4.py:109-153).
 
-    Deviation, stated: the strain is the homogeneous Fourier solution with GaAs elastic constants
-    (strain_fourier.solve_strain) instead of the inhomogeneous FD elasticity PCG
-    (elasticity_fd.solve_strain_fd), a host preprocessing step this package does not rebuild.
+    strain='fd': the inhomogeneous FD elasticity with the dot's and the matrix's constants at
+    tol 1e-10, as the reference computes it (pryor_fig4.py:115), on the device
+    (fields.solve_strain_fd). strain='fourier' (host): the homogeneous Fourier solution with
+    GaAs elastic constants (strain_fourier.solve_strain), a stated deviation.
     """
     dot, mat = PRYOR_TABLE_I['InAs'], PRYOR_TABLE_I['GaAs']
     pyr = fig4_grid(base, h, pad)
     eps_star = (mat['a0'] - dot['a0']) / dot['a0']
-    st = solve_strain(pyr, eps_star, mat['C11'], mat['C12'], mat['C44'], h)
+    if strain == 'fd':
+        from . import fields as dfields
+        st = dfields.solve_strain_fd(pyr, eps_star, (dot['C11'], dot['C12'], dot['C44']),
+                                     (mat['C11'], mat['C12'], mat['C44']), h,
+                                     tol=1e-10).as_dict()
+    elif strain == 'fourier':
+        st = solve_strain(pyr, eps_star, mat['C11'], mat['C12'], mat['C44'], h)
+    else:
+        raise ValueError("strain must be 'fourier' or 'fd'")
     trace = st['exx'] + st['eyy'] + st['ezz']
     Ev0 = np.where(pyr, dot['E_vbo'], mat['E_vbo'])
     Ec0 = Ev0 + np.where(pyr, dot['Eg'], mat['Eg'])

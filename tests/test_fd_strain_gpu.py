@@ -69,3 +69,20 @@ def test_fd_strain_unconverged_raises():
     st = fields.solve_strain_fd(fx['mask'], f['eps_star'], f['C_dot'], f['C_matrix'], f['h'],
                                 tol=1e-10, maxiter=2, require_converged=False)
     assert not st.cg_converged and st.cg_iterations == 2 and st.cg_residual > 1e-10
+
+
+def test_fig4_environment_fd_strain_matches_reference_fields():
+    """workloads.fig4_environment(strain='fd') with this package's Pryor Table I constants and
+    eigenstrain reproduces the reference environment's FD strain (pryor_fig4.py:115)."""
+    from qd3dsolver_b200 import workloads as wl
+    fx = np.load(os.path.join(GOLDEN, 'fig4_b10_fields.npz'))
+    w = wl.fig4_environment(10.0, strain='fd')
+    assert w.mask.shape == fx['mask'].shape and np.array_equal(w.mask, fx['mask'])
+    scale = max(np.abs(fx[k]).max() for k in STRAIN)
+    err = max(np.abs(w.fields[k] - fx[k]).max() for k in STRAIN) / scale
+    assert err < TOL, err
+    # and the band edges and sigmas built from it (Bir-Pikus shifts, piezo potential)
+    for k in ('Ec', 'Ev'):
+        assert np.abs(w.fields[k] - fx[k]).max() < 1e-8, k
+    assert abs(w.sigma['cb'] - float(fx['sigma_e'])) < 1e-8
+    assert abs(w.sigma['vb'] - float(fx['sigma_h'])) < 1e-8
