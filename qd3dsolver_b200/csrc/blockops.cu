@@ -151,57 +151,36 @@ constexpr int kGramParts = 296;
 // f64 kind). A CTA of 3 x 3 warps owns all 8x8 tiles of C' for its slice of rows; each warp
 // owns a rectangle of up to 6 x 6 tiles and keeps them in registers across the slice.
 
+constexpr int kGramSplit = 16;
+
+// A CTA per (row part, column panel): its partial of C', then the last CTAs reduce the
+// partials into `result` (gram_finish_last; `counters`: kGramSplit + 1 zeroed ints)
 template <int MR, int MC, typename T>
 __global__ void __launch_bounds__(512)
 gram_partial_kernel(const BlockList<T> A, const BlockList<T> B, long long n,
-                    long long rows_per_part, double* __restrict__ partial, int ptc) {
+                    long long rows_per_part, double* __restrict__ partial, int ptc,
+                    int* __restrict__ counters, double2* __restrict__ result) {
   extern __shared__ __align__(16) unsigned char gsm_d[];
   const int RP = (2 * A.total() + 7) / 8 * 8, RQ = (2 * B.total() + 7) / 8 * 8;
   const long long r0 = blockIdx.x * rows_per_part;
   double* out = partial + (long long)blockIdx.x * RP * RQ;
+  bool done = false;
   if constexpr (std::is_same<T, float>::value) {
     if (gridDim.y == 1 && gram_tf32_rects(A.total(), B.total()) <= (int)(blockDim.x >> 5)) {
       gram_core_tf32(A, B, r0, min(n, r0 + rows_per_part), out, gsm_d);
-      return;
+      done = true;
     }
   }
-  gram_core<MR, MC>(A, B, r0, min(n, r0 + rows_per_part), out, gsm_d, blockIdx.y * ptc, ptc);
-}
-
-// Stage 1: column-block sums of the partial C' slices (coalesced over the RP x RQ elements);
-// stage 2: the remaining per-split sums folded into the complex Gram matrix.
-constexpr int kGramSplit = 16;
-
-__global__ void gram_reduce1_kernel(const double* __restrict__ partial, int nparts, int elems,
-                                    double* __restrict__ out) {
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  const int sp = blockIdx.y;
-  if (e >= elems) return;
-  const int per = (nparts + kGramSplit - 1) / kGramSplit;
-  const int b0 = sp * per, b1 = min(nparts, b0 + per);
-  double s = 0.0;
-  for (int b = b0; b < b1; ++b) s += partial[(long long)b * elems + e];
-  out[(long long)sp * elems + e] = s;
-}
-
-__global__ void gram_reduce2_kernel(const double* __restrict__ part2, int P, int Q, int RQ,
-                                    int elems, double2* __restrict__ out) {
-  const int o = blockIdx.x * blockDim.x + threadIdx.x;
-  if (o >= P * Q) return;
-  const int i = o / Q, j = o - i * Q;
-  const long long rr = (long long)(2 * i) * RQ + 2 * j;   // C'_{2i,2j}
-  double re = 0.0, im = 0.0;
-  for (int sp = 0; sp < kGramSplit; ++sp) {
-    const double* c = part2 + (long long)sp * elems;
-    re += c[rr] + c[rr + RQ + 1];
-    im += c[rr + 1] - c[rr + RQ];
-  }
-  out[o] = make_double2(re, im);
+  if (!done)
+    gram_core<MR, MC>(A, B, r0, min(n, r0 + rows_per_part), out, gsm_d, blockIdx.y * ptc, ptc);
+  gram_finish_last(partial, (int)gridDim.x, kGramSplit, counters, A.total(), B.total(),
+                   (int)blockIdx.x, result);
 }
 
 size_t gram_partial_elems(int P, int Q) {
   const size_t RP = (2 * P + 7) / 8 * 8, RQ = (2 * Q + 7) / 8 * 8;
-  return (size_t)(kGramParts + kGramSplit) * RP * RQ / 2 + 1;   // in double2 units
+  // the partials, the group sums, then the kGramSplit + 1 counters
+  return (size_t)(kGramParts + kGramSplit) * RP * RQ / 2 + 1 + (kGramSplit + 1 + 3) / 4;
 }
 
 template <typename T>
@@ -219,10 +198,13 @@ int launch_gram(const BlockList<T>& A, const BlockList<T>& B, long long n,
   long long rpp = (n + parts - 1) / parts;
   rpp = (rpp + 3) / 4 * 4;
   parts = (n + rpp - 1) / rpp;
-  if ((size_t)(parts + kGramSplit) * RP * RQ > 2 * partial_elems) {
+  const size_t counter_at = ((size_t)(parts + kGramSplit) * RP * RQ + 1) / 2 + 1;   // double2 units
+  if (counter_at + (kGramSplit + 1 + 3) / 4 > partial_elems) {
     set_error("gram partial buffer too small");
     return QDKP_ERR_WORKSPACE;
   }
+  int* counters = reinterpret_cast<int*>(partial + counter_at);
+  QDKP_CUDA_TRY(cudaMemsetAsync(counters, 0, (kGramSplit + 1) * sizeof(int), st));
   const size_t smem = gram_smem_bytes(P, Q, (int)sizeof(cplx<T>));
   static bool attr = false;
   if (!attr) {
@@ -238,13 +220,7 @@ int launch_gram(const BlockList<T>& A, const BlockList<T>& B, long long n,
   }
   double* pd = reinterpret_cast<double*>(partial);
   gram_partial_kernel<3, 3, T><<<dim3((unsigned)parts, gp.panels), threads, smem, st>>>(
-      A, B, n, rpp, pd, gp.ptc);
-  count_launch();
-  const int elems = RP * RQ;
-  double* part2 = pd + (size_t)parts * elems;
-  gram_reduce1_kernel<<<dim3((elems + 255) / 256, kGramSplit), 256, 0, st>>>(pd, (int)parts, elems, part2);
-  count_launch();
-  gram_reduce2_kernel<<<(P * Q + 127) / 128, 128, 0, st>>>(part2, P, Q, RQ, elems, out);
+      A, B, n, rpp, pd, gp.ptc, counters, out);
   count_launch();
   QDKP_CUDA_TRY(cudaGetLastError());
   return QDKP_OK;

@@ -288,6 +288,61 @@ static __device__ int block_tql(double2* S0, double2* S1, int n, double2* gtmp) 
 }
 
 
+// Partial Gram sums reduced by the CTAs that finish last, with no waiting. The partials
+// (RP x RQ real each, one per part, `parts` of them) form `split` groups of consecutive parts;
+// every CTA of the launch (all parts, all column panels on blockIdx.y) counts itself in its
+// group's counter once its partial is written; the last of a group sums the group's partials
+// in part order into the group's slot after the partials, and the last group to finish folds
+// the group sums, in group order, into the complex P x Q result. The CTA that completes a count
+// resets it to zero. Sums and their order are those of a two-pass reduction.
+static __device__ void gram_finish_last(double* __restrict__ partial, int parts, int split,
+                                        int* __restrict__ counters, int P, int Q, int part,
+                                        double2* __restrict__ out) {
+  __shared__ int s_last;
+  const int RP = (2 * P + 7) / 8 * 8, RQ = (2 * Q + 7) / 8 * 8;
+  const int elems = RP * RQ;
+  const int per = (parts + split - 1) / split;
+  const int ngroups = (parts + per - 1) / per;
+  const int grp = part / per;
+  const int b0 = grp * per, b1 = min(parts, b0 + per);
+  __threadfence();                                   // this CTA's partial, device-wide
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int members = (b1 - b0) * (int)gridDim.y;
+    s_last = atomicAdd(&counters[grp], 1) == members - 1;
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  double* sums = partial + (long long)(parts + grp) * elems;
+  for (int e = threadIdx.x; e < elems; e += blockDim.x) {
+    double acc = 0.0;
+    for (int b = b0; b < b1; ++b) acc += __ldcg(partial + (long long)b * elems + e);
+    sums[e] = acc;
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    counters[grp] = 0;
+    s_last = atomicAdd(&counters[split], 1) == ngroups - 1;
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  for (int o = threadIdx.x; o < P * Q; o += blockDim.x) {
+    const int i = o / Q, j = o - i * Q;
+    const long long rr = (long long)(2 * i) * RQ + 2 * j;   // C'_{2i,2j}
+    double re = 0.0, im = 0.0;
+    for (int g = 0; g < ngroups; ++g) {
+      const double* c = partial + (long long)(parts + g) * elems;
+      re += __ldcg(c + rr) + __ldcg(c + rr + RQ + 1);
+      im += __ldcg(c + rr + 1) - __ldcg(c + rr + RQ);
+    }
+    out[o] = make_double2(re, im);
+  }
+  if (threadIdx.x == 0) counters[split] = 0;
+}
+
 // =============================================================================================
 // Rayleigh-Ritz eigensolve for the wanted eigenpairs only: LOBPCG keeps the m smallest of the
 // 3m Ritz pairs, so the tridiagonal problem is solved for those alone, by multisection with

@@ -250,57 +250,6 @@ __device__ bool gram_lists(const ESlot& d, int which, BlockList<T>& A, BlockList
 
 // Launched once per distinct block width m present: the tile shape (and so the order of every
 // sum) then depends only on the slot's own sizes, never on which other solves share the batch.
-// The partials of a Gram product are summed by the CTAs that finish last, with no waiting: the
-// parts form kEGramSplit groups; the last CTA of a group (an atomic count of the group's CTAs,
-// all column panels included) sums the group's partials in part order into the group's split
-// slot, and the last group to finish forms out = the complex product from the split sums in
-// group order. The sums and their order are those of a separate two-pass reduction.
-__device__ void e_gram_finish(const ESlot& d, int part, int P, int Q, double2* __restrict__ out) {
-  __shared__ int s_last;
-  const int RP = (2 * P + 7) / 8 * 8, RQ = (2 * Q + 7) / 8 * 8;
-  const int elems = RP * RQ;
-  const int per = (d.gparts + kEGramSplit - 1) / kEGramSplit;
-  const int ngroups = (d.gparts + per - 1) / per;
-  const int grp = part / per;
-  const int b0 = grp * per, b1 = min(d.gparts, b0 + per);
-  __threadfence();                                   // this CTA's partial, device-wide
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    const int members = (b1 - b0) * (int)gridDim.y;
-    s_last = atomicAdd(&d.st->gram_done[grp], 1) == members - 1;
-  }
-  __syncthreads();
-  if (!s_last) return;
-  __threadfence();
-  double* split = d.gpart + (long long)(d.gparts + grp) * elems;
-  for (int e = threadIdx.x; e < elems; e += blockDim.x) {
-    double s = 0.0;
-    for (int b = b0; b < b1; ++b) s += __ldcg(d.gpart + (long long)b * elems + e);
-    split[e] = s;
-  }
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    d.st->gram_done[grp] = 0;
-    s_last = atomicAdd(&d.st->gram_done[kEGramSplit], 1) == ngroups - 1;
-  }
-  __syncthreads();
-  if (!s_last) return;
-  __threadfence();
-  for (int o = threadIdx.x; o < P * Q; o += blockDim.x) {
-    const int i = o / Q, j = o - i * Q;
-    const long long rr = (long long)(2 * i) * RQ + 2 * j;
-    double re = 0.0, im = 0.0;
-    for (int sp = 0; sp < ngroups; ++sp) {
-      const double* c = d.gpart + (long long)(d.gparts + sp) * elems;
-      re += __ldcg(c + rr) + __ldcg(c + rr + RQ + 1);
-      im += __ldcg(c + rr + 1) - __ldcg(c + rr + RQ);
-    }
-    out[o] = make_double2(re, im);
-  }
-  if (threadIdx.x == 0) d.st->gram_done[kEGramSplit] = 0;
-}
-
 template <int MR, int MC>
 __global__ void __launch_bounds__(512)
 e_gram_kernel(const ESlot* __restrict__ S, int ns, int which, int m_only, int ptc) {
@@ -320,14 +269,14 @@ e_gram_kernel(const ESlot* __restrict__ S, int ns, int which, int m_only, int pt
     double* po = d.gpart + (long long)part * RP * RQ;
     gram_core<MR, MC>(A, B, r0, min(d.n, r0 + d.rows_per_gpart), po, gsm_e, blockIdx.y * ptc,
                       ptc);
-    e_gram_finish(d, part, A.total(), B.total(), out);
+    gram_finish_last(d.gpart, d.gparts, kEGramSplit, d.st->gram_done, A.total(), B.total(), part, out);
   } else {
     BlockList<double> A, B;
     if (!gram_lists<double>(d, which, A, B, out)) return;
     const int RP = (2 * A.total() + 7) / 8 * 8, RQ = (2 * B.total() + 7) / 8 * 8;
     gram_core<MR, MC>(A, B, r0, min(d.n, r0 + d.rows_per_gpart),
                       d.gpart + (long long)part * RP * RQ, gsm_e, blockIdx.y * ptc, ptc);
-    e_gram_finish(d, part, A.total(), B.total(), out);
+    gram_finish_last(d.gpart, d.gparts, kEGramSplit, d.st->gram_done, A.total(), B.total(), part, out);
   }
 }
 
