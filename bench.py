@@ -293,6 +293,16 @@ def fixed_iteration_legs(torch, device, wl1, wl2, iters):
 # Batched uneven dots and the antimonide serving stream
 # ----------------------------------------------------------------------------------------------
 
+def guarded(leg, *args):
+    """A side leg whose failure is reported in its own key instead of ending the run."""
+    import traceback
+    try:
+        return leg(*args)
+    except Exception as e:                              # noqa: BLE001 -- reported, not hidden
+        traceback.print_exc(file=sys.stderr)
+        return {'error': f'{type(e).__name__}: {e}'[:300]}
+
+
 def batched_dots_leg(torch, device, ndots, budget):
     """64 seeded In(x)Ga(1-x)As/GaAs dots (x ~ U[0.6, 1], pyramid or spherical cap, base 6-20 nm,
     h = 0.5 nm, grids 32^3 to 96x96x72, 2-8 Kramers pairs; seed 1), bands alternating cb / vb,
@@ -703,9 +713,9 @@ def run_ours(args):
         legs = None if args.no_fixed else fixed_iteration_legs(torch, device, w1, w2,
                                                                args.fixed_iterations)
         big = dict(hx2=hx2, legs=legs, w1=w1)
-    dots = (batched_dots_leg(torch, device, args.dots, args.dot_budget)
+    dots = (guarded(batched_dots_leg, torch, device, args.dots, args.dot_budget)
             if (rank == 0 and not args.no_dots) else None)
-    stream5 = (antimonide_stream_leg(torch, device, args.stream5, args.stream5_budget)
+    stream5 = (guarded(antimonide_stream_leg, torch, device, args.stream5, args.stream5_budget)
                if (rank == 0 and not args.no_stream5) else None)
     cpu = finish_cpu_children(children, refs) if children else None
     if cpu is not None and big is not None and big['legs'] is not None:
