@@ -303,6 +303,27 @@ def guarded(leg, *args):
         return {'error': f'{type(e).__name__}: {e}'[:300]}
 
 
+def fd_strain_leg(torch, w2):
+    """The inhomogeneous FD elasticity (fields.solve_strain_fd, the reference's
+    elasticity_fd.solve_strain_fd) on the 128x128x96 pyramid: InAs dot in GaAs with Pryor's
+    Table I constants, tol 1e-10, timed on the device (one warm-up solve first)."""
+    from qd3dsolver_b200 import fields, workloads as wl
+    dot, mat = wl.PRYOR_TABLE_I['InAs'], wl.PRYOR_TABLE_I['GaAs']
+    eps_star = (mat['a0'] - dot['a0']) / dot['a0']
+    args = (w2.mask, eps_star, (dot['C11'], dot['C12'], dot['C44']),
+            (mat['C11'], mat['C12'], mat['C44']), w2.h)
+    fields.solve_strain_fd(*args, tol=1e-10, device=True)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    st = fields.solve_strain_fd(*args, tol=1e-10, device=True)
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    return {'grid': 'x'.join(map(str, w2.shape)), 'sites': int(np.prod(w2.shape)),
+            'seconds': dt, 'iterations': st.cg_iterations, 'residual': st.cg_residual,
+            'converged': st.cg_converged, 'modes_dropped': st.cg_modes_dropped,
+            'ms_per_iteration': dt / max(st.cg_iterations, 1) * 1e3}
+
+
 def batched_dots_leg(torch, device, ndots, budget):
     """64 seeded In(x)Ga(1-x)As/GaAs dots (x ~ U[0.6, 1], pyramid or spherical cap, base 6-20 nm,
     h = 0.5 nm, grids 32^3 to 96x96x72, 2-8 Kramers pairs; seed 1), bands alternating cb / vb,
@@ -712,7 +733,8 @@ def run_ours(args):
         hx2 = None if args.no_config2 else hx_roofline(torch, device, w2)
         legs = None if args.no_fixed else fixed_iteration_legs(torch, device, w1, w2,
                                                                args.fixed_iterations)
-        big = dict(hx2=hx2, legs=legs, w1=w1)
+        fd = None if args.no_config2 else guarded(fd_strain_leg, torch, w2)
+        big = dict(hx2=hx2, legs=legs, w1=w1, fd=fd)
     dots = (guarded(batched_dots_leg, torch, device, args.dots, args.dot_budget)
             if (rank == 0 and not args.no_dots) else None)
     stream5 = (guarded(antimonide_stream_leg, torch, device, args.stream5, args.stream5_budget)
@@ -788,6 +810,7 @@ def run_ours(args):
             'batched_dots': dots,
             'antimonide_stream': stream5,
             'hx_config2': hx2,
+            'fd_strain_config2': big['fd'] if big else None,
             'cpu_baseline': cpu,
             'e2e': e2e,
             'clocks': clocks,
