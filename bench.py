@@ -892,6 +892,46 @@ def engine_probe(args):
         H.close()
 
 
+def tick_probe(args):
+    """Latency of one resident solve: wall-clock milliseconds per engine tick (CUDA-graph
+    replay, 64 ticks after 8, complex64 and complex128 slots) and per plain drop-in iteration
+    ((t(40) - t(5)) / 35), on the chosen sweep solves' valence bands (prints one JSON line)."""
+    import torch
+    from qd3dsolver_b200 import eigensolvers as eg, serving
+    wls, _ = load_sweep()
+    keep = (args.probe_solves or 'b6_vb,b10_vb,b18_vb').split(',')
+    out = {}
+    for w in wls:
+        for band in BANDS:
+            tag = f"b{int(w.meta['base'])}_{band}"
+            if tag not in keep:
+                continue
+            H = make_operator(w)
+            X0 = torch.from_numpy(eg.start_block(H.shape[0], BLOCK, 0)).cuda()
+            ts = {}
+            for it in (5, 40):
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                eg.lobpcg_device(H, X0, folded=True, sigma=w.sigma[band], tol=1e-30, maxiter=it)
+                torch.cuda.synchronize()
+                ts[it] = time.perf_counter() - t0
+            rec = {'rows': H.shape[0], 'plain_ms_per_iteration': (ts[40] - ts[5]) / 35 * 1e3}
+            for prec, name in (('mixed', 'c64'), ('c128', 'c128')):
+                eng = serving.Engine(2, graphs=True)
+                eng.admit(serving.Request(H, k=K, sigma=w.sigma[band], tol=1e-30, maxiter=10 ** 6,
+                                          precision=prec))
+                eng.step(8)
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                eng.step(64)
+                torch.cuda.synchronize()
+                rec[f'{name}_ms_per_tick'] = (time.perf_counter() - t0) / 64 * 1e3
+                eng.close()
+            out[tag] = rec
+            H.close()
+    print(json.dumps({'tick_probe': out}))
+
+
 # ----------------------------------------------------------------------------------------------
 # The reference arm: the reference's CPU algorithm on the host cores
 # ----------------------------------------------------------------------------------------------
@@ -985,6 +1025,8 @@ def main():
     ap.add_argument('--probe-ticks', type=int, default=20)
     ap.add_argument('--probe-solves', default=None,
                     help='comma-separated solves of the probe (e.g. b10_vb); default all 14')
+    ap.add_argument('--tick-probe', action='store_true',
+                    help='only time lone-slot ticks and plain iterations (latency)')
     ap.add_argument('--probe-plain', action='store_true',
                     help='probe the plain drop-in (one solve after the other) instead')
     ap.add_argument('--ticks-per-poll', type=int, default=16)
@@ -1003,6 +1045,8 @@ def main():
         hx_probe(args)
     elif args.engine_probe:
         engine_probe(args)
+    elif args.tick_probe:
+        tick_probe(args)
     elif args.impl == 'reference':
         run_reference(args)
     else:
