@@ -6,6 +6,7 @@
 #include <type_traits>
 
 #include "dense_dev.cuh"
+#include "umma_dev.cuh"
 
 namespace qdkp {
 
@@ -249,6 +250,20 @@ update_kernel(const BlockList<T> A, const CoefList C, int q, long long n, cplx<T
     update_rows(A, Cf, q, r0, min(n, r0 + per), Y, ldy, accumulate, 0, usm);
 }
 
+// complex64 blocks on the tcgen05 tensor cores (umma_dev.cuh): 128-row tiles, rows of a CTA
+// contiguous
+__global__ void __launch_bounds__(kUmmaRows)
+update_umma_kernel(const BlockList<float> A, const CoefList C, int q, long long n, float2* Y,
+                   long long ldy, int accumulate) {
+  extern __shared__ __align__(128) unsigned char usm_u[];
+  const double2* Cf[3] = {C.c[0], C.c[1], C.c[2]};
+  const long long tiles = (n + kUmmaRows - 1) / kUmmaRows;
+  const long long per = (tiles + gridDim.x - 1) / gridDim.x * kUmmaRows;
+  const long long r0 = (long long)blockIdx.x * per;
+  if (r0 >= n) return;
+  update_rows_umma(A, Cf, q, r0, min(n, r0 + per), Y, ldy, accumulate, 0, usm_u);
+}
+
 template <typename T>
 int launch_update(const BlockList<T>& A, const double2* const* C, int q, long long n,
                   cplx<T>* Y, long long ldy, int accumulate, cudaStream_t st) {
@@ -256,6 +271,22 @@ int launch_update(const BlockList<T>& A, const double2* const* C, int q, long lo
   CoefList cl;
   for (int b = 0; b < 3; ++b) cl.c[b] = b < A.nblk ? C[b] : nullptr;
   const int P = A.total();
+  if constexpr (std::is_same<T, float>::value) {
+    static bool uattr = false;
+    if (!uattr) {
+      QDKP_CUDA_TRY(cudaFuncSetAttribute(update_umma_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         kUmmaSmemLimit));
+      uattr = true;
+    }
+    long long ublocks = (n + kUmmaRows - 1) / kUmmaRows;
+    if (ublocks > 148 * 4) ublocks = 148 * 4;
+    update_umma_kernel<<<(unsigned)ublocks, kUmmaRows, umma_update_smem_bytes(P, q, 1), st>>>(
+        A, cl, q, n, Y, ldy, accumulate);
+    count_launch();
+    QDKP_CUDA_TRY(cudaGetLastError());
+    return QDKP_OK;
+  }
   const size_t smem = std::is_same<T, float>::value ? update_tf32_smem_bytes(P, q)
                                                     : update_smem_bytes(P, q);
   static bool attr = false;

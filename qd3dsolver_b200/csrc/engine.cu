@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "engine_dev.cuh"
+#include "umma_dev.cuh"
 
 namespace qdkp {
 
@@ -340,6 +341,26 @@ e_update_kernel(const ESlot* __restrict__ S, int ns, int which) {
     update_rows_tf32(A, Cf, q, r0, r1, Y, (long long)q, accumulate, neg, usm_e, C2, Y2);
   else
     update_rows(A, Cf, q, r0, r1, Y, (long long)q, accumulate, neg, usm_e, C2, Y2);
+}
+
+// complex64 slots: the same updates on the tcgen05 tensor cores (umma_dev.cuh), 128 threads per
+// CTA over the same row partition; a timed-out MMA wait leaves NaN in the outputs, which the
+// slot's next residual check turns into status nonfinite
+__global__ void __launch_bounds__(kUmmaRows)
+e_update_umma_kernel(const ESlot* __restrict__ S, int ns, int which) {
+  extern __shared__ __align__(128) unsigned char usm_u[];
+  const int k = slot_of(S, ns, blockIdx.x, &ESlot::row0);
+  const ESlot& d = S[k];
+  if (d.prec != QDKP_C64) return;
+  const double2* Cf[3];
+  const double2* C2[3] = {nullptr, nullptr, nullptr};
+  int q, accumulate, neg;
+  const long long r0 = (long long)(blockIdx.x - d.row0) * d.rows_per_cta;
+  const long long r1 = min(d.n, r0 + d.rows_per_cta);
+  BlockList<float> A;
+  float2 *Y, *Y2;
+  if (!upd_lists<float>(d, which, A, Cf, q, Y, accumulate, neg, C2, Y2)) return;
+  update_rows_umma(A, Cf, q, r0, r1, Y, (long long)q, accumulate, neg, usm_u, C2, Y2);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -736,8 +757,8 @@ int launch_update_multi(const EGroup& G, int which, cudaStream_t st) {
     count_launch();
   }
   if (G.hx_ns[1]) {
-    const size_t smem = update_tf32_smem_bytes(P, G.m_max, nout);
-    e_update_kernel<float><<<G.row_ctas, kUpdThreads, smem, st>>>(G.d_slots, G.ns, which);
+    const size_t smem = umma_update_smem_bytes(P, G.m_max, nout);
+    e_update_umma_kernel<<<G.row_ctas, kUmmaRows, smem, st>>>(G.d_slots, G.ns, which);
     count_launch();
   }
   QDKP_CUDA_TRY(cudaGetLastError());
@@ -901,6 +922,8 @@ int qdkp_engine_create(int max_slots, int device, qdkp_engine** out) {
   cudaFuncSetAttribute(e_gram_kernel<3, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
   cudaFuncSetAttribute(e_update_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
   cudaFuncSetAttribute(e_update_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+  cudaFuncSetAttribute(e_update_umma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       kUmmaSmemLimit);
   cudaFuncSetAttribute(e_rr_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
   cudaFuncSetAttribute(e_rchol_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
   cudaFuncSetAttribute(e_pchol_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
