@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cmath>
 #include <type_traits>
+#include <vector>
 
 #include "dense_dev.cuh"
 #include "umma_dev.cuh"
@@ -250,18 +251,22 @@ update_kernel(const BlockList<T> A, const CoefList C, int q, long long n, cplx<T
     update_rows(A, Cf, q, r0, min(n, r0 + per), Y, ldy, accumulate, 0, usm);
 }
 
-// complex64 blocks on the tcgen05 tensor cores (umma_dev.cuh): 128-row tiles, rows of a CTA
-// contiguous
-__global__ void __launch_bounds__(kUmmaRows)
+// complex64 blocks on the tcgen05 tensor cores (umma_dev.cuh): one CTA per SM at most, each a
+// contiguous range of 128-row tiles run as one pipeline
+__global__ void __launch_bounds__(kUmmaThreads, 1)
 update_umma_kernel(const BlockList<float> A, const CoefList C, int q, long long n, float2* Y,
-                   long long ldy, int accumulate) {
+                   long long ldy, int accumulate, int cmax, int ldmax) {
   extern __shared__ __align__(128) unsigned char usm_u[];
   const double2* Cf[3] = {C.c[0], C.c[1], C.c[2]};
+  const UmmaPlan pl = umma_plan(A.total(), q, 1, cmax, ldmax);
   const long long tiles = (n + kUmmaRows - 1) / kUmmaRows;
   const long long per = (tiles + gridDim.x - 1) / gridDim.x * kUmmaRows;
   const long long r0 = (long long)blockIdx.x * per;
   if (r0 >= n) return;
-  update_rows_umma(A, Cf, q, r0, min(n, r0 + per), Y, ldy, accumulate, 0, usm_u);
+  UmmaCtx cx;
+  umma_ctx_init(cx, pl);
+  update_rows_umma(pl, cx, A, Cf, q, r0, min(n, r0 + per), Y, ldy, accumulate, 0, usm_u);
+  umma_ctx_free(cx);
 }
 
 template <typename T>
@@ -279,12 +284,41 @@ int launch_update(const BlockList<T>& A, const double2* const* C, int q, long lo
                                          kUmmaSmemLimit));
       uattr = true;
     }
+    // blocks are split into sub-blocks of at most kMaxBlock columns (the operand buffers' width),
+    // three to a launch; a list that needs more sub-blocks is formed by launches that accumulate
+    // (there Y must not alias an input). Raw stages hold rows of up to 32 complex values; a
+    // block with a longer row is read directly.
+    struct Sub { const float2* p; long long ld; int cols; const double2* c; };
+    std::vector<Sub> subs;
+    for (int b = 0; b < A.nblk; ++b)
+      for (int c0 = 0; c0 < A.cols[b]; c0 += kMaxBlock)
+        subs.push_back({A.p[b] + c0, A.ld[b], std::min(kMaxBlock, A.cols[b] - c0),
+                        C[b] ? C[b] + (size_t)c0 * q : nullptr});
+    int nsm = 148;
+    QDKP_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, 0));
     long long ublocks = (n + kUmmaRows - 1) / kUmmaRows;
-    if (ublocks > 148 * 4) ublocks = 148 * 4;
-    update_umma_kernel<<<(unsigned)ublocks, kUmmaRows, umma_update_smem_bytes(P, q, 1), st>>>(
-        A, cl, q, n, Y, ldy, accumulate);
-    count_launch();
-    QDKP_CUDA_TRY(cudaGetLastError());
+    if (ublocks > nsm) ublocks = nsm;
+    for (size_t s0 = 0; s0 < subs.size(); s0 += 3) {
+      BlockList<float> L;
+      CoefList cs;
+      L.nblk = (int)std::min<size_t>(3, subs.size() - s0);
+      int cmax = 1, ldmax = 1, Ps = 0;
+      for (int b = 0; b < 3; ++b) cs.c[b] = nullptr;
+      for (int b = 0; b < L.nblk; ++b) {
+        const Sub& u = subs[s0 + b];
+        L.p[b] = u.p; L.ld[b] = u.ld; L.cols[b] = u.cols; cs.c[b] = u.c;
+        cmax = std::max(cmax, u.cols);
+        if (u.ld <= 32) ldmax = std::max(ldmax, (int)u.ld);
+        Ps += u.cols;
+      }
+      ldmax = std::max(ldmax, cmax);
+      const UmmaPlan pl = umma_plan(Ps, q, 1, cmax, ldmax);
+      if (!pl.nout_pass) { set_error("tcgen05 update plan does not fit shared memory"); return QDKP_ERR_ARG; }
+      update_umma_kernel<<<(unsigned)ublocks, kUmmaThreads, pl.bytes, st>>>(
+          L, cs, q, n, Y, ldy, s0 == 0 ? accumulate : 1, cmax, ldmax);
+      count_launch();
+      QDKP_CUDA_TRY(cudaGetLastError());
+    }
     return QDKP_OK;
   }
   const size_t smem = std::is_same<T, float>::value ? update_tf32_smem_bytes(P, q)

@@ -343,24 +343,53 @@ e_update_kernel(const ESlot* __restrict__ S, int ns, int which) {
     update_rows(A, Cf, q, r0, r1, Y, (long long)q, accumulate, neg, usm_e, C2, Y2);
 }
 
-// complex64 slots: the same updates on the tcgen05 tensor cores (umma_dev.cuh), 128 threads per
-// CTA over the same row partition; a timed-out MMA wait leaves NaN in the outputs, which the
-// slot's next residual check turns into status nonfinite
-__global__ void __launch_bounds__(kUmmaRows)
-e_update_umma_kernel(const ESlot* __restrict__ S, int ns, int which) {
+// complex64 slots: the same updates on the tcgen05 tensor cores (umma_dev.cuh). The CTAs split
+// the 128-row tiles of the group's complex64 slots (slot k's tiles start at utile0) into
+// contiguous ranges, one CTA per SM; a CTA's tiles of one slot form one pipelined run. A wait
+// that gives up leaves NaN in the outputs, which the slot's next residual check turns into status
+// nonfinite. Every row is computed the same way whichever CTA holds it, so results do not depend
+// on the mix of slots.
+__global__ void __launch_bounds__(kUmmaThreads, 1)
+e_update_umma_kernel(const ESlot* __restrict__ S, int ns, int which, int utiles, int m_max) {
   extern __shared__ __align__(128) unsigned char usm_u[];
-  const int k = slot_of(S, ns, blockIdx.x, &ESlot::row0);
-  const ESlot& d = S[k];
-  if (d.prec != QDKP_C64) return;
-  const double2* Cf[3];
-  const double2* C2[3] = {nullptr, nullptr, nullptr};
-  int q, accumulate, neg;
-  const long long r0 = (long long)(blockIdx.x - d.row0) * d.rows_per_cta;
-  const long long r1 = min(d.n, r0 + d.rows_per_cta);
-  BlockList<float> A;
-  float2 *Y, *Y2;
-  if (!upd_lists<float>(d, which, A, Cf, q, Y, accumulate, neg, C2, Y2)) return;
-  update_rows_umma(A, Cf, q, r0, r1, Y, (long long)q, accumulate, neg, usm_u, C2, Y2);
+  const bool fused = which == UP_XPNEW || which == UP_AXPNEW;
+  const UmmaPlan pl = umma_plan((fused ? 3 : 1) * m_max, m_max, fused ? 2 : 1, m_max, m_max);
+  const long long per = (utiles + gridDim.x - 1) / gridDim.x;
+  long long c = (long long)blockIdx.x * per;
+  const long long c1 = min((long long)utiles, c + per);
+  if (c >= c1) return;
+  UmmaCtx cx;
+  umma_ctx_init(cx, pl);
+  bool ok = true;
+  while (c < c1) {
+    int k = -1;
+    long long nt = 0;
+    for (int j = 0; j < ns && k < 0; ++j) {
+      if (S[j].prec != QDKP_C64) continue;
+      nt = (S[j].n + kUmmaRows - 1) / kUmmaRows;
+      if (c >= S[j].utile0 && c < S[j].utile0 + nt) k = j;
+    }
+    if (k < 0) break;                                  // uniform; not reached
+    const ESlot& d = S[k];
+    const long long seg_end = min(c1, (long long)d.utile0 + nt);
+    const double2* Cf[3];
+    const double2* C2[3] = {nullptr, nullptr, nullptr};
+    int q, accumulate, neg;
+    BlockList<float> A;
+    float2 *Y, *Y2;
+    if (upd_lists<float>(d, which, A, Cf, q, Y, accumulate, neg, C2, Y2)) {
+      const long long r0 = (c - d.utile0) * kUmmaRows;
+      const long long r1 = min(d.n, (seg_end - d.utile0) * kUmmaRows);
+      if (ok) {
+        ok = update_rows_umma(pl, cx, A, Cf, q, r0, r1, Y, (long long)q, accumulate, neg, usm_u, C2, Y2);
+      } else {
+        float2* const Ys[2] = {Y, Y2};
+        umma_fill_nan(Ys, Y2 ? 2 : 1, q, r0, r1, (long long)q);
+      }
+    }
+    c = seg_end;
+  }
+  umma_ctx_free(cx);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -541,6 +570,8 @@ struct EGroup {
   ESlot* d_slots = nullptr;            // this group's run of the compact slot array
   HXSlot* d_hx = nullptr;              // [precision][phase][slot]: 2 x 4 x max_slots descriptors
   int ns = 0, norm_ctas = 0, gram_ctas = 0, row_ctas = 0;
+  int utiles = 0;                      // 128-row tiles of the complex64 slots (tcgen05 updates)
+  int nsm = 148;
   int hx_ns[2] = {0, 0}, hx_tiles[2] = {0, 0};   // per precision (QDKP_C128, QDKP_C64)
   int m_max = 1;
   std::vector<int> widths;             // distinct block widths among the group's slots
@@ -558,6 +589,7 @@ struct qdkp_engine {
   int* d_one = nullptr;                // constant 1 (skip flag)
   int ns = 0;                          // used slots
   int ngroups = 0;
+  int nsm = 148;                       // SMs of the device (grid of the tcgen05 updates)
   qdkp::EGroup grp[qdkp::kEGroups];
   bool dirty = true;
   // CUDA graph of `graph_ticks` ticks over the current slot layout, replayed by
@@ -644,7 +676,7 @@ int build_group(qdkp_engine* e, int g, const std::vector<int>& ids, int base, cu
   G.d_hx = e->d_hx + (size_t)g * 8 * e->max_slots;
   std::vector<ESlot> compact;
   std::vector<HXSlot> hx(8 * (size_t)e->max_slots);
-  int norm0 = 0, gram0 = 0, row0 = 0, m_max = 1;
+  int norm0 = 0, gram0 = 0, row0 = 0, m_max = 1, utile0 = 0;
   int tile0[2] = {0, 0}, kp[2] = {0, 0};
   for (int i : ids) {
     SlotHost& h = e->slots[i];
@@ -652,6 +684,8 @@ int build_group(qdkp_engine* e, int g, const std::vector<int>& ids, int base, cu
     d.norm0 = norm0; norm0 += d.nparts;
     d.gram0 = gram0; gram0 += d.gparts;
     d.row0 = row0; row0 += (int)((d.n + d.rows_per_cta - 1) / d.rows_per_cta);
+    d.utile0 = -1;
+    if (d.prec == QDKP_C64) { d.utile0 = utile0; utile0 += (int)((d.n + kUmmaRows - 1) / kUmmaRows); }
     h.d = d;
     compact.push_back(d);
     const int pi = d.prec == QDKP_C64 ? 1 : 0;
@@ -687,6 +721,8 @@ int build_group(qdkp_engine* e, int g, const std::vector<int>& ids, int base, cu
   }
   G.ns = (int)compact.size();
   G.norm_ctas = norm0; G.gram_ctas = gram0; G.row_ctas = row0;
+  G.utiles = utile0;
+  G.nsm = e->nsm;
   for (int pi = 0; pi < 2; ++pi) { G.hx_ns[pi] = kp[pi]; G.hx_tiles[pi] = tile0[pi]; }
   G.m_max = m_max;
   for (const ESlot& d : compact)
@@ -756,9 +792,11 @@ int launch_update_multi(const EGroup& G, int which, cudaStream_t st) {
     e_update_kernel<double><<<G.row_ctas, kUpdThreads, smem, st>>>(G.d_slots, G.ns, which);
     count_launch();
   }
-  if (G.hx_ns[1]) {
-    const size_t smem = umma_update_smem_bytes(P, G.m_max, nout);
-    e_update_umma_kernel<<<G.row_ctas, kUmmaRows, smem, st>>>(G.d_slots, G.ns, which);
+  if (G.hx_ns[1] && G.utiles) {
+    const UmmaPlan pl = umma_plan(P, G.m_max, nout, G.m_max, G.m_max);
+    if (!pl.nout_pass) { set_error("tcgen05 update plan does not fit shared memory"); return QDKP_ERR_ARG; }
+    e_update_umma_kernel<<<std::min(G.utiles, G.nsm), kUmmaThreads, pl.bytes, st>>>(
+        G.d_slots, G.ns, which, G.utiles, G.m_max);
     count_launch();
   }
   QDKP_CUDA_TRY(cudaGetLastError());
@@ -905,6 +943,7 @@ int qdkp_engine_create(int max_slots, int device, qdkp_engine** out) {
   if (err == cudaSuccess) err = cudaEventCreateWithFlags(&e->ev_out, cudaEventDisableTiming);
   if (err == cudaSuccess) err = cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming);
   if (err == cudaSuccess) err = cudaEventCreateWithFlags(&e->ev_join, cudaEventDisableTiming);
+  if (err == cudaSuccess) err = cudaDeviceGetAttribute(&e->nsm, cudaDevAttrMultiProcessorCount, device);
   if (err != cudaSuccess) {
     set_error(std::string("engine tables: ") + cudaGetErrorString(err));
     cudaFree(e->d_slots); cudaFree(e->d_hx); cudaFree(e->d_one);

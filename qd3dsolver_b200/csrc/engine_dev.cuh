@@ -56,6 +56,7 @@ struct ESlot {
   int gparts;           // CTAs of the Gram kernel
   long long rows_per_gpart;
   int norm0, gram0, row0;   // first CTA of this slot in the norm / Gram / row-kernel launches
+  int utile0;           // complex64 slots: first 128-row tile in the group's tcgen05 update space
   int rows_per_cta;     // rows per CTA in the row kernels (gather, update)
   EState* st;
 };
