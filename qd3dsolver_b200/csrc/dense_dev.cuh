@@ -144,7 +144,11 @@ static __device__ int block_tql(double2* S0, double2* S1, int n, double2* gtmp) 
         else if (i > k + 1) v = S0[i * n + k];
         hv[i] = v;
       }
-      if (lane == 0) s_tau = nx2 > 0.0 ? 1.0 / (nx * (nx + ax0)) : 0.0;
+      // a column whose |x| (|x| + |x0|) is below the smallest normal double is left as it is
+      // (entries of that size do not change a tridiagonal of a matrix of ordinary scale; 1 / it
+      // would overflow)
+      const double den = nx * (nx + ax0);
+      if (lane == 0) s_tau = den >= 2.2250738585072014e-308 ? 1.0 / den : 0.0;
     }
     __syncthreads();
     const double tau = s_tau;
@@ -515,7 +519,9 @@ static __device__ void rr_tridiag(const double2* __restrict__ Csm, int n,
     const double nx = sqrt(nx2);
     // alpha = -phase(x0) |x|, v = x - alpha e_1
     const double2 phs = ax0 > 0.0 ? make_double2(x0.x / ax0, x0.y / ax0) : make_double2(1.0, 0.0);
-    const double tau = nx2 > 0.0 ? 1.0 / (nx * (nx + ax0)) : 0.0;
+    // below the smallest normal double the column is left as it is (1 / den would overflow)
+    const double den = nx * (nx + ax0);
+    const double tau = den >= 2.2250738585072014e-308 ? 1.0 / den : 0.0;
     const double2 v0 = make_double2(x0.x + phs.x * nx, x0.y + phs.y * nx);
 #pragma unroll
     for (int q = 0; q < CC; ++q)
