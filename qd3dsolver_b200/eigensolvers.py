@@ -79,6 +79,8 @@ def lobpcg_device(A, X0, folded, sigma=0.0, tol=None, maxiter=20, restart_contro
     A = _require_op(A)
     X0d = X0 if hasattr(X0, 'data_ptr') else _to_device(X0)
     n, block = X0d.shape
+    if n < 5 * block:
+        return _dense_device(A, X0d, folded, sigma)
     prm = _lib.LobpcgParams(block=block, folded=int(bool(folded)), sigma=float(sigma),
                             tol=float(tol) if tol else 0.0, maxiter=int(maxiter),
                             restart_control=int(restart_control), precision=_lib.C128,
@@ -104,6 +106,35 @@ def lobpcg_device(A, X0, folded, sigma=0.0, tol=None, maxiter=20, restart_contro
                                      hx_seconds=float(info.hx_seconds),
                                      hx_bytes=float(info.hx_bytes),
                                      solver_seconds=info.seconds)
+
+
+def _dense_device(A, X0d, folded, sigma):
+    """scipy's lobpcg on a problem smaller than five block widths: it warns and solves the dense
+    eigenproblem instead (lobpcg.py:455-489). Here the dense A (or (A - sigma)^2) is formed on the
+    GPU by applying the device operator to the identity, and its lowest `block` pairs come from
+    the device's dense Hermitian solver; no iterations, an empty history."""
+    import warnings
+    torch = _torch()
+    n, block = X0d.shape
+    warnings.warn(f"The problem size {n} minus the constraints size 0 is too small relative to "
+                  f"the block size {block}. Using a dense eigensolver instead of LOBPCG "
+                  f"iterations. No output of the history of the iterations.", UserWarning,
+                  stacklevel=3)
+    eye = torch.eye(n, dtype=torch.complex128, device=X0d.device)
+    D = torch.empty((n, n), dtype=torch.complex128, device=X0d.device)
+    mode = _lib.APPLY_FOLDED if folded else _lib.APPLY_PLAIN
+    for c0 in range(0, n, 24):
+        c1 = min(n, c0 + 24)
+        D[:, c0:c1] = A.apply(eye[:, c0:c1].contiguous(), sigma=sigma if folded else 0.0,
+                              mode=mode)
+    D = 0.5 * (D + D.conj().T)
+    w, Vf = torch.linalg.eigh(D)
+    lam = w[:block].cpu().numpy()
+    V = Vf[:, :block].contiguous()
+    return lam, V, np.zeros((0, block)), dict(iterations=0, best_iteration=0, status='converged',
+                                              explicit_gram=False, hx_applications=n,
+                                              hx_launches=(n + 23) // 24, hx_seconds=0.0,
+                                              hx_bytes=0.0, solver_seconds=0.0, dense=True)
 
 
 # ------------------------------------------------------------------------------------------

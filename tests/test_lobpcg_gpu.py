@@ -123,3 +123,34 @@ def test_residual_verification_layer(small):
     assert np.allclose(eg.residual_norms(H, E, V), oe.residual_norms(Ho, E, V), rtol=1e-12)
     assert np.allclose(eg.rayleigh_quotients(H, V), oe.rayleigh_quotients(Ho, V), rtol=1e-12)
     assert eg.hermiticity_error(H) < 1e-12
+
+
+def test_small_problem_takes_the_dense_path(small):
+    """Fewer than five block widths of rows: like scipy's lobpcg, the drop-ins warn and solve the
+    dense eigenproblem (here on the device); energies equal the oracle operator's dense ones."""
+    import warnings
+    from qd3dsolver_b200 import eigensolvers as eg, kp_pryor as kpg
+    from oracle import kp_operator as ko
+    shape = (2, 2, 1)
+    f = {k: np.ascontiguousarray(v[:2, :2, :1]) for k, v in small['f8'].items()}
+    st = {k: f[k] for k in ('exx', 'eyy', 'ezz', 'exy', 'eyz', 'ezx')}
+    H = kpg.confined_hamiltonian(kpg.GridOperators(shape, small['h']), f, 8, strain=st)
+    Hd = ko.confined_hamiltonian(shape, small['h'], f, 8, strain=True).toarray()
+    w = np.linalg.eigvalsh(0.5 * (Hd + Hd.conj().T))
+    n = H.shape[0]
+    assert n < 5 * 9
+    with warnings.catch_warnings(record=True) as rec:
+        warnings.simplefilter('always')
+        E, V, info = eg.solve_lowest(H, k=6, verbose=False)
+    assert any('dense eigensolver' in str(r.message) for r in rec)
+    assert info['iterations'] == 0 and info['status'] == 'converged'
+    assert np.abs(E - w[:6]).max() < 1e-10 * np.abs(w).max()
+    assert info['residuals'].max() < 1e-9
+    sigma = float(0.5 * (w[n // 2] + w[n // 2 + 1]) + 1e-3)
+    with warnings.catch_warnings():
+        warnings.simplefilter('ignore')
+        Ei, Vi, ii = eg.solve_interior(H, k=6, sigma=sigma, verbose=False)
+    assert ii['iterations'] == 0
+    near = np.sort(w[np.argsort(np.abs(w - sigma))[:6]])
+    assert np.abs(Ei - near).max() < 1e-9 * np.abs(w).max()
+    H.close()
