@@ -5,6 +5,8 @@
 #include <cmath>
 #include <type_traits>
 #include <vector>
+#include <cstdlib>
+#include <cstring>
 
 #include "dense_dev.cuh"
 #include "umma_dev.cuh"
@@ -269,6 +271,16 @@ update_umma_kernel(const BlockList<float> A, const CoefList C, int q, long long 
   umma_ctx_free(cx);
 }
 
+bool c64_update_tcgen05() {
+  static const bool on = [] {
+    const char* v = std::getenv("QDKP_C64_UPDATE");
+    if (v && std::strcmp(v, "mma") == 0) return false;
+    if (v && std::strcmp(v, "tcgen05") == 0) return true;
+    return kC64UpdateTcgen05Default;
+  }();
+  return on;
+}
+
 template <typename T>
 int launch_update(const BlockList<T>& A, const double2* const* C, int q, long long n,
                   cplx<T>* Y, long long ldy, int accumulate, cudaStream_t st) {
@@ -276,7 +288,7 @@ int launch_update(const BlockList<T>& A, const double2* const* C, int q, long lo
   CoefList cl;
   for (int b = 0; b < 3; ++b) cl.c[b] = b < A.nblk ? C[b] : nullptr;
   const int P = A.total();
-  if constexpr (std::is_same<T, float>::value) {
+  if constexpr (std::is_same<T, float>::value) if (c64_update_tcgen05()) {
     static bool uattr = false;
     if (!uattr) {
       QDKP_CUDA_TRY(cudaFuncSetAttribute(update_umma_kernel,

@@ -33,6 +33,11 @@ struct BlockList {
   }
 };
 
+// Which kernel forms complex64 block updates: the tcgen05 pipeline (umma_dev.cuh) or the
+// split-TF32 mma.sync kernel (dense_dev.cuh). QDKP_C64_UPDATE=tcgen05 or =mma in the environment
+// chooses; read once per process.
+bool c64_update_tcgen05();
+
 // Tall block kernels, for complex128 (T = double) and complex64 (T = float) blocks; sums and
 // the Gram / coefficient matrices are FP64 either way.
 template <typename T>

@@ -792,7 +792,11 @@ int launch_update_multi(const EGroup& G, int which, cudaStream_t st) {
     e_update_kernel<double><<<G.row_ctas, kUpdThreads, smem, st>>>(G.d_slots, G.ns, which);
     count_launch();
   }
-  if (G.hx_ns[1] && G.utiles) {
+  if (G.hx_ns[1] && !c64_update_tcgen05()) {
+    const size_t smem = update_tf32_smem_bytes(P, G.m_max, nout);
+    e_update_kernel<float><<<G.row_ctas, kUpdThreads, smem, st>>>(G.d_slots, G.ns, which);
+    count_launch();
+  } else if (G.hx_ns[1] && G.utiles) {
     const UmmaPlan pl = umma_plan(P, G.m_max, nout, G.m_max, G.m_max);
     if (!pl.nout_pass) { set_error("tcgen05 update plan does not fit shared memory"); return QDKP_ERR_ARG; }
     e_update_umma_kernel<<<std::min(G.utiles, G.nsm), kUmmaThreads, pl.bytes, st>>>(

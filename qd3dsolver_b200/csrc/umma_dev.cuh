@@ -7,22 +7,25 @@
 // lo = the rest rounded to TF32), and the product formed as hi*hi + hi*lo + lo*hi with FP32
 // accumulation: FP32 accuracy from TF32 tensor cores.
 //
-// Work unit: a "chunk" = one block of one 128-row tile. A CTA of 17 warps runs its tiles as a
+// Work unit: a "chunk" = one block of one 128-row tile. A CTA of 13 warps runs its tiles as a
 // warp-specialised pipeline; the roles meet only on mbarriers, so each runs ahead of the next as
 // far as its ring allows:
 //  * producer / MMA warp (one lane): copies each chunk's rows (128 x ld complex64, contiguous in
 //    global memory) into one of S raw stages with cp.async.bulk, S chunks ahead, completion counted
-//    on the stage's mbarrier; when a chunk has been converted, issues its MMAs (M = 128,
-//    N = outputs x 2q padded to 16, K = 8 per instruction, three per K step for the split) into
-//    one of two TMEM accumulators and commits them to the operand buffer's "empty" mbarrier and,
-//    after a tile's last block, to the accumulator's "full" mbarrier;
+//    on the stage's mbarrier; when a chunk has been converted, issues its MMAs into one of two
+//    TMEM accumulators (M = 128, K = 8 per instruction; per K step Ahi [Bhi | Blo] with N = 2 Nr
+//    and Alo Bhi with N = Nr into the first Nr columns, Nr = outputs x 2q padded to 16, so that
+//    the accumulator holds Ahi Bhi + Alo Bhi beside Ahi Blo) and commits them to the operand
+//    buffer's "empty" mbarrier and, after a tile's last block, to the accumulator's "full" one;
 //  * eight converter warps: split the raw chunk into TF32 hi / lo parts and store them in one of
 //    two operand buffers in the no-swizzle K-major layout the MMA reads (8-row x 16-byte core
 //    matrices: element (row, k) at float offset ((k / 4) (R / 8) + row / 8) 32 + (row % 8) 4 + k % 4
 //    for R rows; leading-byte offset between the two 16-byte halves of an MMA-K step (R / 8) 128,
 //    stride-byte offset between 8-row groups 128);
-//  * eight epilogue warps: read a finished accumulator (tcgen05.ld 32x32b; warp w reads lane
-//    quarter w % 4 and one column half) and write the tile's output rows.
+//  * four epilogue warps: read a finished accumulator (tcgen05.ld 32x32b; warp w reads lane
+//    quarter w % 4), add its two halves and write the tile's output rows.
+// The coefficients are staged once per run as B = [Bhi; Blo], Bhi / Blo the TF32 parts of C''^T
+// (all outputs stacked along N, all blocks along K).
 #pragma once
 #include <cstdint>
 
@@ -32,19 +35,25 @@ namespace qdkp {
 
 constexpr int kUmmaRows = 128;          // MMA M: rows of a tile
 constexpr int kUmmaConvWarps = 8;      // converter warps (0-7)
-constexpr int kUmmaEpiWarps = 8;       // epilogue warps (8-15): two per TMEM lane quarter
-constexpr int kUmmaMmaWarp = kUmmaConvWarps + kUmmaEpiWarps;   // producer / MMA warp (16)
+constexpr int kUmmaEpiWarps = 4;       // epilogue warps (8-11): one per TMEM lane quarter
+constexpr int kUmmaMmaWarp = kUmmaConvWarps + kUmmaEpiWarps;   // producer / MMA warp (12)
+constexpr int kUmmaRowGroups = kUmmaRows / 8 / kUmmaConvWarps;  // 8-row groups per converter warp
 constexpr int kUmmaThreads = 32 * (kUmmaMmaWarp + 1);
 constexpr int kUmmaMaxStages = 8;       // raw chunk stages
 constexpr int kUmmaSmemLimit = 224 * 1024;
+// Complex64 block updates default to the split-TF32 mma.sync kernel, which measured faster on
+// the Fig-4 sweep's engine ticks (0.77 against 0.88 ms per complex64 tick of the b = 10 nm
+// valence solve); QDKP_C64_UPDATE=tcgen05 selects this pipeline.
+constexpr bool kC64UpdateTcgen05Default = false;
 
 __device__ __forceinline__ uint32_t umma_saddr(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
 }
+// x rounded to TF32 (10 explicit mantissa bits), to nearest with ties away from zero: the bits of
+// an IEEE float order its magnitudes, so adding half of the dropped unit and clearing the 13
+// dropped bits rounds the magnitude (integer ops at full rate; infinities and NaNs stay so)
 __device__ __forceinline__ uint32_t umma_tf32(float x) {
-  uint32_t r;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-  return r;
+  return (__float_as_uint(x) + 0x1000u) & 0xFFFFE000u;
 }
 // shared-memory matrix descriptor, no swizzle: start, leading and stride byte offsets (16-byte
 // units), descriptor version 1 at bit 46
@@ -101,6 +110,36 @@ __device__ __forceinline__ void umma_bulk_load(uint32_t dst, const void* src, ui
       "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
       :: "r"(dst), "l"(src), "r"(bytes), "r"(mbar) : "memory");
 }
+// bulk copy of `bytes` (a multiple of 16, both addresses 16-byte aligned) from this CTA's shared
+// memory to global memory, in the issuing thread's current bulk async-group
+__device__ __forceinline__ void umma_bulk_store(void* dst, uint32_t src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;"
+               :: "l"(dst), "r"(src), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void umma_bulk_commit() {
+  asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+// the issuing thread's bulk stores have read their shared memory, all but the newest `keep` groups
+__device__ __forceinline__ void umma_bulk_wait_read(int keep) {
+  if (keep) asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+  else asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+__device__ __forceinline__ void umma_bulk_wait_all() {
+  asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+}
+// barrier 1 among the epilogue warps only
+__device__ __forceinline__ void umma_epi_sync() {
+  asm volatile("bar.sync 1, %0;" :: "r"(32 * kUmmaEpiWarps) : "memory");
+}
+// barrier 1 among the epilogue warps, returning whether v held for any of them (a decision all
+// of them take alike)
+__device__ __forceinline__ bool umma_epi_any(bool v) {
+  uint32_t r;
+  asm volatile("{\n\t.reg .pred p, q;\n\tsetp.ne.u32 q, %1, 0;\n\t"
+               "bar.red.or.pred p, 1, %2, q;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+               : "=r"(r) : "r"((uint32_t)v), "r"(32 * kUmmaEpiWarps) : "memory");
+  return r != 0;
+}
 __device__ __forceinline__ void umma_ld8(uint32_t taddr, float (&v)[8]) {
   uint32_t r[8];
   asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
@@ -128,9 +167,11 @@ struct UmmaPlan {
   int Kcap;           // K capacity of B (floats): every split of P columns over three blocks fits
   int KbMax;          // K of one operand buffer (floats)
   int nbuf;           // operand buffers (2: the MMA of chunk i overlaps the conversion of i + 1)
+  int nob;            // output staging buffers (0: the epilogue writes rows directly)
   int S;              // raw stages
-  int ldmax;
-  unsigned offA, offRaw, bytes;
+  int ldmax, q;
+  unsigned ostage;    // bytes of one output staging buffer (all outputs of a tile)
+  unsigned offA, offOut, offRaw, bytes;
 };
 __host__ __device__ inline UmmaPlan umma_plan(int P, int q, int nout, int cmax, int ldmax) {
   UmmaPlan p{};
@@ -138,26 +179,30 @@ __host__ __device__ inline UmmaPlan umma_plan(int P, int q, int nout, int cmax, 
   p.Kcap = 8 * ((P + 3) / 4 + 2);
   p.KbMax = umma_Kb(cmax < P ? cmax : P);
   p.ldmax = ldmax;
+  p.q = q;
   const unsigned raw = (unsigned)kUmmaRows * ldmax * 8u;
   const unsigned abuf = 2u * kUmmaRows * p.KbMax * 4u;
+  // one pass over A first, then two operand buffers, then double-buffered output staging
   for (int np = nout; np >= 1; --np)
-    for (int nb = 2; nb >= 1; --nb) {
-      const unsigned b = 2u * np * p.N * p.Kcap * 4u;
-      const unsigned fixed = b + nb * abuf;
-      if (fixed + 2 * raw > (unsigned)kUmmaSmemLimit) continue;
-      int S = (int)(((unsigned)kUmmaSmemLimit - fixed) / raw);
-      if (S > kUmmaMaxStages) S = kUmmaMaxStages;
-      p.nout_pass = np; p.Ntot = np * p.N; p.nbuf = nb; p.S = S;
-      p.offA = b; p.offRaw = fixed; p.bytes = fixed + S * raw;
-      return p;
-    }
+    for (int nb = 2; nb >= 1; --nb)
+      for (int nob = 2; nob >= 0; --nob) {
+        const unsigned b = 2u * np * p.N * p.Kcap * 4u;
+        const unsigned ost = (unsigned)np * kUmmaRows * q * 8u;
+        const unsigned fixed = b + nb * abuf + nob * ost;
+        if (fixed + 2 * raw > (unsigned)kUmmaSmemLimit) continue;
+        int S = (int)(((unsigned)kUmmaSmemLimit - fixed) / raw);
+        if (S > kUmmaMaxStages) S = kUmmaMaxStages;
+        p.nout_pass = np; p.Ntot = np * p.N; p.nbuf = nb; p.nob = nob; p.ostage = ost; p.S = S;
+        p.offA = b; p.offOut = b + nb * abuf; p.offRaw = fixed; p.bytes = fixed + S * raw;
+        return p;
+      }
   p.nout_pass = 0;                 // does not fit (rejected by the launchers)
   return p;
 }
-// accumulator columns a CTA allocates: two accumulators of Ntot columns, a power of two >= 32
+// accumulator columns a CTA allocates: two accumulators of 2 Ntot columns, a power of two >= 32
 __host__ __device__ __forceinline__ uint32_t umma_tmem_cols(const UmmaPlan& p) {
   uint32_t c = 32;
-  while ((int)c < 2 * p.Ntot) c <<= 1;
+  while ((int)c < 4 * p.Ntot) c <<= 1;
   return c;
 }
 
@@ -273,8 +318,7 @@ static __device__ __noinline__ bool umma_run(const UmmaPlan& pl_in, UmmaCtx& cx_
   }
   const int P = cols[0] + cols[1] + cols[2];
   const int N = pl.N, Nr = nout * N;          // accumulator columns of this run
-  float* Bhi = reinterpret_cast<float*>(smem);
-  float* Blo = Bhi + Nr * pl.Kcap;
+  float* Bs = reinterpret_cast<float*>(smem);   // [Bhi; Blo]: 2 Nr rows x Kcap
   const int Ktot = kb0[nb];
   const float sg = neg ? -1.f : 1.f;
   // B = C''^T (Nr x Ktot): for the coefficient of A's column c (block b, local i) and output
@@ -297,17 +341,16 @@ static __device__ __noinline__ bool umma_run(const UmmaPlan& pl_in, UmmaCtx& cx_
     for (int t = 0; t < 4; ++t) {
       const int j = o * N + 2 * jj + (t >> 1), k = kb0[b] + 2 * i + (t & 1);
       const uint32_t hi = umma_tf32(v[t]);
-      const int off = umma_off(j, k, Nr);
-      Bhi[off] = __uint_as_float(hi);
-      Blo[off] = __uint_as_float(umma_tf32(v[t] - __uint_as_float(hi)));
+      Bs[umma_off(j, k, 2 * Nr)] = __uint_as_float(hi);
+      Bs[umma_off(Nr + j, k, 2 * Nr)] = __uint_as_float(umma_tf32(v[t] - __uint_as_float(hi)));
     }
   }
   for (int e = tid; e < Nr * Ktot; e += blockDim.x) {
     const int j = e / Ktot, k = e - j * Ktot;
     const int b = k < kb0[1] ? 0 : (k < kb0[2] ? 1 : 2);
     if (((j % N) >> 1) >= q || ((k - kb0[b]) >> 1) >= cols[b]) {
-      Bhi[umma_off(j, k, Nr)] = 0.f;
-      Blo[umma_off(j, k, Nr)] = 0.f;
+      Bs[umma_off(j, k, 2 * Nr)] = 0.f;
+      Bs[umma_off(Nr + j, k, 2 * Nr)] = 0.f;
     }
   }
   if (tid == 0) s_fault = 0;
@@ -333,13 +376,14 @@ static __device__ __noinline__ bool umma_run(const UmmaPlan& pl_in, UmmaCtx& cx_
     int s = (int)(g0 % S), h = (int)(g0 % nbuf);
     uint32_t fpar = (uint32_t)((g0 / S) & 1), hpar = (uint32_t)((g0 / nbuf) & 1);
     bool hused = g0 >= nbuf;                     // buffer h was filled by an earlier chunk
-    // a thread's elements: rows (warp + 8 p) 8 + lane % 8 (p = 0, 1), complex columns 4 kk + lane / 8
+    // a thread's elements: rows (warp + W p) 8 + lane % 8 (W converter warps, p < 16 / W),
+    // complex columns 4 kk + lane / 8
     const int lrow = lane & 7, lq = lane >> 3;
-    int rowp[2], offp[2];
+    int rowp[kUmmaRowGroups], offp[kUmmaRowGroups];
 #pragma unroll
-    for (int p = 0; p < 2; ++p) {
-      rowp[p] = (warp + 8 * p) * 8 + lrow;
-      offp[p] = (((lq >> 1) * 16) + warp + 8 * p) * 32 + lrow * 4 + (lq & 1) * 2;
+    for (int p = 0; p < kUmmaRowGroups; ++p) {
+      rowp[p] = (warp + kUmmaConvWarps * p) * 8 + lrow;
+      offp[p] = (((lq >> 1) * 16) + warp + kUmmaConvWarps * p) * 32 + lrow * 4 + (lq & 1) * 2;
     }
     long long ti = 0;
     int b = 0;
@@ -355,23 +399,70 @@ static __device__ __noinline__ bool umma_run(const UmmaPlan& pl_in, UmmaCtx& cx_
       const int ld = (int)ldl, rows = tile_rows(ti), cb = cols[b], nq = (cb + 3) / 4;
       const float2* gp = bp[b];
       constexpr int kQuads = kMaxBlock / 4;
-      float2 x[2][kQuads];
+      float2 x[kUmmaRowGroups][kQuads];
+      if (bk && (ld & 1) == 0) {
+        // complex pairs: lane (8-row offset lane % 8, pair lane / 8) loads columns c, c + 1
+        // (c = 8 kk + 2 (lane / 8)) of its rows as one 16-byte word and stores their four K
+        // values as one 16-byte word each of hi and lo
+        const int lp = lane >> 3, cmaxe = (cb - 1) & ~1, c4 = (cb + 3) / 4 * 4;
+        constexpr int kPairs = (kMaxBlock + 7) / 8;
+        float4 y[kUmmaRowGroups][kPairs];
 #pragma unroll
-      for (int kk = 0; kk < kQuads; ++kk)
+        for (int kk = 0; kk < kPairs; ++kk) {
+          const int c = 8 * kk + 2 * lp, cl = min(c, cmaxe);
 #pragma unroll
-        for (int p = 0; p < 2; ++p) {
-          const int c = 4 * kk + lq;
-          x[p][kk] = make_float2(0.f, 0.f);
-          if (kk < nq && c < cb) {
-            if (bk) x[p][kk] = rw[rowp[p] * ld + c];
-            else if (rowp[p] < rows) x[p][kk] = gp[(t0 + rowp[p]) * ldl + c];
+          for (int p = 0; p < kUmmaRowGroups; ++p) {
+            float4 v = reinterpret_cast<const float4*>(rw)[(rowp[p] * ld + cl) >> 1];
+            if (c >= cb) { v.x = 0.f; v.y = 0.f; }
+            if (c + 1 >= cb) { v.z = 0.f; v.w = 0.f; }
+            y[p][kk] = v;
           }
         }
+#pragma unroll
+        for (int kk = 0; kk < kPairs; ++kk) {
+          const int c = 8 * kk + 2 * lp;
+#pragma unroll
+          for (int p = 0; p < kUmmaRowGroups; ++p)
+            if (c < c4) {
+              const float4 v = y[p][kk];
+              const int off = ((4 * kk + lp) * 16 + warp + kUmmaConvWarps * p) * 32 + lrow * 4;
+              float4 hi, lo;
+              hi.x = __uint_as_float(umma_tf32(v.x)); lo.x = __uint_as_float(umma_tf32(v.x - hi.x));
+              hi.y = __uint_as_float(umma_tf32(v.y)); lo.y = __uint_as_float(umma_tf32(v.y - hi.y));
+              hi.z = __uint_as_float(umma_tf32(v.z)); lo.z = __uint_as_float(umma_tf32(v.z - hi.z));
+              hi.w = __uint_as_float(umma_tf32(v.w)); lo.w = __uint_as_float(umma_tf32(v.w - hi.w));
+              *reinterpret_cast<float4*>(Ah + off) = hi;
+              *reinterpret_cast<float4*>(Al + off) = lo;
+            }
+        }
+      } else {
+      if (bk) {
+        // straight-line shared loads (an in-range index everywhere, zero selected past the
+        // block's columns), so that all of a thread's loads are in flight together
+#pragma unroll
+        for (int kk = 0; kk < kQuads; ++kk) {
+          const int c = 4 * kk + lq, cc = min(c, cb - 1);
+#pragma unroll
+          for (int p = 0; p < kUmmaRowGroups; ++p) {
+            const float2 v = kk < nq ? rw[rowp[p] * ld + cc] : make_float2(0.f, 0.f);
+            x[p][kk] = c < cb ? v : make_float2(0.f, 0.f);
+          }
+        }
+      } else {
+#pragma unroll
+        for (int kk = 0; kk < kQuads; ++kk)
+#pragma unroll
+          for (int p = 0; p < kUmmaRowGroups; ++p) {
+            const int c = 4 * kk + lq;
+            x[p][kk] = make_float2(0.f, 0.f);
+            if (kk < nq && c < cb && rowp[p] < rows) x[p][kk] = gp[(t0 + rowp[p]) * ldl + c];
+          }
+      }
 #pragma unroll
       for (int kk = 0; kk < kQuads; ++kk) {
         if (kk >= nq) break;
 #pragma unroll
-        for (int p = 0; p < 2; ++p) {
+        for (int p = 0; p < kUmmaRowGroups; ++p) {
           const float2 v = x[p][kk];
           const uint32_t hx = umma_tf32(v.x), hy = umma_tf32(v.y);
           const int off = offp[p] + kk * 1024;
@@ -380,6 +471,7 @@ static __device__ __noinline__ bool umma_run(const UmmaPlan& pl_in, UmmaCtx& cx_
               make_float2(__uint_as_float(umma_tf32(v.x - __uint_as_float(hx))),
                           __uint_as_float(umma_tf32(v.y - __uint_as_float(hy))));
         }
+      }
       }
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       __syncwarp();
@@ -391,12 +483,23 @@ static __device__ __noinline__ bool umma_run(const UmmaPlan& pl_in, UmmaCtx& cx_
     }
   } else if (warp < kUmmaMmaWarp) {
     // ---------------- epilogue: accumulator -> output rows ----------------
-    const int e = warp - kUmmaConvWarps, quarter = warp & 3, half = e >> 2;
-    const int ng = Nr / 8, gh = ng / 2, gfirst = half * gh;   // this half's 8-column groups
-    const bool vec = (ldy & 1) == 0 &&
-                     ((reinterpret_cast<uintptr_t>(Ys[0]) | (nout == 2 ? reinterpret_cast<uintptr_t>(Ys[1]) : 0)) & 15) == 0;
+    // With staging (pl.nob > 0) a tile's rows go to a shared-memory image of the output rows first
+    // and from there to global memory: one bulk store per output for a full tile of contiguous
+    // rows (ldy == q), otherwise a coalesced copy by the epilogue warps.
+    constexpr int kParts = kUmmaEpiWarps / 4;    // warps per lane quarter, each a column part
+    const int e = warp - kUmmaConvWarps, quarter = warp & 3, part = e / 4;
+    const int et = tid - 32 * kUmmaConvWarps;   // 0 .. 32 kUmmaEpiWarps - 1
+    const int ng = Nr / 8, gh = ng / kParts, gfirst = part * gh;   // this part's 8-column groups
+    const bool stage = pl.nob > 0;
+    uintptr_t al = 0;
+    for (int o = 0; o < nout; ++o) al |= reinterpret_cast<uintptr_t>(Ys[o]);
+    const bool vec = (ldy & 1) == 0 && (al & 15) == 0;
+    const bool bulk_out = stage && ldy == q && (q & 1) == 0 && (al & 15) == 0;
+    const bool svec = (q & 1) == 0;              // 16-byte staging writes
+    int ob = 0, pending = 0;                     // staging buffer; bulk groups not yet read
     for (long long ti = 0; ti < T; ++ti) {
-      if (*vfault) break;
+      // with staging the epilogue warps meet on barrier 1, so they stop together
+      if (stage ? umma_epi_any(*vfault != 0) : (*vfault != 0)) break;
       const long long tg = tg0 + ti;
       const int a = (int)(tg & 1);
       const bool ok = umma_wait(umma_bar_afull(cx, a), (uint32_t)((tg >> 1) & 1));
@@ -404,12 +507,20 @@ static __device__ __noinline__ bool umma_run(const UmmaPlan& pl_in, UmmaCtx& cx_
       asm volatile("tcgen05.fence::after_thread_sync;");
       const int rows = tile_rows(ti), rl = quarter * 32 + lane;
       const long long r = r0 + ti * kUmmaRows + rl;
-      const uint32_t tb = cx.tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(a * pl.Ntot);
+      float2* sb = reinterpret_cast<float2*>(smem + pl.offOut + (size_t)ob * pl.ostage);
+      if (stage) {                               // the buffer's last bulk store has read it
+        if (et == 0 && pending >= pl.nob) { umma_bulk_wait_read(pl.nob - 1); --pending; }
+        umma_epi_sync();
+      }
+      const uint32_t tb = cx.tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(a * 2 * pl.Ntot);
       for (int u0 = 0; u0 < gh; u0 += 2) {       // two groups at a time
-        float v[2][8];
+        float v[2][8], w[2][8];
 #pragma unroll
         for (int du = 0; du < 2; ++du)
-          if (u0 + du < gh) umma_ld8(tb + (uint32_t)(8 * (gfirst + u0 + du)), v[du]);
+          if (u0 + du < gh) {
+            umma_ld8(tb + (uint32_t)(8 * (gfirst + u0 + du)), v[du]);
+            umma_ld8(tb + (uint32_t)(Nr + 8 * (gfirst + u0 + du)), w[du]);
+          }
         float2 old[2][4];
 #pragma unroll
         for (int du = 0; du < 2; ++du) {
@@ -427,11 +538,11 @@ static __device__ __noinline__ bool umma_run(const UmmaPlan& pl_in, UmmaCtx& cx_
           float2 y[4];
 #pragma unroll
           for (int x = 0; x < 4; ++x) {
-            y[x] = make_float2(v[du][2 * x], v[du][2 * x + 1]);
+            y[x] = make_float2(v[du][2 * x] + w[du][2 * x], v[du][2 * x + 1] + w[du][2 * x + 1]);
             if (o == 0) { y[x].x += old[du][x].x; y[x].y += old[du][x].y; }
           }
-          float2* dst = Ys[o] + r * ldy + jj0;
-          if (vec && jj0 + 4 <= q) {
+          float2* dst = stage ? sb + ((size_t)o * kUmmaRows + rl) * q + jj0 : Ys[o] + r * ldy + jj0;
+          if ((stage ? svec : vec) && jj0 + 4 <= q) {
             reinterpret_cast<float4*>(dst)[0] = make_float4(y[0].x, y[0].y, y[1].x, y[1].y);
             reinterpret_cast<float4*>(dst)[1] = make_float4(y[2].x, y[2].y, y[3].x, y[3].y);
           } else {
@@ -443,14 +554,35 @@ static __device__ __noinline__ bool umma_run(const UmmaPlan& pl_in, UmmaCtx& cx_
       }
       asm volatile("tcgen05.fence::before_thread_sync;");
       __syncwarp();
-      if (lane == 0) umma_arrive(umma_bar_aempty(cx, a));
+      if (lane == 0) umma_arrive(umma_bar_aempty(cx, a));   // the accumulator is free again
+      if (stage) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        umma_epi_sync();
+        const long long row0 = r0 + ti * kUmmaRows;
+        if (bulk_out && rows == kUmmaRows) {
+          if (et == 0) {
+            for (int o = 0; o < nout; ++o)
+              umma_bulk_store(Ys[o] + row0 * q, umma_saddr(sb + (size_t)o * kUmmaRows * q),
+                              (uint32_t)(kUmmaRows * q * 8));
+            umma_bulk_commit();
+            ++pending;
+          }
+        } else {
+          for (int o = 0; o < nout; ++o)
+            for (int k = et; k < rows * q; k += 32 * kUmmaEpiWarps)
+              Ys[o][(row0 + k / q) * ldy + k % q] = sb[(size_t)o * kUmmaRows * q + k];
+          umma_epi_sync();                       // read before the buffer is written again
+        }
+        if (pl.nob == 2) ob ^= 1;
+      }
       if (!ok) *vfault = 1;
     }
+    if (et == 0 && pending) umma_bulk_wait_all();   // the output rows are written
   } else if (lane == 0) {
     // ---------------- producer / MMA issue (one thread) ----------------
-    const uint32_t idesc = umma_idesc_tf32(Nr);
-    const uint32_t lboA = (kUmmaRows / 8) * 128, lboB = (uint32_t)(Nr / 8) * 128;
-    const uint64_t dBh = umma_desc(umma_saddr(Bhi), lboB, 128), dBl = umma_desc(umma_saddr(Blo), lboB, 128);
+    const uint32_t idesc2 = umma_idesc_tf32(2 * Nr), idesc1 = umma_idesc_tf32(Nr);
+    const uint32_t lboA = (kUmmaRows / 8) * 128, lboB = (uint32_t)(2 * Nr / 8) * 128;
+    const uint64_t dB = umma_desc(umma_saddr(Bs), lboB, 128);
     uint64_t dAh[2], dAl[2];
     for (int h = 0; h < 2; ++h) {
       const uint32_t aH = umma_saddr(smem + pl.offA + (size_t)h * abytes);
@@ -489,17 +621,16 @@ static __device__ __noinline__ bool umma_run(const UmmaPlan& pl_in, UmmaCtx& cx_
       if (!ok) break;
       done = i + 1;                              // chunk i has been converted (its stage is free)
       asm volatile("tcgen05.fence::after_thread_sync;");
-      const uint32_t d = cx.tmem + (uint32_t)(a * pl.Ntot);
+      const uint32_t d = cx.tmem + (uint32_t)(a * 2 * pl.Ntot);
       const int steps = umma_Kb(cols[b]) / 8;
       const uint64_t ah = dAh[h], al = dAl[h];
-      uint64_t bh = dBh + (uint64_t)((kb0[b] / 4) * lboB >> 4), bl = dBl + (uint64_t)((kb0[b] / 4) * lboB >> 4);
+      uint64_t bd = dB + (uint64_t)((kb0[b] / 4) * lboB >> 4);
       uint64_t oa = 0;
       const uint64_t sa = (2 * lboA) >> 4, sb = (2 * lboB) >> 4;
       for (int st = 0; st < steps; ++st) {
-        umma_mma(d, ah + oa, bh, idesc, (b > 0 || st > 0) ? 1u : 0u);
-        umma_mma(d, ah + oa, bl, idesc, 1u);
-        umma_mma(d, al + oa, bh, idesc, 1u);
-        oa += sa; bh += sb; bl += sb;
+        umma_mma(d, ah + oa, bd, idesc2, (b > 0 || st > 0) ? 1u : 0u);   // Ahi [Bhi | Blo]
+        umma_mma(d, al + oa, bd, idesc1, 1u);                             // + Alo Bhi
+        oa += sa; bd += sb;
       }
       umma_commit(umma_bar_cempty(cx, h));
       if (b == nb - 1) umma_commit(umma_bar_afull(cx, a));
