@@ -626,32 +626,6 @@ kp_apply_kernel(const HXArgs<T> a) {
   hx_item<T, NB>(a, s, it - s * a.m);
 }
 
-// Many operators and blocks in one launch (the batched engine): CTA b serves slot k with
-// tile0[k] <= b < tile0[k+1]; the column count is read on the device (the slot's active width).
-template <typename T>
-__global__ void __launch_bounds__(kApplyThreads, ApplyOcc<T>::kMinBlocks)
-kp_apply_multi_kernel(const HXSlot* __restrict__ slots, int nslots) {
-  int k = 0;
-  while (k + 1 < nslots && (int)blockIdx.x >= slots[k + 1].tile0) ++k;
-  const HXSlot& d = slots[k];
-  if (d.skip && *d.skip) return;
-  const int m = d.m_dev ? *d.m_dev : d.m;
-  const int it = (blockIdx.x - d.tile0) * kApplyThreads + threadIdx.x;
-  if (m <= 0 || it >= d.N * m) return;
-  HXArgs<T> a;
-  a.rec = static_cast<const T*>(d.rec);
-  a.msk = d.msk;
-  a.X = static_cast<const cplx<T>*>(d.X);
-  a.Y = static_cast<cplx<T>*>(d.Y);
-  a.N = d.N; a.ldx = d.ld_same ? m : d.ldx; a.ldy = d.ld_same ? m : d.ldy;
-  a.m = m; a.sx = d.sx; a.sy = d.sy;
-  a.nz = d.sy; a.nzp = d.nzp; a.NP = d.NP;
-  a.shift = d.shifted ? (T)(-d.sigma) : T(0);
-  a.cb = (T)d.cb;
-  const int s = it / m;
-  hx_item<T, 8>(a, s, it - s * m);
-}
-
 // ---------------------------------------------------------------------------------------------
 // Staged kernel (eight bands): a CTA owns a TY x TZ tile of (y, z) sites and MC consecutive
 // columns and walks a run of x planes. A ring of four shared-memory plane buffers holds planes
@@ -1014,6 +988,94 @@ __device__ __forceinline__ void hx_packed_cols(const L& ld, const Rc& rc, float 
       Y[c][b] = make_float2(a.x - d.y, a.y + d.x);
     }
 }
+
+// Two adjacent complex64 columns of one site from global memory, eight bands, for
+// hx_packed_cols: a band of both columns is one 16-byte load. A neighbour outside the grid reads
+// the site itself instead: its weight in the record is zero, so it adds nothing.
+struct GlobalPairLoader {
+  const unsigned long long* __restrict__ xs;   // &X[0, s, j], j even
+  long long bs;                                // band stride N ldx (complex values)
+  int xstr[3];                                 // site strides of x, y, z (complex values)
+  unsigned msk;                                // neighbour mask of the site (site_mask)
+  __device__ __forceinline__ void at(int off, int b0, f2 (&x)[2][8]) const {
+#pragma unroll
+    for (int b = b0; b < 8; ++b) {
+      const ulonglong2 v = __ldg(reinterpret_cast<const ulonglong2*>(xs + (b * bs + off)));
+      x[0][b] = v.x;
+      x[1][b] = v.y;
+    }
+  }
+  __device__ __forceinline__ void centre(f2 (&x)[2][8]) const { at(0, 0, x); }
+  __device__ __forceinline__ void face(int f, f2 (&x)[2][8]) const {
+    const int off = (f & 1) ? -xstr[f >> 1] : xstr[f >> 1];
+    at(((msk >> f) & 1u) ? off : 0, 0, x);
+  }
+  __device__ __forceinline__ void edge(int pl, int e, f2 (&x)[2][8]) const {
+    const int ea = pl == 0 ? 0 : 2, eb = pl == 0 ? 1 : (pl == 1 ? 0 : 1);
+    const int sa = (e & 1) ? -1 : 1, sb = (e & 2) ? -1 : 1;
+    const int off = sa * xstr[ea] + sb * xstr[eb];
+    at(((msk >> (6 + 4 * pl + e)) & 1u) ? off : 0, 2, x);
+  }
+};
+
+// complex64, eight bands: columns j, j + 1 of site s (m, ldx and ldy even, X and Y 16-byte
+// aligned)
+__device__ __forceinline__ void hx_item_pair(const HXArgs<float>& a, int s, int j) {
+  GlobalPairLoader ld;
+  ld.xs = reinterpret_cast<const unsigned long long*>(a.X + ((long long)s * a.ldx + j));
+  ld.bs = (long long)a.N * a.ldx;
+  ld.xstr[0] = a.sx * a.ldx; ld.xstr[1] = a.sy * a.ldx; ld.xstr[2] = a.ldx;
+  ld.msk = __ldg(a.msk + s);
+  GlobalRecord<float> rc;
+  rc.R = a.rec + (s + (s / a.nz) * (a.nzp - a.nz));
+  rc.NP = a.NP;
+  float2 y[2][8];
+  hx_packed_cols<2>(ld, rc, a.shift, a.cb, y);
+  float2* __restrict__ ys = a.Y + ((long long)s * a.ldy + j);
+  const long long ybs = (long long)a.N * a.ldy;
+#pragma unroll
+  for (int b = 0; b < 8; ++b)
+    *reinterpret_cast<float4*>(ys + b * ybs) = make_float4(y[0][b].x, y[0][b].y, y[1][b].x, y[1][b].y);
+}
+
+// Many operators and blocks in one launch (the batched engine): CTA b serves slot k with
+// tile0[k] <= b < tile0[k+1]; the column count is read on the device (the slot's active width).
+template <typename T>
+__global__ void __launch_bounds__(kApplyThreads, 2)
+kp_apply_multi_kernel(const HXSlot* __restrict__ slots, int nslots) {
+  int k = 0;
+  while (k + 1 < nslots && (int)blockIdx.x >= slots[k + 1].tile0) ++k;
+  const HXSlot& d = slots[k];
+  if (d.skip && *d.skip) return;
+  const int m = d.m_dev ? *d.m_dev : d.m;
+  const int it = (blockIdx.x - d.tile0) * kApplyThreads + threadIdx.x;
+  if (m <= 0 || it >= d.N * m) return;
+  HXArgs<T> a;
+  a.rec = static_cast<const T*>(d.rec);
+  a.msk = d.msk;
+  a.X = static_cast<const cplx<T>*>(d.X);
+  a.Y = static_cast<cplx<T>*>(d.Y);
+  a.N = d.N; a.ldx = d.ld_same ? m : d.ldx; a.ldy = d.ld_same ? m : d.ldy;
+  a.m = m; a.sx = d.sx; a.sy = d.sy;
+  a.nz = d.sy; a.nzp = d.nzp; a.NP = d.NP;
+  a.shift = d.shifted ? (T)(-d.sigma) : T(0);
+  a.cb = (T)d.cb;
+  if constexpr (std::is_same<T, float>::value) {
+    // complex64: two columns per thread where the widths and pointers allow 16-byte words (the
+    // slot's CTAs past the pairs' count exit)
+    if (((m | a.ldx | a.ldy) & 1) == 0 &&
+        ((reinterpret_cast<uintptr_t>(a.X) | reinterpret_cast<uintptr_t>(a.Y)) & 15) == 0) {
+      const int mp = m >> 1;
+      if (it >= d.N * mp) return;
+      const int s = it / mp;
+      hx_item_pair(a, s, 2 * (it - s * mp));
+      return;
+    }
+  }
+  const int s = it / m;
+  hx_item<T, 8>(a, s, it - s * m);
+}
+
 
 // mbarrier and bulk-tensor copy primitives (PTX ISA: mbarrier, cp.async.bulk.tensor)
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
