@@ -281,7 +281,9 @@ int qdkp_engine_retire(qdkp_engine* e, int slot, double* lambda, void* V, double
  * accumulated in FP32, partial sums in FP64).
  *   qdkp_block_gram:   out (host, P x Q complex128, row-major) = A^H B, A (n x P, lda), B (n x Q)
  *   qdkp_block_update: Y (n x q) = A (n x P) C, C (host, P x q complex128, row-major)
- * Synchronous on `stream`; workspaces from the *_workspace_size functions.
+ * Synchronous on `stream`; workspaces from the *_workspace_size functions. Complex64 updates (here
+ * and in the engine) run on the split-TF32 mma.sync kernel unless the environment variable
+ * QDKP_C64_UPDATE=tcgen05 selects the tcgen05 / TMEM pipeline; it is read once per process.
  */
 size_t qdkp_block_gram_workspace_size(int P, int Q);
 int qdkp_block_gram(const void* A, int64_t lda, int P, const void* B, int64_t ldb, int Q,
